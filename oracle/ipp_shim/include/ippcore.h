@@ -1,0 +1,2 @@
+/* ippcore.h -- oracle stand-in; every declaration lives in ipps.h. */
+#include "ipps.h"
