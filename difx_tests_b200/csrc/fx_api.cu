@@ -1,0 +1,564 @@
+// fx_api.cu -- C ABI (include/fxcorr.h): context lifetime, buffer layout and
+// the per-call launch sequence  K0 delay table -> counts -> [F stage -> X stage]
+// per chunk of FFTs -> finalise on demand.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "../../include/fxcorr.h"
+#include "fx_internal.h"
+#include "fx_kernels.h"
+
+using namespace fx;
+
+struct fxc_ctx {
+    fxc_config cfg;
+    int device = 0;
+    int F = 0, nsig = 0, npair = 0, npair_ant = 0, nbl = 0, nout = 0;
+    int ld = 0;            // delay-table leading dimension (FFTs, multiple of 128)
+    int T = 0;             // FFT slots per chunk (multiple of 64)
+    int rows = 0;          // F16 spectra rows per channel
+    size_t pitch = 0;      // input row pitch
+    size_t subint = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    uint8_t* d_in = nullptr;
+    double* d_delays = nullptr;
+    double* d_offs = nullptr;
+    double* d_sblo = nullptr;
+    float* d_chan_sub = nullptr;
+    float* d_chan_step = nullptr;
+    DelayEntry* d_dtab = nullptr;
+    uint32_t* d_vbits = nullptr;
+    void* d_spec = nullptr;
+    size_t spec_bytes = 0;
+    float2* d_acc = nullptr;
+    size_t acc_bytes = 0;
+    int* d_counts = nullptr;
+    float2* d_vis = nullptr;
+    size_t vis_bytes = 0;
+    // stage timing (fxc_enable_stage_timing / fxc_stage_times)
+    bool timing = false;
+    struct Pending {
+        int stage;
+        cudaEvent_t a, b;
+    };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> event_pool;
+    double stage_ms[FXC_NSTAGE] = {0, 0, 0, 0};
+    long long stage_launches[FXC_NSTAGE] = {0, 0, 0, 0};
+};
+
+namespace {
+
+cudaEvent_t pool_event(fxc_ctx* x)
+{
+    if (!x->event_pool.empty()) {
+        cudaEvent_t e = x->event_pool.back();
+        x->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// Brackets the launches of one stage with events when timing is enabled.
+struct StageScope {
+    fxc_ctx* x;
+    int stage;
+    cudaEvent_t a = nullptr;
+    StageScope(fxc_ctx* x_, int s, int nlaunch) : x(x_), stage(s)
+    {
+        x->stage_launches[s] += nlaunch;
+        if (x->timing) {
+            a = pool_event(x);
+            cudaEventRecord(a, x->stream);
+        }
+    }
+    ~StageScope()
+    {
+        if (a) {
+            cudaEvent_t b = pool_event(x);
+            cudaEventRecord(b, x->stream);
+            x->pending.push_back({stage, a, b});
+        }
+    }
+};
+
+}  // namespace
+
+static thread_local int g_last_cuda = 0;
+
+#define FXC_CK(call)                                   \
+    do {                                               \
+        cudaError_t e_ = (call);                       \
+        if (e_ != cudaSuccess) {                       \
+            g_last_cuda = (int)e_;                     \
+            return e_ == cudaErrorMemoryAllocation ? FXC_ERR_NOMEM : FXC_ERR_CUDA; \
+        }                                              \
+    } while (0)
+
+static size_t round_up(size_t x, size_t m) { return (x + m - 1) / m * m; }
+
+extern "C" {
+
+void fxc_config_default(fxc_config* c)
+{
+    if (!c) return;
+    std::memset(c, 0, sizeof(*c));
+    c->npol = 2;
+    c->nbit = 2;
+    c->iscomplex = 0;
+    c->nsubband = 1;
+    c->xmode = FXC_X_PLAIN_FP32;
+}
+
+size_t fxc_subint_bytes(const fxc_config* c)
+{
+    if (!c) return 0;
+    // allocDataHost.c:21 (cfactor = 2 for real data)
+    return (size_t)c->nchan * 2 * (size_t)(c->numffts + 1) * c->nbit / 8 * c->npol;
+}
+
+int fxc_num_baselines(const fxc_config* c) { return c ? c->nant * (c->nant - 1) / 2 : 0; }
+
+size_t fxc_vis_count(const fxc_config* c)
+{
+    if (!c) return 0;
+    return (size_t)c->nsubband * (fxc_num_baselines(c) + c->nant) * c->npol * c->npol * c->nchan;
+}
+
+const char* fxc_strerror(int s)
+{
+    switch (s) {
+    case FXC_OK: return "ok";
+    case FXC_ERR_INVALID: return "invalid configuration or argument";
+    case FXC_ERR_CUDA: return "CUDA runtime error";
+    case FXC_ERR_NOMEM: return "out of device or pinned host memory";
+    case FXC_ERR_UNSUPPORTED: return "not supported by this build";
+    case FXC_ERR_NODEVICE: return "no sm_100 CUDA device";
+    default: return "unknown status";
+    }
+}
+
+int fxc_last_cuda_error(void) { return g_last_cuda; }
+
+static int validate(const fxc_config* c)
+{
+    if (!c) return FXC_ERR_INVALID;
+    if (c->nant < 2 || c->npol < 1 || c->npol > 2 || c->numffts < 1 || c->nsubband < 1) return FXC_ERR_INVALID;
+    if (c->nchan < 128 || c->nchan > 4096 || (c->nchan & (c->nchan - 1))) return FXC_ERR_INVALID;
+    if (c->nbit != 2 || c->iscomplex != 0) return FXC_ERR_UNSUPPORTED;
+    if (!(c->bw > 0.0) || !std::isfinite(c->lo) || !std::isfinite(c->sb_spacing)) return FXC_ERR_INVALID;
+    if (c->xmode != FXC_X_PLAIN_FP32 && c->xmode != FXC_X_TC_FP16) return FXC_ERR_INVALID;
+    if (c->chunk_ffts < 0 || c->chunk_ffts % 64) return FXC_ERR_INVALID;
+    if ((long long)(c->numffts + 1) * 2 * c->nchan > 0x7fffffffLL) return FXC_ERR_INVALID;  // int sample offsets
+    if (c->xmode == FXC_X_TC_FP16) return FXC_ERR_UNSUPPORTED;
+    if (c->nant * c->npol > 64) return FXC_ERR_UNSUPPORTED;
+    return FXC_OK;
+}
+
+static void free_ctx(fxc_ctx* x)
+{
+    if (!x) return;
+    cudaFree(x->d_in);
+    cudaFree(x->d_delays);
+    cudaFree(x->d_offs);
+    cudaFree(x->d_sblo);
+    cudaFree(x->d_chan_sub);
+    cudaFree(x->d_chan_step);
+    cudaFree(x->d_dtab);
+    cudaFree(x->d_vbits);
+    cudaFree(x->d_spec);
+    cudaFree(x->d_acc);
+    cudaFree(x->d_counts);
+    cudaFree(x->d_vis);
+    for (auto& p : x->pending) {
+        cudaEventDestroy(p.a);
+        cudaEventDestroy(p.b);
+    }
+    for (auto e : x->event_pool) cudaEventDestroy(e);
+    if (x->own_stream) cudaStreamDestroy(x->own_stream);
+    delete x;
+}
+
+int fxc_create(const fxc_config* cfg, fxc_ctx** out)
+{
+    if (!out) return FXC_ERR_INVALID;
+    *out = nullptr;
+    int st = validate(cfg);
+    if (st != FXC_OK) return st;
+    int dev = 0;
+    FXC_CK(cudaGetDevice(&dev));
+    cudaDeviceProp prop;
+    FXC_CK(cudaGetDeviceProperties(&prop, dev));
+    if (prop.major != 10) return FXC_ERR_NODEVICE;
+
+    fxc_ctx* x = new fxc_ctx();
+    x->cfg = *cfg;
+    x->device = dev;
+    const fxc_config& c = x->cfg;
+    x->F = 2 * c.nchan;
+    x->nsig = c.nant * c.npol;
+    x->npair = x->nsig * (x->nsig + 1) / 2;
+    x->npair_ant = c.nant * (c.nant + 1) / 2;
+    x->nbl = c.nant * (c.nant - 1) / 2;
+    x->nout = x->nbl + c.nant;
+    x->ld = (int)round_up((size_t)c.numffts, 128);
+    x->subint = fxc_subint_bytes(cfg);
+    x->pitch = round_up(x->subint + 16, 256);
+    x->rows = (int)round_up((size_t)2 * x->nsig, 128);
+
+    // chunk length: spectra buffer <= ~1 GiB
+    const size_t per_slot = (size_t)c.nsubband * x->nsig * c.nchan * sizeof(float2);
+    size_t T = c.chunk_ffts;
+    if (T == 0) {
+        T = ((size_t)1 << 30) / per_slot;
+        T = T / 64 * 64;
+        if (T < 64) T = 64;
+        if (T > 4096) T = 4096;
+    }
+    T = std::min(T, round_up((size_t)c.numffts, 64));
+    x->T = (int)T;
+    x->spec_bytes = per_slot * T;
+
+    auto fail = [&](cudaError_t e) {
+        g_last_cuda = (int)e;
+        free_ctx(x);
+        return e == cudaErrorMemoryAllocation ? FXC_ERR_NOMEM : FXC_ERR_CUDA;
+    };
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&x->own_stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e);
+    x->stream = x->own_stream;
+    const size_t in_bytes = (size_t)c.nsubband * c.nant * x->pitch;
+    x->acc_bytes = (size_t)c.nsubband * x->npair * c.nchan * sizeof(float2);
+    x->vis_bytes = fxc_vis_count(cfg) * sizeof(float2);
+    const int stride = 1 << ((int)std::log2((double)c.nchan) / 2);
+    if ((e = cudaMalloc(&x->d_in, in_bytes)) != cudaSuccess) return fail(e);
+    if ((e = cudaMemset(x->d_in, 0, in_bytes)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&x->d_delays, 3 * sizeof(double) * c.nant)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&x->d_offs, sizeof(double) * c.nant)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&x->d_sblo, sizeof(double) * c.nsubband)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&x->d_chan_sub, sizeof(float) * stride)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&x->d_chan_step, sizeof(float) * (c.nchan / stride))) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&x->d_dtab, sizeof(DelayEntry) * (size_t)c.nant * x->ld)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&x->d_vbits, sizeof(uint32_t) * (size_t)c.nant * (x->ld / 32))) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&x->d_spec, x->spec_bytes)) != cudaSuccess) return fail(e);
+    if ((e = cudaMemset(x->d_spec, 0, x->spec_bytes)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&x->d_acc, x->acc_bytes)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&x->d_counts, sizeof(int) * x->npair_ant)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&x->d_vis, x->vis_bytes)) != cudaSuccess) return fail(e);
+
+    // constant tables: per-subband LO, f32 channel angular frequencies (kernel.c:162-166)
+    std::vector<double> sblo(c.nsubband);
+    for (int s = 0; s < c.nsubband; s++) sblo[s] = c.lo + c.sb_spacing * s;
+    std::vector<float> csub(stride), cstep(c.nchan / stride);
+    const double two_pi = 2 * 3.14159265358979323846;
+    for (int j = 0; j < stride; j++) csub[j] = (float)((two_pi * j * c.bw) / (double)c.nchan);
+    for (int i = 0; i < c.nchan / stride; i++) cstep[i] = (float)((two_pi * i * stride * c.bw) / (double)c.nchan);
+    if ((e = cudaMemcpy(x->d_sblo, sblo.data(), sizeof(double) * c.nsubband, cudaMemcpyHostToDevice)) != cudaSuccess)
+        return fail(e);
+    if ((e = cudaMemcpy(x->d_chan_sub, csub.data(), sizeof(float) * stride, cudaMemcpyHostToDevice)) != cudaSuccess)
+        return fail(e);
+    if ((e = cudaMemcpy(x->d_chan_step, cstep.data(), sizeof(float) * cstep.size(), cudaMemcpyHostToDevice)) !=
+        cudaSuccess)
+        return fail(e);
+    if ((e = cudaMemset(x->d_acc, 0, x->acc_bytes)) != cudaSuccess) return fail(e);
+    if ((e = cudaMemset(x->d_counts, 0, sizeof(int) * x->npair_ant)) != cudaSuccess) return fail(e);
+    *out = x;
+    return FXC_OK;
+}
+
+void fxc_destroy(fxc_ctx* x)
+{
+    if (!x) return;
+    cudaSetDevice(x->device);
+    if (x->stream) cudaStreamSynchronize(x->stream);
+    free_ctx(x);
+}
+
+int fxc_reset(fxc_ctx* x)
+{
+    if (!x) return FXC_ERR_INVALID;
+    FXC_CK(cudaSetDevice(x->device));
+    FXC_CK(cudaMemsetAsync(x->d_acc, 0, x->acc_bytes, x->stream));
+    FXC_CK(cudaMemsetAsync(x->d_counts, 0, sizeof(int) * x->npair_ant, x->stream));
+    return FXC_OK;
+}
+
+int fxc_set_stream(fxc_ctx* x, void* s)
+{
+    if (!x) return FXC_ERR_INVALID;
+    x->stream = s ? (cudaStream_t)s : x->own_stream;
+    return FXC_OK;
+}
+
+int fxc_synchronize(fxc_ctx* x)
+{
+    if (!x) return FXC_ERR_INVALID;
+    FXC_CK(cudaSetDevice(x->device));
+    FXC_CK(cudaStreamSynchronize(x->stream));
+    return FXC_OK;
+}
+
+int fxc_device_input(fxc_ctx* x, uint8_t** d, size_t* pitch)
+{
+    if (!x || !d || !pitch) return FXC_ERR_INVALID;
+    *d = x->d_in;
+    *pitch = x->pitch;
+    return FXC_OK;
+}
+
+int fxc_host_alloc(void** p, size_t bytes)
+{
+    if (!p) return FXC_ERR_INVALID;
+    FXC_CK(cudaHostAlloc(p, bytes, cudaHostAllocDefault));
+    return FXC_OK;
+}
+
+int fxc_host_free(void* p)
+{
+    FXC_CK(cudaFreeHost(p));
+    return FXC_OK;
+}
+
+// delays / offsets to the device, then K0 over FFTs first..first+nfft-1
+static int run_delay_table(fxc_ctx* x, const double* delays, const double* offs, int first, int nfft, int* ld_out)
+{
+    const fxc_config& c = x->cfg;
+    if (!delays || !offs || first < 0 || nfft < 1 || (long long)first + nfft > c.numffts) return FXC_ERR_INVALID;
+    for (int a = 0; a < 3 * c.nant; a++)
+        if (!std::isfinite(delays[a])) return FXC_ERR_INVALID;
+    for (int a = 0; a < c.nant; a++)
+        if (!std::isfinite(offs[a])) return FXC_ERR_INVALID;
+    FXC_CK(cudaMemcpyAsync(x->d_delays, delays, 3 * sizeof(double) * c.nant, cudaMemcpyHostToDevice, x->stream));
+    FXC_CK(cudaMemcpyAsync(x->d_offs, offs, sizeof(double) * c.nant, cudaMemcpyHostToDevice, x->stream));
+    const int ld = (int)round_up((size_t)nfft, 128);
+    const int maxoffset = (c.numffts - 1) * x->F;  // kernel.c:730
+    const double sampletime = 1.0 / (2.0 * c.bw);  // kernel.c:14
+    FXC_CK(launch_delay_table(x->d_delays, x->d_offs, nullptr, first, c.nant, nfft, ld, x->F, maxoffset, sampletime,
+                              x->d_dtab, x->d_vbits, x->stream));
+    *ld_out = ld;
+    return FXC_OK;
+}
+
+static FArgs make_fargs(fxc_ctx* x, const uint8_t* d_data, size_t pitch, int ld)
+{
+    FArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.data = d_data;
+    a.pitch = pitch;
+    a.dtab = x->d_dtab;
+    a.ld = ld;
+    a.nant = x->cfg.nant;
+    a.npol = x->cfg.npol;
+    a.nsb = x->cfg.nsubband;
+    a.sb_lo = x->d_sblo;
+    a.chan_sub = x->d_chan_sub;
+    a.chan_step = x->d_chan_step;
+    a.spec = x->d_spec;
+    a.rows = x->rows;
+    a.T = x->T;
+    return a;
+}
+
+int fxc_process_device(fxc_ctx* x, const uint8_t* d_data, size_t pitch, const double* delays,
+                       const double* offs, int first, int nfft)
+{
+    if (!x || !d_data || pitch < x->subint + 16 || pitch % 16 || ((uintptr_t)d_data & 15)) return FXC_ERR_INVALID;
+    FXC_CK(cudaSetDevice(x->device));
+    int ld = 0;
+    {
+        StageScope sc(x, 0, 2);
+        int st = run_delay_table(x, delays, offs, first, nfft, &ld);
+        if (st != FXC_OK) return st;
+        FXC_CK(launch_counts(x->d_vbits, x->cfg.nant, ld / 32, x->d_counts, x->stream));
+    }
+    FArgs fa = make_fargs(x, d_data, pitch, ld);
+    XArgs xa;
+    xa.spec = x->d_spec;
+    xa.acc = x->d_acc;
+    xa.nsig = x->nsig;
+    xa.T = x->T;
+    xa.nchan = x->cfg.nchan;
+    xa.nsb = x->cfg.nsubband;
+    xa.rows = x->rows;
+    for (int c0 = 0; c0 < nfft; c0 += x->T) {
+        fa.t_base = c0;
+        fa.nfft = std::min(x->T, nfft - c0);
+        {
+            StageScope sc(x, 1, 1);
+            FXC_CK(launch_fstage(x->cfg.nchan, kSpecF32, fa, x->stream));
+        }
+        {
+            StageScope sc(x, 2, 1);
+            FXC_CK(launch_xplain(xa, x->stream));
+        }
+    }
+    return FXC_OK;
+}
+
+int fxc_upload_input(fxc_ctx* x, const uint8_t* const* data)
+{
+    if (!x || !data) return FXC_ERR_INVALID;
+    FXC_CK(cudaSetDevice(x->device));
+    const fxc_config& c = x->cfg;
+    for (int r = 0; r < c.nsubband * c.nant; r++)
+        if (!data[r]) return FXC_ERR_INVALID;
+    for (int r = 0; r < c.nsubband * c.nant; r++)
+        FXC_CK(cudaMemcpyAsync(x->d_in + (size_t)r * x->pitch, data[r], x->subint, cudaMemcpyHostToDevice,
+                               x->stream));
+    return FXC_OK;
+}
+
+int fxc_process_host(fxc_ctx* x, const uint8_t* const* data, const double* delays, const double* offs, int first,
+                     int nfft)
+{
+    const int st = fxc_upload_input(x, data);
+    if (st != FXC_OK) return st;
+    return fxc_process_device(x, x->d_in, x->pitch, delays, offs, first, nfft);
+}
+
+static void counts_out(fxc_ctx* x, const std::vector<int>& pc, int* counts)
+{
+    const int A = x->cfg.nant;
+    int b = 0;
+    auto pidx = [A](int a1, int a2) { return a1 * A - (a1 * (a1 - 1)) / 2 + (a2 - a1); };
+    for (int a1 = 0; a1 < A - 1; a1++)
+        for (int a2 = a1 + 1; a2 < A; a2++) counts[b++] = pc[pidx(a1, a2)];
+    for (int a = 0; a < A; a++) counts[b++] = pc[pidx(a, a)];
+}
+
+int fxc_get_visibilities_device(fxc_ctx* x, float* d_vis, int normalize)
+{
+    if (!x || !d_vis) return FXC_ERR_INVALID;
+    FXC_CK(cudaSetDevice(x->device));
+    const fxc_config& c = x->cfg;
+    StageScope sc(x, 3, 1);
+    FXC_CK(launch_finalize(x->d_acc, 0, x->nsig, c.npol, c.nant, c.nchan, c.nsubband, x->d_counts, normalize,
+                           reinterpret_cast<float2*>(d_vis), x->stream));
+    return FXC_OK;
+}
+
+int fxc_get_visibilities(fxc_ctx* x, float* vis, int* counts, int normalize)
+{
+    if (!x || !vis) return FXC_ERR_INVALID;
+    int st = fxc_get_visibilities_device(x, reinterpret_cast<float*>(x->d_vis), normalize);
+    if (st != FXC_OK) return st;
+    FXC_CK(cudaMemcpyAsync(vis, x->d_vis, x->vis_bytes, cudaMemcpyDeviceToHost, x->stream));
+    std::vector<int> pc(x->npair_ant);
+    FXC_CK(cudaMemcpyAsync(pc.data(), x->d_counts, sizeof(int) * x->npair_ant, cudaMemcpyDeviceToHost, x->stream));
+    FXC_CK(cudaStreamSynchronize(x->stream));
+    if (counts) counts_out(x, pc, counts);
+    return FXC_OK;
+}
+
+int fxc_enable_stage_timing(fxc_ctx* x, int enable)
+{
+    if (!x) return FXC_ERR_INVALID;
+    x->timing = enable != 0;
+    return FXC_OK;
+}
+
+int fxc_stage_times(fxc_ctx* x, double* ms, long long* launches, int reset)
+{
+    if (!x) return FXC_ERR_INVALID;
+    FXC_CK(cudaSetDevice(x->device));
+    FXC_CK(cudaStreamSynchronize(x->stream));
+    for (auto& p : x->pending) {
+        float t = 0.f;
+        FXC_CK(cudaEventElapsedTime(&t, p.a, p.b));
+        x->stage_ms[p.stage] += t;
+        x->event_pool.push_back(p.a);
+        x->event_pool.push_back(p.b);
+    }
+    x->pending.clear();
+    for (int s = 0; s < FXC_NSTAGE; s++) {
+        if (ms) ms[s] = x->stage_ms[s];
+        if (launches) launches[s] = x->stage_launches[s];
+        if (reset) {
+            x->stage_ms[s] = 0;
+            x->stage_launches[s] = 0;
+        }
+    }
+    return FXC_OK;
+}
+
+int fxc_debug_delay_table(fxc_ctx* x, const double* delays, const double* offs, int first, int nfft, int* offsets,
+                          int* valid, double* frac, double* a, double* b)
+{
+    if (!x) return FXC_ERR_INVALID;
+    FXC_CK(cudaSetDevice(x->device));
+    int ld = 0;
+    int st = run_delay_table(x, delays, offs, first, nfft, &ld);
+    if (st != FXC_OK) return st;
+    const int A = x->cfg.nant;
+    std::vector<DelayEntry> h((size_t)A * ld);
+    FXC_CK(cudaMemcpyAsync(h.data(), x->d_dtab, sizeof(DelayEntry) * h.size(), cudaMemcpyDeviceToHost, x->stream));
+    FXC_CK(cudaStreamSynchronize(x->stream));
+    for (int an = 0; an < A; an++)
+        for (int t = 0; t < nfft; t++) {
+            const DelayEntry& e = h[(size_t)an * ld + t];
+            const size_t o = (size_t)an * nfft + t;
+            if (offsets) offsets[o] = e.offset;
+            if (valid) valid[o] = e.valid;
+            if (frac) frac[o] = e.frac;
+            if (a) a[o] = e.a;
+            if (b) b[o] = e.b;
+        }
+    return FXC_OK;
+}
+
+int fxc_debug_unpack(fxc_ctx* x, const double* delays, const double* offs, int first, int nfft, float* out)
+{
+    if (!x || !out) return FXC_ERR_INVALID;
+    FXC_CK(cudaSetDevice(x->device));
+    int ld = 0;
+    int st = run_delay_table(x, delays, offs, first, nfft, &ld);
+    if (st != FXC_OK) return st;
+    const fxc_config& c = x->cfg;
+    const size_t n = (size_t)c.nsubband * c.nant * c.npol * nfft * x->F;
+    float* d = nullptr;
+    FXC_CK(cudaMalloc(&d, n * sizeof(float)));
+    FArgs fa = make_fargs(x, x->d_in, x->pitch, ld);
+    fa.t_base = 0;
+    fa.nfft = nfft;
+    cudaError_t e = launch_unpack_debug(c.nchan, fa, d, x->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, n * sizeof(float), cudaMemcpyDeviceToHost, x->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(x->stream);
+    cudaFree(d);
+    FXC_CK(e);
+    return FXC_OK;
+}
+
+int fxc_debug_spectra(fxc_ctx* x, const double* delays, const double* offs, int first, int nfft, float* out)
+{
+    if (!x || !out || nfft > x->T) return FXC_ERR_INVALID;
+    FXC_CK(cudaSetDevice(x->device));
+    int ld = 0;
+    int st = run_delay_table(x, delays, offs, first, nfft, &ld);
+    if (st != FXC_OK) return st;
+    const fxc_config& c = x->cfg;
+    const int T = (int)round_up((size_t)nfft, 64);
+    const size_t n = (size_t)c.nsubband * x->nsig * T * c.nchan;
+    float2* d = nullptr;
+    FXC_CK(cudaMalloc(&d, n * sizeof(float2)));
+    FArgs fa = make_fargs(x, x->d_in, x->pitch, ld);
+    fa.t_base = 0;
+    fa.nfft = nfft;
+    fa.T = T;
+    fa.spec = d;
+    cudaError_t e = launch_fstage(c.nchan, kSpecF32, fa, x->stream);
+    for (int r = 0; e == cudaSuccess && r < c.nsubband * x->nsig; r++)
+        e = cudaMemcpyAsync(out + (size_t)r * nfft * c.nchan * 2, d + (size_t)r * T * c.nchan,
+                            sizeof(float2) * nfft * c.nchan, cudaMemcpyDeviceToHost, x->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(x->stream);
+    cudaFree(d);
+    FXC_CK(e);
+    return FXC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,59 @@
+// fx_internal.h -- layouts and launch arguments shared by the host driver and
+// the sm_100a kernels of the FX correlator hot path.
+//
+// Device memory layout (one process call, per subintegration):
+//   packed input   u8   [nsb][nant][pitch]        pitch >= subintbytes + 16, 16-B multiple
+//   delay table    DelayEntry [nant][ld]           one entry per (antenna, FFT of the call)
+//   valid bits     u32  [nant][ld/32]              bit t = antenna valid for FFT t
+//   spectra (F32)  f32x2 [nsb][nsig][T][nchan]     plain X stage input, channel-contiguous
+//   spectra (F16)  f16  [nsb][nchan][rows][T]      tensor-core X stage input, K(=time)-major;
+//                                                  row 2*sig = Re, 2*sig+1 = Im, rows padded
+//   accumulators   f32x2 [nsb][npair][nchan]       plain form, pair = upper-triangle (i<=j)
+//                  f32x2 [nsb][nchan][npair]       tensor-core form
+//   counts         i32  [npair_ant]                antenna pairs (a1<=a2) incl. autos
+// sig = ant*npol + pol; npair = nsig*(nsig+1)/2 in row-major upper-triangle order.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+namespace fx {
+
+constexpr float kHiMag = 3.3359f;                        // kernel.c:191
+constexpr double kNeg2Pi = -2.0 * 3.14159265358979323846;  // -TWO_PI (vectordefs.h:4)
+
+struct DelayEntry {
+    double a;       // delay change across the FFT, seconds (kernel.c:383)
+    double b;       // delay at the FFT start, seconds (kernel.c:384)
+    double frac;    // fractional-sample delay, seconds (kernel.c:739-751)
+    int offset;     // integer sample offset of the FFT in the antenna stream
+    int valid;      // 0/1 (kernel.c:752-756)
+};
+
+enum SpecMode { kSpecF32 = 0, kSpecF16 = 1 };
+
+// Arguments of the fused F-stage kernel (passed by value).
+struct FArgs {
+    const uint8_t* data;        // packed input [nsb][nant][pitch]
+    size_t pitch;
+    const DelayEntry* dtab;     // [nant][ld]
+    int ld;                     // leading dimension of dtab (FFTs of the call, padded)
+    int t_base;                 // dtab column of the chunk's first FFT
+    int nfft;                   // FFTs of the chunk that carry data
+    int T;                      // FFT slots in the spectra buffer (>= nfft; extra slots zero)
+    int nant, npol, nsb;
+    const double* sb_lo;        // [nsb] LO per subband, Hz (device)
+    const float* chan_sub;      // [stride]     (f32)(2 pi j bw / nchan)       kernel.c:164
+    const float* chan_step;     // [nchan/stride] (f32)(2 pi i stride bw / nchan) kernel.c:165
+    void* spec;                 // spectra buffer (layout per SpecMode)
+    int rows;                   // F16 layout: rows per channel (>= 2*nsig)
+};
+
+struct XArgs {
+    const void* spec;
+    void* acc;
+    int nsig, T, nchan, nsb;
+    int rows;
+};
+
+}  // namespace fx

@@ -1,0 +1,21 @@
+// fx_kernels.h -- host-side launchers of the sm_100a kernels (internal).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "fx_internal.h"
+
+namespace fx {
+
+cudaError_t launch_delay_table(const double* delays, const double* fileoffsets, const int* fftindex, int first,
+                               int nant, int nfft, int ld, int F, int maxoffset, double sampletime, DelayEntry* tab,
+                               uint32_t* vbits, cudaStream_t st);
+cudaError_t launch_counts(const uint32_t* vbits, int nant, int nwords, int* counts, cudaStream_t st);
+cudaError_t launch_finalize(const float2* acc, int acc_layout, int nsig, int npol, int nant, int nchan, int nsb,
+                            const int* counts, int normalize, float2* vis, cudaStream_t st);
+cudaError_t launch_fstage(int nchan, int mode, const FArgs& a, cudaStream_t st);
+size_t fstage_smem_bytes(int nchan, int mode, int npol);
+cudaError_t launch_xplain(const XArgs& a, cudaStream_t st);
+cudaError_t launch_unpack_debug(int nchan, const FArgs& a, float* out, cudaStream_t st);
+
+}  // namespace fx

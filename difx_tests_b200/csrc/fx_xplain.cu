@@ -1,0 +1,174 @@
+// fx_xplain.cu -- plain FP32 X stage (baseline cross-multiply-accumulate).
+//
+// For every channel c and signal pair i <= j:
+//     acc[sb][pair(i,j)][c] += sum_t X[sb][i][t][c] * conj(X[sb][j][t][c])
+// which is kernel.c:829-854 (ippsAddProduct of channelised[j] and the conjugated
+// channelised[k]) generalised to all signal pairs incl. autos; the conjugation
+// of kernel.c:557-568 is folded into the multiply.
+//
+// Register tiling: each thread owns an 8x8 block of signal pairs for one
+// channel (64 complex FP32 accumulators, 256 FFMA per time sample).  A CTA
+// covers CG channels x every upper-triangle 8x8 tile, so each spectrum value is
+// read from HBM/L2 once.  Time blocks of TK samples are double-buffered in
+// shared memory with cp.async; lanes of a warp are (CG channels) x (32/CG
+// tiles), so the operand loads are broadcasts or conflict-free.
+#include "fx_common.cuh"
+#include "fx_kernels.h"
+
+namespace fx {
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+template <int NB, int CG, int TK>
+struct XPlan {
+    static constexpr int NTILE = NB * (NB + 1) / 2;
+    static constexpr int NTHREADS = CG * NTILE;
+    static constexpr int NS = NB * 8;                       // staged signals
+    // element (s, tk, cl) at s*TK*CG + (s/8)*8 + tk*CG + cl  (64-byte skew per 8-signal block)
+    static constexpr int STAGE = NS * TK * CG + NB * 8;     // float2 per buffer
+};
+
+template <int NB, int CG, int TK>
+__device__ __forceinline__ int xoff(int s, int tk, int cl)
+{
+    return s * TK * CG + (s >> 3) * 8 + tk * CG + cl;
+}
+
+template <int NB, int CG, int TK>
+__global__ void __launch_bounds__(XPlan<NB, CG, TK>::NTHREADS, 1)
+k_xplain(XArgs a)
+{
+    using P = XPlan<NB, CG, TK>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    float2* xs = reinterpret_cast<float2*>(smem);   // [2][STAGE]
+
+    const int tid = threadIdx.x;
+    const int tile = tid / CG;
+    const int cl = tid - tile * CG;
+    int I = 0, rem = tile;
+    while (rem >= NB - I) {
+        rem -= NB - I;
+        I++;
+    }
+    const int J = I + rem;
+
+    const int c0 = blockIdx.x * CG;
+    const int sb = blockIdx.y;
+    const int nsig = a.nsig;
+    const int C = a.nchan;
+    const float2* spec = reinterpret_cast<const float2*>(a.spec) + (size_t)sb * nsig * a.T * C;
+
+    // zero the padding signals once (both buffers)
+    for (int e = tid; e < 2 * P::STAGE; e += P::NTHREADS) xs[e] = make_float2(0.f, 0.f);
+    __syncthreads();
+
+    constexpr int VPR = CG / 2;                                    // 16-byte vectors per (s, tk) row
+    const int nvec = nsig * TK * VPR;
+    auto issue = [&](int buf, int t0) {
+        float2* dst = xs + buf * P::STAGE;
+        for (int v = tid; v < nvec; v += P::NTHREADS) {
+            const int s = v / (TK * VPR);
+            const int r = v - s * (TK * VPR);
+            const int tk = r / VPR;
+            const int q = r - tk * VPR;
+            const float2* src = spec + ((size_t)s * a.T + t0 + tk) * C + c0 + 2 * q;
+            cp_async16(dst + xoff<NB, CG, TK>(s, tk, 2 * q), src);
+        }
+        cp_async_commit();
+    };
+
+    float2 acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[i][j] = make_float2(0.f, 0.f);
+
+    const int nblk = a.T / TK;
+    issue(0, 0);
+    for (int blk = 0; blk < nblk; blk++) {
+        if (blk + 1 < nblk) {
+            issue((blk + 1) & 1, (blk + 1) * TK);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const float2* x = xs + (blk & 1) * P::STAGE;
+        for (int tk = 0; tk < TK; tk++) {
+            float2 xi[8];
+#pragma unroll
+            for (int ii = 0; ii < 8; ii++) xi[ii] = x[xoff<NB, CG, TK>(I * 8 + ii, tk, cl)];
+#pragma unroll
+            for (int jj = 0; jj < 8; jj++) {
+                const float2 xj = x[xoff<NB, CG, TK>(J * 8 + jj, tk, cl)];
+#pragma unroll
+                for (int ii = 0; ii < 8; ii++) {
+                    // acc += xi * conj(xj)
+                    acc[ii][jj].x = fmaf(xi[ii].x, xj.x, fmaf(xi[ii].y, xj.y, acc[ii][jj].x));
+                    acc[ii][jj].y = fmaf(xi[ii].y, xj.x, fmaf(-xi[ii].x, xj.y, acc[ii][jj].y));
+                }
+            }
+        }
+        __syncthreads();   // buffer (blk & 1) is refilled by the next issue
+    }
+
+    float2* out = reinterpret_cast<float2*>(a.acc);
+    const int npair = nsig * (nsig + 1) / 2;
+#pragma unroll
+    for (int ii = 0; ii < 8; ii++) {
+        const int i = I * 8 + ii;
+#pragma unroll
+        for (int jj = 0; jj < 8; jj++) {
+            const int j = J * 8 + jj;
+            if (i <= j && j < nsig) {
+                const int p = i * nsig - (i * (i - 1)) / 2 + (j - i);
+                float2* o = out + ((size_t)sb * npair + p) * C + c0 + cl;
+                float2 cur = *o;
+                cur.x += acc[ii][jj].x;
+                cur.y += acc[ii][jj].y;
+                *o = cur;
+            }
+        }
+    }
+}
+
+template <int NB, int CG, int TK>
+static cudaError_t launch_x(const XArgs& a, cudaStream_t st)
+{
+    using P = XPlan<NB, CG, TK>;
+    const size_t sm = 2 * (size_t)P::STAGE * sizeof(float2);
+    auto kern = k_xplain<NB, CG, TK>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    dim3 grid(a.nchan / CG, a.nsb);
+    kern<<<grid, P::NTHREADS, sm, st>>>(a);
+    return cudaGetLastError();
+}
+
+// Tile shape per signal count: NB = ceil(nsig/8) blocks of 8 signals; CG
+// channels per CTA chosen so a CTA has 96..512 threads.
+cudaError_t launch_xplain(const XArgs& a, cudaStream_t st)
+{
+    const int nb = (a.nsig + 7) / 8;
+    if (a.T % 16 != 0) return cudaErrorInvalidValue;  // T is a multiple of every TK
+    switch (nb) {
+    case 1: return a.nchan % 32 ? cudaErrorInvalidValue : launch_x<1, 32, 8>(a, st);
+    case 2: return a.nchan % 32 ? cudaErrorInvalidValue : launch_x<2, 32, 8>(a, st);
+    case 3: return a.nchan % 32 ? cudaErrorInvalidValue : launch_x<3, 32, 8>(a, st);
+    case 4: return a.nchan % 32 ? cudaErrorInvalidValue : launch_x<4, 32, 8>(a, st);
+    case 5: return a.nchan % 16 ? cudaErrorInvalidValue : launch_x<5, 16, 8>(a, st);
+    case 6: return a.nchan % 16 ? cudaErrorInvalidValue : launch_x<6, 16, 8>(a, st);
+    case 7: return a.nchan % 8 ? cudaErrorInvalidValue : launch_x<7, 8, 16>(a, st);
+    case 8: return a.nchan % 8 ? cudaErrorInvalidValue : launch_x<8, 8, 16>(a, st);
+    default: return cudaErrorNotSupported;
+    }
+}
+
+}  // namespace fx

@@ -1,0 +1,173 @@
+/*
+ * fxcorr.h -- C ABI of the B200 (sm_100a) FX correlator hot path.
+ *
+ * Drop-in for the per-subintegration processing of the reference CPU
+ * correlator (twiG56/difx_tests, kernel.c): 2-bit unpack, integer and
+ * fractional delay, fringe rotation, FFT, fractional-sample correction and
+ * baseline cross-multiply-accumulate, on one GPU.  Plain pointers and sizes
+ * only; every call returns an int status (FXC_OK or a negative FXC_ERR_*),
+ * never exits the process.  One context per host thread; contexts on the same
+ * device may run concurrently on different streams.
+ *
+ * Reference interfaces replaced (file:line in the reference):
+ *   init_FxKernel                   kernel.h:63-66, kernel.c:8-115   -> fxc_create
+ *   processAntennasAndBaselinePara  kernel.h:106-110, kernel.c:709-827
+ *                                                                    -> fxc_process_host / fxc_process_device
+ *   merge                           kernel.h:123, kernel.c:856-878   -> accumulation across calls (fxc_process_*)
+ *   processNormalize                kernel.h:95, kernel.c:348-359    -> fxc_get_visibilities(normalize = 1)
+ *   resetBeforeProcess              kernel.h:112, kernel.c:361-371   -> fxc_reset
+ *   allocDataHost (subintbytes)     allocDataHost.c:8-22             -> fxc_subint_bytes
+ * The exact reference symbols (init_FxKernel, processAntennasAndBaselinePara,
+ * merge, processNormalize, saveVisibilities, ...) are exported by the
+ * compatibility layer declared in fxkernel_compat.h.
+ */
+#ifndef FXCORR_H
+#define FXCORR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#define FXC_OK                0
+#define FXC_ERR_INVALID      -1   /* bad configuration or argument */
+#define FXC_ERR_CUDA         -2   /* CUDA runtime error (see fxc_last_cuda_error) */
+#define FXC_ERR_NOMEM        -3   /* device or pinned-host allocation failed */
+#define FXC_ERR_UNSUPPORTED  -4   /* valid request this build does not implement */
+#define FXC_ERR_NODEVICE     -5   /* no sm_100 CUDA device */
+
+/* X-stage arithmetic */
+#define FXC_X_PLAIN_FP32 0        /* FP32 CUDA-core cross-multiply-accumulate */
+#define FXC_X_TC_FP16    1        /* tcgen05 tensor cores, FP16 inputs, FP32 accumulation */
+
+typedef struct fxc_config {
+    int nant;          /* antennas, >= 2 */
+    int npol;          /* 1, or 2 = the reference's interleaved dual-polarisation format */
+    int nchan;         /* channels per subband: power of two in [128, 4096]; FFT length 2*nchan */
+    int nbit;          /* bits per sample: 2 (the reference's only unpacker, kernel.c:388-395) */
+    int iscomplex;     /* 0: real sampling (kernel.c:15) */
+    int numffts;       /* FFTs per subintegration; sets the maximum sample offset (kernel.c:730) */
+    int nsubband;      /* independent subbands sharing the antennas' delay model, >= 1 */
+    int xmode;         /* FXC_X_PLAIN_FP32 or FXC_X_TC_FP16 */
+    double lo;         /* LO (sky) frequency of subband 0, Hz; |lo| < 2^31 for reference-identical phases */
+    double bw;         /* bandwidth per subband, Hz; sampling interval 1/(2 bw) (kernel.c:14) */
+    double sb_spacing; /* LO step between consecutive subbands, Hz */
+    int chunk_ffts;    /* FFTs per F->X chunk (multiple of 64), 0 = chosen by the library */
+} fxc_config;
+
+typedef struct fxc_ctx fxc_ctx;
+
+/* Initialise a config with the reference's defaults (NPOL 2, NBIT 2, COMPLEX 0,
+ * main.c:29-31) and one subband. */
+void fxc_config_default(fxc_config* cfg);
+
+/* Bytes of one (subband, antenna) input stream for one subintegration:
+ * nchan * 2 * (numffts + 1) * nbit / 8 * npol (allocDataHost.c:21). */
+size_t fxc_subint_bytes(const fxc_config* cfg);
+
+/* Number of output baselines (A(A-1)/2 crosses in the reference's order, then
+ * A autocorrelations) and the size of one visibility set in complex values:
+ * nsubband * (nbl + nant) * npol^2 * nchan. */
+int fxc_num_baselines(const fxc_config* cfg);
+size_t fxc_vis_count(const fxc_config* cfg);
+
+/* Create a context on the current CUDA device: validates the config, allocates
+ * all device buffers, zeroes the accumulators. */
+int fxc_create(const fxc_config* cfg, fxc_ctx** out);
+void fxc_destroy(fxc_ctx* ctx);
+
+/* Zero visibilities and counts (resetBeforeProcess). */
+int fxc_reset(fxc_ctx* ctx);
+
+/* Process FFTs first_fft .. first_fft+nfft-1 (0 <= first_fft, first_fft+nfft <= numffts)
+ * and accumulate into the context's visibilities.  Calls accumulate, so time
+ * shards of one subintegration may be processed by successive calls (the
+ * reference's split/merge, main.c:398-433).
+ *   data[sb*nant + ant]  host pointer to the subintegration's packed bytes
+ *                        (fxc_subint_bytes each); pinned memory (fxc_host_alloc)
+ *                        transfers fastest
+ *   delays[3*ant + k]    (quad, lin, const) seconds, t in FFT units (kernel.c:378-380)
+ *   fileoffsets[ant]     seconds (kernel.c:736)
+ */
+int fxc_process_host(fxc_ctx* ctx, const uint8_t* const* data, const double* delays, const double* fileoffsets,
+                     int first_fft, int nfft);
+
+/* Same with the input already in device memory: d_data holds nsubband*nant rows
+ * of `pitch` bytes (pitch >= fxc_subint_bytes + 16, multiple of 16, 16-byte
+ * aligned base).  delays / fileoffsets are host arrays. */
+int fxc_process_device(fxc_ctx* ctx, const uint8_t* d_data, size_t pitch, const double* delays,
+                       const double* fileoffsets, int first_fft, int nfft);
+
+/* Copy one subintegration's host input rows (data[sb*nant + ant], fxc_subint_bytes
+ * each) into the context's device input buffer, asynchronously on its stream. */
+int fxc_upload_input(fxc_ctx* ctx, const uint8_t* const* data);
+
+/* The context's own device input buffer (rows of *pitch bytes) for callers
+ * that fill device memory themselves. */
+int fxc_device_input(fxc_ctx* ctx, uint8_t** d_data, size_t* pitch);
+
+/* Copy visibilities to the host: vis holds fxc_vis_count complex values as
+ * interleaved float pairs, layout [sb][bl][2*l + m][chan] with bl = crosses in
+ * the reference's order then autos; counts (nbl + nant ints, may be NULL) get
+ * the number of FFTs accumulated per baseline.  normalize != 0 divides each
+ * baseline by its count (processNormalize, kernel.c:348-359). */
+int fxc_get_visibilities(fxc_ctx* ctx, float* vis, int* counts, int normalize);
+
+/* Same into device memory (d_vis: fxc_vis_count complex values). */
+int fxc_get_visibilities_device(fxc_ctx* ctx, float* d_vis, int normalize);
+
+/* Stream used by the context (a cudaStream_t); NULL restores the context's own. */
+int fxc_set_stream(fxc_ctx* ctx, void* stream);
+int fxc_synchronize(fxc_ctx* ctx);
+
+/* Pinned host memory for input staging. */
+int fxc_host_alloc(void** p, size_t bytes);
+int fxc_host_free(void* p);
+
+/* Per-stage device timing (the counterpart of the reference's per-stage clock()
+ * timers, kernel.c:720-821).  With enable != 0 every launch is bracketed by CUDA
+ * events on the context's stream.  fxc_stage_times waits for the stream and
+ * returns accumulated milliseconds and launch counts per stage
+ * [0] delay table + counts, [1] F stage, [2] X stage, [3] finalise;
+ * reset != 0 clears the accumulators.  Launch counts are kept even when timing
+ * is disabled. */
+#define FXC_NSTAGE 4
+int fxc_enable_stage_timing(fxc_ctx* ctx, int enable);
+int fxc_stage_times(fxc_ctx* ctx, double* ms, long long* launches, int reset);
+
+const char* fxc_strerror(int status);
+/* Last CUDA error code seen by this thread's calls (cudaError_t as int). */
+int fxc_last_cuda_error(void);
+
+/* ---- inspection entry points (parity tests; not needed for correlation) ---- */
+
+/* Delay table of FFTs first_fft..first_fft+nfft-1 computed on the GPU
+ * (kernel.c:733-756): offsets / valid as int [nant][nfft], frac / a / b as
+ * double [nant][nfft] (any may be NULL). */
+int fxc_debug_delay_table(fxc_ctx* ctx, const double* delays, const double* fileoffsets, int first_fft, int nfft,
+                          int* offsets, int* valid, double* frac, double* a, double* b);
+
+/* Unpacked 2-bit samples (before fringe rotation) of the F stage for FFTs
+ * first_fft..+nfft-1 from the context's device input buffer:
+ * out float [nsb][nant][npol][nfft][2*nchan]; zero where an antenna is invalid. */
+int fxc_debug_unpack(fxc_ctx* ctx, const double* delays, const double* fileoffsets, int first_fft, int nfft,
+                     float* out);
+
+/* F-stage spectra (after fractional-sample correction) for FFTs
+ * first_fft..+nfft-1 (nfft <= chunk length) from the context's device input
+ * buffer: out interleaved complex float [nsb][nant*npol][nfft][nchan]. */
+int fxc_debug_spectra(fxc_ctx* ctx, const double* delays, const double* fileoffsets, int first_fft, int nfft,
+                      float* out);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+#ifdef __cplusplus
+}
+#endif
+#endif

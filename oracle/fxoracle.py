@@ -145,6 +145,7 @@ def fringe_rotator(a, b, lo, nchan, ref_args=True):
     reference's formula and is kept as is.
     """
     F, stride, S = geometry(nchan)
+    out_shape = np.broadcast(np.asarray(a), np.asarray(b)).shape + (F,)
     a = np.asarray(a, np.float64)[..., None]
     b = np.asarray(b, np.float64)[..., None]
     intdelay = np.trunc(b)
@@ -163,7 +164,7 @@ def fringe_rotator(a, b, lo, nchan, ref_args=True):
     sub = np.exp(1j * subarg)            # [..., S]
     step = np.exp(1j * steparg)          # [..., stride]
     rot = step[..., :, None] * sub[..., None, :]   # [..., stride, S]
-    return rot.reshape(rot.shape[:-2] + (F,))
+    return rot.reshape(out_shape)
 
 
 def channel_freq_tables(bw, nchan):
@@ -188,6 +189,7 @@ def frac_rotator(frac, bw, nchan, ref_args=True):
     """
     _, stride, _ = geometry(nchan)
     sub, step = channel_freq_tables(bw, nchan)
+    out_shape = np.shape(frac) + (nchan,)
     frac = np.asarray(frac, np.float64)[..., None]
     if ref_args:
         f32 = frac.astype(np.float32)
@@ -197,7 +199,7 @@ def frac_rotator(frac, bw, nchan, ref_args=True):
         subarg = sub.astype(np.float64) * frac
         steparg = step.astype(np.float64) * frac
     rot = np.exp(1j * steparg)[..., :, None] * np.exp(1j * subarg)[..., None, :]
-    return rot.reshape(rot.shape[:-2] + (nchan,))
+    return rot.reshape(out_shape)
 
 
 def channelise(data, delays, fileoffsets, bw, lo, nchan, npol, fftindex, maxoffset_ffts,

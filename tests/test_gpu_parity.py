@@ -1,0 +1,194 @@
+"""GPU parity: the CUDA path (through the C ABI) against the oracle.
+
+Bars: integer/bit work (delay table, unpacked samples) bit-exact; FP32 spectra
+and plain-form visibilities within 1e-5 relative (max|d| / max|ref| per spectrum)
+of the reference kernel.c outputs (golden fixtures) and of the FP64 oracle.
+"""
+import numpy as np
+import pytest
+
+import difx_tests_b200 as fx
+from difx_tests_b200 import synth
+from oracle import fxoracle as fo
+from oracle import refcall
+
+pytestmark = pytest.mark.gpu
+
+VIS_TOL = 1e-5       # plain FP32 form vs reference / FP64 oracle, relative to max|V| per spectrum
+SPEC_TOL = 2e-5      # FP32 F stage vs FP64 oracle, relative to max|X| per spectrum
+
+
+def corr_for(job, **kw):
+    cfg = fx.make_config(job.nant, job.nchan, job.numffts, job.bw, job.lo, npol=job.npol, nsubband=job.nsubband,
+                         sb_spacing=(job.sb_lo[1] - job.sb_lo[0]) if job.nsubband > 1 else job.bw, **kw)
+    return fx.Correlator(cfg)
+
+
+def oracle_vis(job, sb=0, fftindex=None):
+    lo = float(job.sb_lo[sb])
+    return fo.correlate(job.data[sb], job.delays, job.fileoffsets, job.bw, lo, job.nchan, job.npol,
+                        fftindex=fftindex, numffts=job.numffts, maxoffset_ffts=job.numffts)
+
+
+def assert_vis_close(got, ref, tol=VIS_TOL):
+    mx, rms = fo.vis_error(got, ref)
+    assert mx.max() < tol, f"max rel err {mx.max():.3e} (rms {rms.max():.3e})"
+
+
+def test_delay_table_bit_exact_vs_reference(golden):
+    g = golden("delay_table")
+    nant = g["delays"].shape[0]
+    nf = int(g["numffts"])
+    cfg = fx.make_config(nant, int(g["nchan"]), nf, float(g["bw"]), 1.4e9, npol=2)
+    with fx.Correlator(cfg) as c:
+        tab = c.delay_table(g["delays"], g["fileoffsets"], 0, nf)
+    np.testing.assert_array_equal(tab["valid"], g["valid"].astype(bool))
+    v = tab["valid"]
+    np.testing.assert_array_equal(tab["offset"][v], g["offset"][v])
+    assert np.array_equal(tab["frac"][v].view(np.int64), g["frac"][v].view(np.int64))
+    assert np.array_equal(tab["a"].view(np.int64), g["a"].view(np.int64))
+    assert np.array_equal(tab["b"].view(np.int64), g["b"].view(np.int64))
+
+
+@pytest.mark.parametrize("nchan,first", [(256, 0), (2048, 17), (4096, 5)])
+def test_delay_table_bit_exact_vs_oracle(nchan, first):
+    job = synth.random_job(nant=9, npol=1, nchan=nchan, numffts=300, bw=64e6, seed=nchan)
+    job.delays[2, 1] *= 400  # fast drift: invalid FFTs at one end
+    job.fileoffsets[3] += 0.6 / (2 * job.bw)
+    nf = 200
+    with corr_for(job) as c:
+        tab = c.delay_table(job.delays, job.fileoffsets, first, nf)
+    ref = fo.delay_table(job.delays, job.fileoffsets, job.bw, nchan, np.arange(first, first + nf), job.numffts)
+    np.testing.assert_array_equal(tab["valid"], ref["valid"])
+    v = ref["valid"]
+    assert (~v).any()
+    np.testing.assert_array_equal(tab["offset"][v], ref["offset"][v])
+    assert np.array_equal(tab["frac"][v].view(np.int64), ref["frac"][v].view(np.int64))
+
+
+@pytest.mark.parametrize("npol", [1, 2])
+@pytest.mark.parametrize("nchan", [128, 256, 1024, 4096])
+def test_unpack_bit_exact(npol, nchan):
+    job = synth.random_job(nant=3, npol=npol, nchan=nchan, numffts=20, bw=32e6, seed=npol * 7 + nchan)
+    job.fileoffsets[1] += 1.0 / (2 * job.bw)      # odd offsets
+    job.fileoffsets[2] += 3.0 / (2 * job.bw)
+    with corr_for(job) as c:
+        got = c.unpacked(job.data, job.delays, job.fileoffsets, 0, job.numffts)[0]   # [ant][pol][t][F]
+    tab = fo.delay_table(job.delays, job.fileoffsets, job.bw, nchan, np.arange(job.numffts), job.numffts)
+    F = 2 * nchan
+    for a in range(job.nant):
+        v = tab["valid"][a]
+        ref = fo.unpack(job.data[0, a], tab["offset"][a][v], F, npol)    # [P][n][F]
+        np.testing.assert_array_equal(got[a][:, v, :], ref)
+        assert np.all(got[a][:, ~v, :] == 0)
+
+
+def test_unpack_matches_reference_golden(golden):
+    g = golden("unpack")
+    nchan = int(g["nchan"])
+    F = 2 * nchan
+    # drive the F stage's decoder with offsets from a constant-delay model: one antenna per golden offset
+    offs = g["offsets"]
+    nant = len(offs)
+    bw = 32e6
+    Ts = 1.0 / (2 * bw)
+    numffts = 16                                   # subint_bytes = 4352 >= len(data)
+    cfg = fx.make_config(nant, nchan, numffts, bw, 1.4e9, npol=2)
+    delays = np.zeros((nant, 3))
+    # nf = -(o + 1)  ->  n = (int)(nf + 0.5) = -o (truncation toward zero)  ->  offset(k=0) = o
+    fileoffsets = np.array([(o + 1.0) * Ts for o in offs])
+    data = np.zeros((1, nant, fx.lib().fxc_subint_bytes(cfg)), np.uint8)
+    data[0, :, : len(g["data"])] = g["data"][None, :]
+    with fx.Correlator(cfg) as c:
+        got = c.unpacked(data, delays, fileoffsets, 0, 1)[0][:, :, 0, :]   # [ant][pol][F]
+    np.testing.assert_array_equal(got, g["unpacked"])
+
+
+@pytest.mark.parametrize("npol", [1, 2])
+@pytest.mark.parametrize("nchan", [128, 256, 512, 1024, 2048, 4096])
+def test_spectra_vs_fp64(npol, nchan):
+    nf = 24
+    job = synth.random_job(nant=2, npol=npol, nchan=nchan, numffts=nf, bw=64e6, lo=1.4e9 + 0.3, seed=nchan + npol)
+    with corr_for(job) as c:
+        got = c.spectra(job.data, job.delays, job.fileoffsets, 0, nf)[0]         # [sig][t][C]
+    spec, tab = fo.channelise(job.data[0], job.delays, job.fileoffsets, job.bw, job.lo, nchan, npol,
+                              np.arange(nf), nf)
+    ref = spec.reshape(job.nant * npol, nf, nchan)
+    err = np.abs(got - ref).max(axis=-1) / np.maximum(np.abs(ref).max(axis=-1), 1e-30)
+    valid = np.repeat(tab["valid"], npol, axis=0)
+    assert err[valid].max() < SPEC_TOL, err[valid].max()
+    assert np.all(got[~valid] == 0)
+
+
+@pytest.mark.parametrize("name", ["e2e_c256", "e2e_c1024_split2", "e2e_c256_fraclo"])
+def test_vis_vs_reference_golden(golden, name):
+    g = golden(name)
+    nchan, numffts = int(g["nchan"]), int(g["numffts"])
+    nant = g["data"].shape[0]
+    cfg = fx.make_config(nant, nchan, numffts, float(g["bw"]), float(g["lo"]), npol=2)
+    with fx.Correlator(cfg) as c:
+        split = int(g["split"])
+        per = numffts // split
+        for i in range(split):     # the reference's split ranges, accumulated (merge)
+            c.process(g["data"][None], g["delays"], g["fileoffsets"], i * per, per)
+        vis, counts = c.visibilities()
+    nbl = len(g["counts"])
+    np.testing.assert_array_equal(counts[:nbl], g["counts"])
+    assert_vis_close(vis[0, :nbl], g["vis"])
+
+
+@pytest.mark.skipif(not refcall.available(), reason="oracle/_ref not present")
+def test_vis_vs_reference_live():
+    job = synth.make_job(nant=6, npol=2, nchan=256, numffts=64, bw=32e6, lo=1.65e9, rho=0.1, seed=21)
+    vr, cr = refcall.run_reference(job.data[0], job.delays, job.fileoffsets, 256, 64, 32e6, 1.65e9)
+    with corr_for(job) as c:
+        c.process(job.data, job.delays, job.fileoffsets)
+        vis, counts = c.visibilities()
+    np.testing.assert_array_equal(counts[:15], cr)
+    assert_vis_close(vis[0, :15], vr)
+
+
+@pytest.mark.parametrize("nant,npol,nchan,nsb", [(4, 1, 256, 1), (8, 2, 512, 2), (16, 2, 2048, 1), (64, 1, 1024, 1),
+                                                  (12, 1, 128, 3), (5, 2, 4096, 1)])
+def test_vis_vs_fp64_oracle(nant, npol, nchan, nsb):
+    numffts = 40 if nchan <= 1024 else 16
+    job = synth.make_job(nant=nant, npol=npol, nchan=nchan, numffts=numffts, bw=64e6, lo=1.4e9, rho=0.1,
+                         seed=nant * 100 + nchan, nsubband=nsb)
+    with corr_for(job) as c:
+        c.process(job.data, job.delays, job.fileoffsets)
+        vis, counts = c.visibilities()
+    for sb in range(nsb):
+        ref, rc = oracle_vis(job, sb)
+        np.testing.assert_array_equal(counts, rc)
+        assert_vis_close(vis[sb], ref)
+
+
+def test_time_shards_and_chunks_accumulate():
+    job = synth.make_job(nant=5, npol=1, nchan=256, numffts=200, bw=32e6, lo=1.4e9, rho=0.1, seed=77)
+    ref, rc = oracle_vis(job)
+    with corr_for(job, chunk_ffts=64) as c:
+        for first, n in [(0, 37), (37, 100), (137, 63)]:
+            c.process(job.data, job.delays, job.fileoffsets, first, n)
+        vis, counts = c.visibilities()
+        np.testing.assert_array_equal(counts, rc)
+        assert_vis_close(vis[0], ref)
+        visn, _ = c.visibilities(normalize=True)
+        assert_vis_close(visn[0], fo.normalise(ref, rc))
+        c.reset()
+        vis0, counts0 = c.visibilities()
+        assert not vis0.any() and not counts0.any()
+
+
+def test_invalid_calls_return_status():
+    job = synth.random_job(nant=3, npol=1, nchan=256, numffts=10, seed=3)
+    with corr_for(job) as c:
+        with pytest.raises(fx.FxcError) as e:
+            c.process(job.data, job.delays, job.fileoffsets, 5, 6)
+        assert e.value.status == fx.FXC_ERR_INVALID
+        bad = job.delays.copy()
+        bad[1, 2] = np.nan
+        with pytest.raises(fx.FxcError) as e:
+            c.process(job.data, bad, job.fileoffsets)
+        assert e.value.status == fx.FXC_ERR_INVALID
+        c.process(job.data, job.delays, job.fileoffsets)   # context still usable
+        c.synchronize()

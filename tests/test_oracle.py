@@ -1,0 +1,134 @@
+"""CPU tests: the FP64 oracle against the reference's own outputs.
+
+Golden fixtures (tests/golden/*.npz, made by tests/golden/make_golden.py from the
+reference kernel.c built against the IPP stand-in) pin the oracle everywhere;
+when oracle/_ref is present the oracle is also compared with the reference live
+on fresh seeded inputs.
+"""
+import numpy as np
+import pytest
+
+from difx_tests_b200 import synth
+from oracle import fxoracle as fo
+from oracle import refcall
+
+needs_ref = pytest.mark.skipif(not refcall.available(), reason="oracle/_ref (reference build) not present")
+
+
+def test_lut_levels():
+    lut = fo.lut2bit()
+    assert lut.dtype == np.float32
+    assert lut[0b11100100].tolist() == [np.float32(-3.3359), -1.0, 1.0, np.float32(3.3359)]
+    assert set(np.unique(lut).tolist()) == set(fo.LEVELS.tolist())
+
+
+def test_delay_table_bit_exact_vs_golden(golden):
+    g = golden("delay_table")
+    nf = int(g["numffts"])
+    tab = fo.delay_table(g["delays"], g["fileoffsets"], float(g["bw"]), int(g["nchan"]), np.arange(nf), nf)
+    np.testing.assert_array_equal(tab["valid"], g["valid"].astype(bool))
+    v = tab["valid"]
+    np.testing.assert_array_equal(tab["offset"][v], g["offset"][v])
+    # bit-exact FP64: compare the raw bit patterns
+    assert np.array_equal(tab["frac"][v].view(np.int64), g["frac"][v].view(np.int64))
+    assert np.array_equal(tab["a"].view(np.int64), g["a"].view(np.int64))
+    assert np.array_equal(tab["b"].view(np.int64), g["b"].view(np.int64))
+
+
+def test_delay_table_covers_edge_cases(golden):
+    g = golden("delay_table")
+    nf = int(g["numffts"])
+    F = 2 * int(g["nchan"])
+    Ts = 1.0 / (2 * float(g["bw"]))
+    tab = fo.delay_table(g["delays"], g["fileoffsets"], float(g["bw"]), int(g["nchan"]), np.arange(nf), nf)
+    v = tab["valid"]
+    assert (~v).any(), "no invalid FFTs exercised"
+    # a nudge moves the fractional delay outside the unnudged range [-Ts/2, Ts/2]
+    assert (np.abs(tab["frac"][v]) > 0.5 * Ts * (1 + 1e-9)).any(), "no nudged offsets exercised"
+    assert (tab["offset"][v] == 0).any() and (tab["offset"][v] == (nf - 1) * F).any()
+
+
+def test_unpack_bit_exact_vs_golden(golden):
+    g = golden("unpack")
+    F = 2 * int(g["nchan"])
+    got = fo.unpack(g["data"], g["offsets"], F, 2)        # [P][n][F]
+    np.testing.assert_array_equal(got.transpose(1, 0, 2), g["unpacked"])
+
+
+def test_rotators_vs_golden(golden):
+    g = golden("rotators")
+    for nchan in (256, 1024):
+        params = g[f"params_{nchan}"]
+        bw = float(g[f"bw_{nchan}"])
+        for i, (lo, a, b, frac) in enumerate(params):
+            fr = fo.fringe_rotator(a, b, lo, nchan)
+            np.testing.assert_allclose(fr, g[f"fringe_{nchan}"][i], rtol=0, atol=2e-6)
+            fc = fo.frac_rotator(frac, bw, nchan)
+            np.testing.assert_allclose(fc, g[f"frac_{nchan}"][i], rtol=0, atol=2e-6)
+
+
+@pytest.mark.parametrize("name", ["e2e_c256", "e2e_c1024_split2", "e2e_c256_fraclo"])
+def test_end_to_end_vs_golden(golden, name):
+    g = golden(name)
+    nchan, numffts = int(g["nchan"]), int(g["numffts"])
+    vis, counts = fo.correlate(g["data"], g["delays"], g["fileoffsets"], float(g["bw"]), float(g["lo"]), nchan, 2,
+                               numffts=numffts)
+    nbl = len(g["counts"])
+    np.testing.assert_array_equal(counts[:nbl], g["counts"])
+    mx, rms = fo.vis_error(g["vis"], vis[:nbl])
+    assert mx.max() < 1e-5, mx.max()
+    assert rms.max() < 1e-5, rms.max()
+
+
+@needs_ref
+@pytest.mark.parametrize("nchan,numffts,split", [(256, 32, 1), (256, 40, 4), (1024, 12, 3)])
+def test_end_to_end_vs_reference_live(nchan, numffts, split):
+    job = synth.make_job(nant=4, npol=2, nchan=nchan, numffts=numffts, bw=32e6, lo=1.4e9, rho=0.1, seed=nchan + split)
+    vr, cr = refcall.run_reference(job.data[0], job.delays, job.fileoffsets, nchan, numffts, 32e6, 1.4e9, split=split)
+    vo, co = fo.correlate(job.data[0], job.delays, job.fileoffsets, 32e6, 1.4e9, nchan, 2, numffts=numffts)
+    np.testing.assert_array_equal(co[:6], cr)
+    mx, _ = fo.vis_error(vr, vo[:6])
+    assert mx.max() < 1e-5
+
+
+def test_normalise_matches_reference_semantics():
+    vis = np.ones((3, 1, 4), np.complex128) * (6 + 3j)
+    counts = np.array([3, 0, 2])
+    out = fo.normalise(vis, counts)
+    np.testing.assert_allclose(out[0], 2 + 1j)
+    np.testing.assert_allclose(out[1], 6 + 3j)  # count 0: left as is (kernel.c:350)
+    np.testing.assert_allclose(out[2], 3 + 1.5j)
+
+
+def test_nonsquare_geometry_and_frac_closed_form():
+    for nchan in (128, 512, 2048, 4096):
+        F, stride, S = fo.geometry(nchan)
+        assert F == stride * S
+        frac = 7.3e-9
+        bw = 64e6
+        r = fo.frac_rotator(frac, bw, nchan, ref_args=False)
+        c = np.arange(nchan)
+        np.testing.assert_allclose(r, np.exp(2j * np.pi * c * bw / nchan * frac), atol=1e-5)
+
+
+def test_single_pol_unpack_order():
+    # npol=1: 4 consecutive samples per byte, LSB first
+    data = np.array([0b11100100, 0b00011011], np.uint8)
+    got = fo.unpack(data, np.array([0, 1, 3]), 4, 1)[0]
+    L = fo.LEVELS
+    np.testing.assert_array_equal(got[0], [L[0], L[1], L[2], L[3]])
+    np.testing.assert_array_equal(got[1], [L[1], L[2], L[3], L[3]])
+    np.testing.assert_array_equal(got[2], [L[3], L[3], L[2], L[1]])
+
+
+def test_generator_phases_align():
+    """Synthetic data: corrected cross phases ~0 and |V_cross|/|V_auto| ~ rho x quantiser efficiency."""
+    job = synth.make_job(nant=3, npol=1, nchan=256, numffts=96, bw=32e6, lo=1.4e9, rho=0.2, seed=5)
+    vis, counts = fo.correlate(job.data[0], job.delays, job.fileoffsets, 32e6, 1.4e9, 256, 1, numffts=96)
+    V = fo.normalise(vis, counts)
+    nbl = 3
+    cross = V[:nbl, 0, 8:-8].mean(axis=-1)
+    auto = np.abs(V[nbl:, 0, 8:-8].mean(axis=-1)).mean()
+    assert np.all(np.abs(np.angle(cross)) < 0.15)
+    ratio = np.abs(cross) / auto
+    assert np.all((ratio > 0.12) & (ratio < 0.22)), ratio
