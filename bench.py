@@ -306,7 +306,11 @@ def run_gpu_arm(args):
     delays, offs = delay_model(w["nant"], w["nchan"], w["bw"], seed=42 + rank)
     data = gen_device_data(torch, w["nsb"], w["nant"], w["npol"], subint, pitch, w["rho"], seed=1000 + rank,
                            device=dev)
-    stream = torch.cuda.current_stream()
+    # a dedicated (non-default) stream: the correlator's kernels and the timing
+    # events are then ordered on the same stream
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+    torch.cuda.synchronize()
     corr.set_stream(stream.cuda_stream)
     samples_per_step = w["nant"] * w["npol"] * w["nsb"] * w["numffts"] * F
 

@@ -24,6 +24,7 @@ FXC_ERR_CUDA = -2
 FXC_ERR_NOMEM = -3
 FXC_ERR_UNSUPPORTED = -4
 FXC_ERR_NODEVICE = -5
+FXC_ERR_TIMEOUT = -6
 
 FXC_X_PLAIN_FP32 = 0
 FXC_X_TC_FP16 = 1
@@ -43,7 +44,8 @@ class FxcError(RuntimeError):
         self.status = status
         msg = _lib().fxc_strerror(status).decode() if _LIB is not None else str(status)
         cuda = _lib().fxc_last_cuda_error() if _LIB is not None else 0
-        super().__init__(f"{what}: {msg} (status {status}, cuda error {cuda})")
+        dev = _lib().fxc_last_device_error() if _LIB is not None else 0
+        super().__init__(f"{what}: {msg} (status {status}, cuda error {cuda}, device code {dev})")
 
 
 _LIB = None
@@ -78,6 +80,7 @@ SIGNATURES = {
     "fxc_stage_times": (_I, [_P, _DP, C.POINTER(C.c_longlong), _I]),
     "fxc_strerror": (C.c_char_p, [_I]),
     "fxc_last_cuda_error": (_I, []),
+    "fxc_last_device_error": (_I, []),
     "fxc_debug_delay_table": (_I, [_P, _DP, _DP, _I, _I, _IP, _IP, _DP, _DP, _DP]),
     "fxc_debug_unpack": (_I, [_P, _DP, _DP, _I, _I, _FP]),
     "fxc_debug_spectra": (_I, [_P, _DP, _DP, _I, _I, _FP]),

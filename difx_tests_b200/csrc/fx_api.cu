@@ -37,6 +37,15 @@ struct fxc_ctx {
     float2* d_acc = nullptr;
     size_t acc_bytes = 0;
     int* d_counts = nullptr;
+    int* d_err = nullptr;   // device-side wait expiry code of the tensor-core X stage
+    int nsm = 148;
+    // delay-model upload: [3*nant delays | nant file offsets], pinned ring
+    static constexpr int NRING = 4;
+    double* h_stage = nullptr;
+    cudaEvent_t stage_ev[NRING] = {};
+    int stage_next = 0;
+    std::vector<double> last_model;
+    bool model_valid = false;
     float2* d_vis = nullptr;
     size_t vis_bytes = 0;
     // stage timing (fxc_enable_stage_timing / fxc_stage_times)
@@ -91,6 +100,7 @@ struct StageScope {
 }  // namespace
 
 static thread_local int g_last_cuda = 0;
+static thread_local int g_last_device = 0;
 
 #define FXC_CK(call)                                   \
     do {                                               \
@@ -140,11 +150,13 @@ const char* fxc_strerror(int s)
     case FXC_ERR_NOMEM: return "out of device or pinned host memory";
     case FXC_ERR_UNSUPPORTED: return "not supported by this build";
     case FXC_ERR_NODEVICE: return "no sm_100 CUDA device";
+    case FXC_ERR_TIMEOUT: return "device-side wait expired (result invalid)";
     default: return "unknown status";
     }
 }
 
 int fxc_last_cuda_error(void) { return g_last_cuda; }
+int fxc_last_device_error(void) { return g_last_device; }
 
 static int validate(const fxc_config* c)
 {
@@ -156,8 +168,9 @@ static int validate(const fxc_config* c)
     if (c->xmode != FXC_X_PLAIN_FP32 && c->xmode != FXC_X_TC_FP16) return FXC_ERR_INVALID;
     if (c->chunk_ffts < 0 || c->chunk_ffts % 64) return FXC_ERR_INVALID;
     if ((long long)(c->numffts + 1) * 2 * c->nchan > 0x7fffffffLL) return FXC_ERR_INVALID;  // int sample offsets
-    if (c->xmode == FXC_X_TC_FP16) return FXC_ERR_UNSUPPORTED;
     if (c->nant * c->npol > 64) return FXC_ERR_UNSUPPORTED;
+    // tensor-core form: the F stage stages 16 FFTs x npol x nchan FP16 pairs in shared memory
+    if (c->xmode == FXC_X_TC_FP16 && c->npol * c->nchan > 2048) return FXC_ERR_UNSUPPORTED;
     return FXC_OK;
 }
 
@@ -166,7 +179,9 @@ static void free_ctx(fxc_ctx* x)
     if (!x) return;
     cudaFree(x->d_in);
     cudaFree(x->d_delays);
-    cudaFree(x->d_offs);
+    for (auto& ev : x->stage_ev)
+        if (ev) cudaEventDestroy(ev);
+    if (x->h_stage) cudaFreeHost(x->h_stage);
     cudaFree(x->d_sblo);
     cudaFree(x->d_chan_sub);
     cudaFree(x->d_chan_step);
@@ -175,6 +190,7 @@ static void free_ctx(fxc_ctx* x)
     cudaFree(x->d_spec);
     cudaFree(x->d_acc);
     cudaFree(x->d_counts);
+    cudaFree(x->d_err);
     cudaFree(x->d_vis);
     for (auto& p : x->pending) {
         cudaEventDestroy(p.a);
@@ -200,6 +216,7 @@ int fxc_create(const fxc_config* cfg, fxc_ctx** out)
     fxc_ctx* x = new fxc_ctx();
     x->cfg = *cfg;
     x->device = dev;
+    x->nsm = prop.multiProcessorCount;
     const fxc_config& c = x->cfg;
     x->F = 2 * c.nchan;
     x->nsig = c.nant * c.npol;
@@ -213,10 +230,13 @@ int fxc_create(const fxc_config* cfg, fxc_ctx** out)
     x->rows = (int)round_up((size_t)2 * x->nsig, 128);
 
     // chunk length: spectra buffer <= ~1 GiB
-    const size_t per_slot = (size_t)c.nsubband * x->nsig * c.nchan * sizeof(float2);
+    // bytes per FFT slot of the spectra buffer: plain f32x2 [sb][sig][T][chan]; TC f16 [sb][chan][rows][T]
+    const bool tc = c.xmode == FXC_X_TC_FP16;
+    const size_t per_slot = tc ? (size_t)c.nsubband * c.nchan * x->rows * sizeof(uint16_t)
+                               : (size_t)c.nsubband * x->nsig * c.nchan * sizeof(float2);
     size_t T = c.chunk_ffts;
     if (T == 0) {
-        T = ((size_t)1 << 30) / per_slot;
+        T = ((size_t)(tc ? 2 : 1) << 30) / per_slot;
         T = T / 64 * 64;
         if (T < 64) T = 64;
         if (T > 4096) T = 4096;
@@ -239,8 +259,14 @@ int fxc_create(const fxc_config* cfg, fxc_ctx** out)
     const int stride = 1 << ((int)std::log2((double)c.nchan) / 2);
     if ((e = cudaMalloc(&x->d_in, in_bytes)) != cudaSuccess) return fail(e);
     if ((e = cudaMemset(x->d_in, 0, in_bytes)) != cudaSuccess) return fail(e);
-    if ((e = cudaMalloc(&x->d_delays, 3 * sizeof(double) * c.nant)) != cudaSuccess) return fail(e);
-    if ((e = cudaMalloc(&x->d_offs, sizeof(double) * c.nant)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&x->d_delays, 4 * sizeof(double) * c.nant)) != cudaSuccess) return fail(e);
+    x->d_offs = x->d_delays + 3 * c.nant;
+    x->last_model.assign(4 * (size_t)c.nant, 0.0);
+    if ((e = cudaHostAlloc(&x->h_stage, fxc_ctx::NRING * 4 * sizeof(double) * c.nant, cudaHostAllocDefault)) !=
+        cudaSuccess)
+        return fail(e);
+    for (auto& ev : x->stage_ev)
+        if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
     if ((e = cudaMalloc(&x->d_sblo, sizeof(double) * c.nsubband)) != cudaSuccess) return fail(e);
     if ((e = cudaMalloc(&x->d_chan_sub, sizeof(float) * stride)) != cudaSuccess) return fail(e);
     if ((e = cudaMalloc(&x->d_chan_step, sizeof(float) * (c.nchan / stride))) != cudaSuccess) return fail(e);
@@ -250,6 +276,8 @@ int fxc_create(const fxc_config* cfg, fxc_ctx** out)
     if ((e = cudaMemset(x->d_spec, 0, x->spec_bytes)) != cudaSuccess) return fail(e);
     if ((e = cudaMalloc(&x->d_acc, x->acc_bytes)) != cudaSuccess) return fail(e);
     if ((e = cudaMalloc(&x->d_counts, sizeof(int) * x->npair_ant)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&x->d_err, sizeof(int))) != cudaSuccess) return fail(e);
+    if ((e = cudaMemset(x->d_err, 0, sizeof(int))) != cudaSuccess) return fail(e);
     if ((e = cudaMalloc(&x->d_vis, x->vis_bytes)) != cudaSuccess) return fail(e);
 
     // constant tables: per-subband LO, f32 channel angular frequencies (kernel.c:162-166)
@@ -296,12 +324,25 @@ int fxc_set_stream(fxc_ctx* x, void* s)
     return FXC_OK;
 }
 
+// Reads (and clears) the device-side wait-expiry code; the stream must be idle.
+static int device_status(fxc_ctx* x)
+{
+    int h = 0;
+    FXC_CK(cudaMemcpy(&h, x->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h != 0) {
+        FXC_CK(cudaMemset(x->d_err, 0, sizeof(int)));
+        g_last_device = h;
+        return FXC_ERR_TIMEOUT;
+    }
+    return FXC_OK;
+}
+
 int fxc_synchronize(fxc_ctx* x)
 {
     if (!x) return FXC_ERR_INVALID;
     FXC_CK(cudaSetDevice(x->device));
     FXC_CK(cudaStreamSynchronize(x->stream));
-    return FXC_OK;
+    return device_status(x);
 }
 
 int fxc_device_input(fxc_ctx* x, uint8_t** d, size_t* pitch)
@@ -334,8 +375,25 @@ static int run_delay_table(fxc_ctx* x, const double* delays, const double* offs,
         if (!std::isfinite(delays[a])) return FXC_ERR_INVALID;
     for (int a = 0; a < c.nant; a++)
         if (!std::isfinite(offs[a])) return FXC_ERR_INVALID;
-    FXC_CK(cudaMemcpyAsync(x->d_delays, delays, 3 * sizeof(double) * c.nant, cudaMemcpyHostToDevice, x->stream));
-    FXC_CK(cudaMemcpyAsync(x->d_offs, offs, sizeof(double) * c.nant, cudaMemcpyHostToDevice, x->stream));
+    // The delay model goes to the device only when it changed, through a ring of
+    // pinned slots so the copy stays asynchronous (a pageable source would block
+    // the host until the stream's earlier work had finished).
+    const size_t nmodel = 4 * (size_t)c.nant;
+    bool same = x->model_valid;
+    for (size_t i = 0; same && i < 3 * (size_t)c.nant; i++) same = x->last_model[i] == delays[i];
+    for (int i = 0; same && i < c.nant; i++) same = x->last_model[3 * c.nant + i] == offs[i];
+    if (!same) {
+        const int slot = x->stage_next;
+        x->stage_next = (slot + 1) % fxc_ctx::NRING;
+        FXC_CK(cudaEventSynchronize(x->stage_ev[slot]));
+        double* h = x->h_stage + slot * nmodel;
+        std::memcpy(h, delays, 3 * sizeof(double) * c.nant);
+        std::memcpy(h + 3 * c.nant, offs, sizeof(double) * c.nant);
+        FXC_CK(cudaMemcpyAsync(x->d_delays, h, nmodel * sizeof(double), cudaMemcpyHostToDevice, x->stream));
+        FXC_CK(cudaEventRecord(x->stage_ev[slot], x->stream));
+        std::memcpy(x->last_model.data(), h, nmodel * sizeof(double));
+        x->model_valid = true;
+    }
     const int ld = (int)round_up((size_t)nfft, 128);
     const int maxoffset = (c.numffts - 1) * x->F;  // kernel.c:730
     const double sampletime = 1.0 / (2.0 * c.bw);  // kernel.c:14
@@ -377,6 +435,7 @@ int fxc_process_device(fxc_ctx* x, const uint8_t* d_data, size_t pitch, const do
         if (st != FXC_OK) return st;
         FXC_CK(launch_counts(x->d_vbits, x->cfg.nant, ld / 32, x->d_counts, x->stream));
     }
+    const bool tc = x->cfg.xmode == FXC_X_TC_FP16;
     FArgs fa = make_fargs(x, d_data, pitch, ld);
     XArgs xa;
     xa.spec = x->d_spec;
@@ -391,11 +450,11 @@ int fxc_process_device(fxc_ctx* x, const uint8_t* d_data, size_t pitch, const do
         fa.nfft = std::min(x->T, nfft - c0);
         {
             StageScope sc(x, 1, 1);
-            FXC_CK(launch_fstage(x->cfg.nchan, kSpecF32, fa, x->stream));
+            FXC_CK(launch_fstage(x->cfg.nchan, tc ? kSpecF16 : kSpecF32, fa, x->stream));
         }
         {
             StageScope sc(x, 2, 1);
-            FXC_CK(launch_xplain(xa, x->stream));
+            FXC_CK(tc ? launch_xtc(xa, x->d_err, x->nsm, x->stream) : launch_xplain(xa, x->stream));
         }
     }
     return FXC_OK;
@@ -438,7 +497,7 @@ int fxc_get_visibilities_device(fxc_ctx* x, float* d_vis, int normalize)
     FXC_CK(cudaSetDevice(x->device));
     const fxc_config& c = x->cfg;
     StageScope sc(x, 3, 1);
-    FXC_CK(launch_finalize(x->d_acc, 0, x->nsig, c.npol, c.nant, c.nchan, c.nsubband, x->d_counts, normalize,
+    FXC_CK(launch_finalize(x->d_acc, c.xmode == FXC_X_TC_FP16 ? 1 : 0, x->nsig, c.npol, c.nant, c.nchan, c.nsubband, x->d_counts, normalize,
                            reinterpret_cast<float2*>(d_vis), x->stream));
     return FXC_OK;
 }
@@ -453,7 +512,7 @@ int fxc_get_visibilities(fxc_ctx* x, float* vis, int* counts, int normalize)
     FXC_CK(cudaMemcpyAsync(pc.data(), x->d_counts, sizeof(int) * x->npair_ant, cudaMemcpyDeviceToHost, x->stream));
     FXC_CK(cudaStreamSynchronize(x->stream));
     if (counts) counts_out(x, pc, counts);
-    return FXC_OK;
+    return device_status(x);
 }
 
 int fxc_enable_stage_timing(fxc_ctx* x, int enable)

@@ -14,6 +14,21 @@
 
 namespace fx {
 
+// Sets a kernel's dynamic shared-memory limit once per device (the attribute is
+// per function and device).  `mask` is the caller's per-kernel static word.
+template <typename Kern>
+inline cudaError_t set_smem_once(Kern kern, size_t bytes, unsigned* mask)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const unsigned bit = 1u << (dev & 31);
+    if (*mask & bit) return cudaSuccess;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) *mask |= bit;
+    return e;
+}
+
 // ---------------------------------------------------------------- FP64 (no FMA)
 __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }

@@ -426,7 +426,8 @@ static cudaError_t launch_f(const FArgs& a, cudaStream_t st)
     using P = FPlan<F>;
     const size_t sm = fstage_smem<F>(MODE, TB, a.npol);
     auto kern = k_fstage<F, MODE, TB>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    static unsigned configured = 0;  // per instantiation and device
+    cudaError_t e = set_smem_once(kern, sm, &configured);
     if (e != cudaSuccess) return e;
     dim3 grid((a.T + TB - 1) / TB, a.nant, a.nsb);
     kern<<<grid, P::NTHREADS, sm, st>>>(a);

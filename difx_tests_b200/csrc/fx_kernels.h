@@ -16,6 +16,8 @@ cudaError_t launch_finalize(const float2* acc, int acc_layout, int nsig, int npo
 cudaError_t launch_fstage(int nchan, int mode, const FArgs& a, cudaStream_t st);
 size_t fstage_smem_bytes(int nchan, int mode, int npol);
 cudaError_t launch_xplain(const XArgs& a, cudaStream_t st);
+cudaError_t launch_xtc(const XArgs& a, int* d_err, int nsm, cudaStream_t st);
+size_t xtc_smem_bytes();
 cudaError_t launch_unpack_debug(int nchan, const FArgs& a, float* out, cudaStream_t st);
 
 }  // namespace fx

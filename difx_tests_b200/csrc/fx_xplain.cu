@@ -145,7 +145,8 @@ static cudaError_t launch_x(const XArgs& a, cudaStream_t st)
     using P = XPlan<NB, CG, TK>;
     const size_t sm = 2 * (size_t)P::STAGE * sizeof(float2);
     auto kern = k_xplain<NB, CG, TK>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    static unsigned configured = 0;  // per instantiation and device
+    cudaError_t e = set_smem_once(kern, sm, &configured);
     if (e != cudaSuccess) return e;
     dim3 grid(a.nchan / CG, a.nsb);
     kern<<<grid, P::NTHREADS, sm, st>>>(a);

@@ -1,0 +1,392 @@
+// fx_xtc.cu -- tensor-core X stage (tcgen05, FP16 inputs, FP32 accumulation).
+//
+// Per channel c the visibility matrix V = sum_t X_t X_t^H over signals is a
+// Hermitian rank-T update.  With the spectra stored real-ified and K(=time)-major,
+//   A[c] (rows x T), row 2s = Re X_s, row 2s+1 = Im X_s,
+// the real Gram matrix G = A A^T holds every product:
+//   Re V[i][j] = G[2i][2j] + G[2i+1][2j+1],   Im V[i][j] = G[2i+1][2j] - G[2i][2j+1]
+// (V[i][j] = X_i conj(X_j), kernel.c:846 with the conjugation of kernel.c:557-568).
+// One 128x128 FP32 accumulator covers up to 64 signals per channel.
+//
+// Persistent, warp-specialised CTA per SM; work item = (subband, channel):
+//   warp 0     TMA producer: 128-row x 64-FFT FP16 boxes (SWIZZLE_128B) into an
+//              NSTAGE ring of shared-memory stages (mbarrier full/empty pairs)
+//   warp 1     MMA issuer: 4 x tcgen05.mma.kind::f16 M128 N128 K16 per stage, A and
+//              B descriptors on the same tile; tcgen05.commit frees the stage and,
+//              after the channel's last stage, publishes the TMEM accumulator
+//   warps 2-5  epilogue: tcgen05.ld of the accumulator (two TMEM buffers, so the
+//              next channel's MMAs overlap), one lane shuffle combines Re/Im rows,
+//              FP32 accumulate into acc[sb][c][pair(i,j)], i <= j.
+// Every wait is bounded by time; on expiry the CTA records an error code, drains
+// what it issued (again bounded), frees TMEM and returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <cstdio>
+
+#include "fx_common.cuh"
+#include "fx_kernels.h"
+
+namespace fx {
+
+namespace tc {
+
+constexpr int BM = 128;                    // rows per channel tile (2 x 64 signals)
+constexpr int BK = 64;                     // FFTs per stage (128 B of FP16 = one swizzle row)
+constexpr int NSTAGE = 8;
+constexpr int STAGE_BYTES = BM * BK * 2;   // 16 KB
+constexpr int NTHREADS = 192;              // 6 warps
+constexpr int TMEM_COLS = 256;             // two 128-column FP32 accumulators
+constexpr unsigned long long WAIT_NS = 1000000000ull;   // 1 s per wait
+
+struct Smem {
+    alignas(1024) uint8_t stage[NSTAGE][STAGE_BYTES];
+    alignas(8) uint64_t full[NSTAGE];
+    uint64_t empty[NSTAGE];
+    uint64_t acc_full[2];
+    uint64_t acc_empty[2];
+    uint64_t drain;          // final tcgen05.commit: every MMA of this CTA retired
+    uint32_t tmem_base;
+    int abort;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ unsigned long long globaltimer()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* b)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: true when the phase completed, false after WAIT_NS or on abort.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag)
+{
+    if (mbar_try(b, parity)) return true;
+    const unsigned long long t0 = globaltimer();
+    while (true) {
+        if (mbar_try(b, parity)) return true;
+        if (*abort_flag) return false;
+        if (globaltimer() - t0 > WAIT_NS) return false;
+    }
+}
+
+__device__ __forceinline__ void tma_load_2d(const CUtensorMap* map, uint64_t* bar, void* dst, int x, int y)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
+        ::"r"(smem_u32(dst)), "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y)
+        : "memory");
+}
+
+// UMMA shared-memory descriptor: K-major, SWIZZLE_128B, 8-row groups 1024 B apart.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);   // start address
+    d |= (uint64_t)1 << 16;                   // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)(1024 >> 4) << 32;         // stride byte offset
+    d |= (uint64_t)1 << 46;                   // descriptor version (sm100)
+    d |= (uint64_t)2 << 61;                   // SWIZZLE_128B
+    return d;
+}
+
+// Instruction descriptor, kind::f16: D F32, A/B F16, both K-major, M=128, N=128.
+constexpr uint32_t kIdesc = (1u << 4) | (0u << 7) | (0u << 10) | ((uint32_t)(128 >> 3) << 17) |
+                            ((uint32_t)(128 >> 4) << 24);
+
+__device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(tmem_d), "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t* r)
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+}  // namespace tc
+
+// err: 0 ok; 1 TMA wait expired; 2 stage-free wait expired; 3 accumulator wait expired;
+//      4 epilogue wait expired; 5 drain expired
+__global__ void __launch_bounds__(tc::NTHREADS, 1)
+k_xtc(const __grid_constant__ CUtensorMap tmap, XArgs a, int* err)
+{
+    using namespace tc;
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    Smem& sm = *reinterpret_cast<Smem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    volatile int* abort_flag = &sm.abort;
+
+    const int nitems = a.nsb * a.nchan;
+    const int nk = a.T / BK;
+    const int nsig = a.nsig;
+    const int npair = nsig * (nsig + 1) / 2;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < NSTAGE; s++) {
+            mbar_init(&sm.full[s], 1);
+            mbar_init(&sm.empty[s], 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            mbar_init(&sm.acc_full[b], 1);
+            mbar_init(&sm.acc_empty[b], 128);
+        }
+        mbar_init(&sm.drain, 1);
+        sm.abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sm.tmem_base)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = sm.tmem_base;
+
+    if (warp == 0) {
+        // ------------------------------------------------------------ producer
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            long long issued = 0;
+            for (int item = blockIdx.x; item < nitems && !*abort_flag; item += gridDim.x) {
+                const int row0 = item * a.rows;   // (sb * nchan + c) * rows
+                for (int kb = 0; kb < nk; kb++) {
+                    if (!mbar_wait(&sm.empty[stage], phase ^ 1, abort_flag)) {
+                        if (!*abort_flag) atomicCAS(err, 0, 2);
+                        *abort_flag = 1;
+                        break;
+                    }
+                    mbar_expect_tx(&sm.full[stage], STAGE_BYTES);
+                    tma_load_2d(&tmap, &sm.full[stage], sm.stage[stage], kb * BK, row0);
+                    issued++;
+                    if (++stage == NSTAGE) {
+                        stage = 0;
+                        phase ^= 1;
+                    }
+                }
+            }
+            // drain: every stage issued must have landed before the CTA exits
+            for (int s = 0; s < NSTAGE && issued > 0; s++) {
+                // the last NSTAGE issues are the only ones that may still be in flight
+                const long long idx = issued - 1 - s;
+                if (idx < 0) break;
+                const int st = (int)(idx % NSTAGE);
+                const uint32_t ph = (uint32_t)((idx / NSTAGE) & 1);
+                const unsigned long long t0 = globaltimer();
+                while (!mbar_try(&sm.full[st], ph)) {
+                    if (globaltimer() - t0 > WAIT_NS) {
+                        atomicCAS(err, 0, 5);
+                        break;
+                    }
+                }
+            }
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------------------ MMA issuer
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            int buf = 0;
+            uint32_t acc_phase = 0;
+            for (int item = blockIdx.x; item < nitems && !*abort_flag; item += gridDim.x) {
+                if (!mbar_wait(&sm.acc_empty[buf], acc_phase ^ 1, abort_flag)) {
+                    if (!*abort_flag) atomicCAS(err, 0, 3);
+                    *abort_flag = 1;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t d = tmem + buf * 128;
+                bool ok = true;
+                for (int kb = 0; kb < nk; kb++) {
+                    if (!mbar_wait(&sm.full[stage], phase, abort_flag)) {
+                        if (!*abort_flag) atomicCAS(err, 0, 1);
+                        *abort_flag = 1;
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t s0 = smem_u32(sm.stage[stage]);
+#pragma unroll
+                    for (int k = 0; k < BK / 16; k++) {
+                        const uint64_t desc = umma_desc(s0 + k * 32);
+                        umma_f16(d, desc, desc, (kb > 0 || k > 0) ? 1u : 0u);
+                    }
+                    umma_commit(&sm.empty[stage]);
+                    if (++stage == NSTAGE) {
+                        stage = 0;
+                        phase ^= 1;
+                    }
+                }
+                if (!ok) break;
+                umma_commit(&sm.acc_full[buf]);
+                if (++buf == 2) {
+                    buf = 0;
+                    acc_phase ^= 1;
+                }
+            }
+            // drain: wait for every issued MMA before TMEM is freed
+            // (a dedicated barrier: committing to acc_full would advance it past a lagging epilogue)
+            uint64_t* fin = &sm.drain;
+            umma_commit(fin);
+            const unsigned long long t0 = globaltimer();
+            while (!mbar_try(fin, 0)) {
+                if (globaltimer() - t0 > WAIT_NS) {
+                    atomicCAS(err, 0, 5);
+                    break;
+                }
+            }
+        }
+    } else {
+        // ------------------------------------------------------------ epilogue
+        const int q = warp & 3;                  // TMEM lane quadrant of this warp
+        const int r = q * 32 + lane;             // accumulator row
+        const int i = r >> 1;                    // signal of this row
+        const bool odd = (r & 1) != 0;
+        int buf = 0;
+        uint32_t acc_phase = 0;
+        float2* acc = reinterpret_cast<float2*>(a.acc);
+        for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+            if (!mbar_wait(&sm.acc_full[buf], acc_phase, abort_flag)) {
+                if (!*abort_flag) atomicCAS(err, 0, 4);
+                *abort_flag = 1;
+                break;
+            }
+            tc_fence_after();
+            float* out = reinterpret_cast<float*>(acc + (size_t)item * npair);
+            const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + buf * 128;
+#pragma unroll 1
+            for (int cq = 0; cq < 4; cq++) {      // 32 columns = 16 signal pairs j per chunk
+                uint32_t v[32];
+                tmem_ld32(taddr + cq * 32, v);
+                tmem_wait_ld();
+                if (cq == 3) {
+                    tc_fence_before();
+                    mbar_arrive(&sm.acc_empty[buf]);
+                }
+#pragma unroll
+                for (int jj = 0; jj < 16; jj++) {
+                    const int j = cq * 16 + jj;
+                    const float g0 = __uint_as_float(v[2 * jj]);      // G[r][2j]
+                    const float g1 = __uint_as_float(v[2 * jj + 1]);  // G[r][2j+1]
+                    // even row 2i holds (a, b) = (G[2i][2j], G[2i][2j+1]); odd row holds (c, d) =
+                    // (G[2i+1][2j], G[2i+1][2j+1]).  Both send column 2j+1: even receives d, odd b.
+                    const float other = __shfl_xor_sync(0xffffffffu, g1, 1);
+                    const float val = odd ? (g0 - other) : (g0 + other);   // Im = c - b ; Re = a + d
+                    if (j >= i && j < nsig) {
+                        const int p = i * nsig - (i * (i - 1)) / 2 + (j - i);
+                        float* o = out + 2 * p + (odd ? 1 : 0);
+                        *o += val;
+                    }
+                }
+            }
+            if (++buf == 2) {
+                buf = 0;
+                acc_phase ^= 1;
+            }
+        }
+    }
+
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+    }
+}
+
+static PFN_cuTensorMapEncodeTiled_v12000 get_encode()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void* p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+size_t xtc_smem_bytes() { return sizeof(tc::Smem) + 1024; }
+
+cudaError_t launch_xtc(const XArgs& a, int* d_err, int nsm, cudaStream_t st)
+{
+    if (a.rows != tc::BM || a.T % tc::BK != 0 || a.nsig > 64) return cudaErrorInvalidValue;
+    auto enc = get_encode();
+    if (!enc) return cudaErrorNotSupported;
+    CUtensorMap map;
+    const cuuint64_t dims[2] = {(cuuint64_t)a.T, (cuuint64_t)a.nsb * a.nchan * a.rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)a.T * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)tc::BK, (cuuint32_t)tc::BM};
+    const cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<void*>(a.spec), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+    const size_t sm = xtc_smem_bytes();
+    static unsigned configured = 0;
+    cudaError_t e = set_smem_once(k_xtc, sm, &configured);
+    if (e != cudaSuccess) return e;
+    const int nitems = a.nsb * a.nchan;
+    const int grid = nitems < nsm ? nitems : nsm;
+    k_xtc<<<grid, tc::NTHREADS, sm, st>>>(map, a, d_err);
+    return cudaGetLastError();
+}
+
+}  // namespace fx

@@ -40,6 +40,7 @@ extern "C" {
 #define FXC_ERR_NOMEM        -3   /* device or pinned-host allocation failed */
 #define FXC_ERR_UNSUPPORTED  -4   /* valid request this build does not implement */
 #define FXC_ERR_NODEVICE     -5   /* no sm_100 CUDA device */
+#define FXC_ERR_TIMEOUT      -6   /* a bounded device-side wait expired; that call's result is invalid */
 
 /* X-stage arithmetic */
 #define FXC_X_PLAIN_FP32 0        /* FP32 CUDA-core cross-multiply-accumulate */
@@ -143,6 +144,10 @@ int fxc_stage_times(fxc_ctx* ctx, double* ms, long long* launches, int reset);
 const char* fxc_strerror(int status);
 /* Last CUDA error code seen by this thread's calls (cudaError_t as int). */
 int fxc_last_cuda_error(void);
+/* Which device-side wait expired when a call returned FXC_ERR_TIMEOUT on this
+ * thread: 1 stage load, 2 stage release, 3 accumulator release, 4 accumulator
+ * ready, 5 drain at exit; 0 if none. */
+int fxc_last_device_error(void);
 
 /* ---- inspection entry points (parity tests; not needed for correlation) ---- */
 

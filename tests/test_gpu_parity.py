@@ -39,7 +39,7 @@ def test_delay_table_bit_exact_vs_reference(golden):
     g = golden("delay_table")
     nant = g["delays"].shape[0]
     nf = int(g["numffts"])
-    cfg = fx.make_config(nant, int(g["nchan"]), nf, float(g["bw"]), 1.4e9, npol=2)
+    cfg = fx.make_config(nant, int(g["nchan"]), nf, float(g["bw"]), 1.4e9, npol=1)
     with fx.Correlator(cfg) as c:
         tab = c.delay_table(g["delays"], g["fileoffsets"], 0, nf)
     np.testing.assert_array_equal(tab["valid"], g["valid"].astype(bool))
@@ -53,8 +53,10 @@ def test_delay_table_bit_exact_vs_reference(golden):
 @pytest.mark.parametrize("nchan,first", [(256, 0), (2048, 17), (4096, 5)])
 def test_delay_table_bit_exact_vs_oracle(nchan, first):
     job = synth.random_job(nant=9, npol=1, nchan=nchan, numffts=300, bw=64e6, seed=nchan)
-    job.delays[2, 1] *= 400  # fast drift: invalid FFTs at one end
-    job.fileoffsets[3] += 0.6 / (2 * job.bw)
+    Ts = 1.0 / (2 * job.bw)
+    job.delays[2, 1] = 0.5 * 2 * nchan * Ts   # drifts half an FFT per FFT: out of range at the end
+    job.fileoffsets[4] -= 50.3 * 2 * nchan * Ts   # net delay 50 FFTs: the first FFTs are invalid
+    job.fileoffsets[3] += 0.6 * Ts
     nf = 200
     with corr_for(job) as c:
         tab = c.delay_table(job.delays, job.fileoffsets, first, nf)
@@ -192,3 +194,38 @@ def test_invalid_calls_return_status():
         assert e.value.status == fx.FXC_ERR_INVALID
         c.process(job.data, job.delays, job.fileoffsets)   # context still usable
         c.synchronize()
+
+
+# ---------------------------------------------------------------- tensor-core form
+TC_RMS_TOL = 1e-3    # FP16 inputs, FP32 accumulation: RMS relative error per spectrum vs FP64
+TC_MAX_TOL = 1e-2    # max |d| / max |ref| per spectrum
+
+
+@pytest.mark.parametrize("nant,npol,nchan,nsb,numffts", [(4, 1, 256, 1, 64), (16, 2, 512, 2, 64),
+                                                          (64, 1, 1024, 1, 64), (12, 1, 2048, 1, 32),
+                                                          (33, 1, 128, 2, 128)])
+def test_tc_vis_vs_fp64_oracle(nant, npol, nchan, nsb, numffts):
+    job = synth.make_job(nant=nant, npol=npol, nchan=nchan, numffts=numffts, bw=64e6, lo=1.4e9, rho=0.1,
+                         seed=nant * 7 + nchan, nsubband=nsb)
+    with corr_for(job, xmode=fx.FXC_X_TC_FP16) as c:
+        c.process(job.data, job.delays, job.fileoffsets)
+        vis, counts = c.visibilities()
+    for sb in range(nsb):
+        ref, rc = oracle_vis(job, sb)
+        np.testing.assert_array_equal(counts, rc)
+        mx, rms = fo.vis_error(vis[sb], ref)
+        assert rms.max() < TC_RMS_TOL, f"rms {rms.max():.3e}"
+        assert mx.max() < TC_MAX_TOL, f"max {mx.max():.3e}"
+
+
+def test_tc_matches_plain_and_accumulates_over_chunks():
+    job = synth.make_job(nant=24, npol=1, nchan=1024, numffts=300, bw=64e6, lo=1.4e9, rho=0.1, seed=31)
+    out = {}
+    for mode in (fx.FXC_X_PLAIN_FP32, fx.FXC_X_TC_FP16):
+        with corr_for(job, xmode=mode, chunk_ffts=128) as c:
+            c.process(job.data, job.delays, job.fileoffsets, 0, 150)
+            c.process(job.data, job.delays, job.fileoffsets, 150, 150)
+            out[mode] = c.visibilities(normalize=True)
+    np.testing.assert_array_equal(out[0][1], out[1][1])
+    mx, rms = fo.vis_error(out[1][0][0], out[0][0][0])
+    assert rms.max() < TC_RMS_TOL and mx.max() < TC_MAX_TOL
