@@ -236,7 +236,7 @@ int fxc_create(const fxc_config* cfg, fxc_ctx** out)
                                : (size_t)c.nsubband * x->nsig * c.nchan * sizeof(float2);
     size_t T = c.chunk_ffts;
     if (T == 0) {
-        T = ((size_t)(tc ? 2 : 1) << 30) / per_slot;
+        T = ((size_t)(tc ? 6 : 1) << 30) / per_slot;
         T = T / 64 * 64;
         if (T < 64) T = 64;
         if (T > 4096) T = 4096;

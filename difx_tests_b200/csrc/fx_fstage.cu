@@ -43,6 +43,7 @@ struct FPlan {
     static constexpr int BUF = F + F / 16;                    // padded exchange buffer (float2)
     static constexpr bool TWREG = (F <= 2048);                // twiddles cached in registers
     static constexpr int TWQ = F / 4;                         // quarter-wave twiddle table
+    static constexpr int MINB = (NTHREADS <= 256) ? 2 : 1;    // CTAs per SM the registers must allow
 };
 
 template <int F, int PASS>
@@ -136,20 +137,25 @@ __device__ __forceinline__ void init_pass_tw(PassTw<F, PASS>& tw, int t)
     }
 }
 
-// Load pass inputs from the exchange buffer and apply the DIT twiddles.
+// Load pass inputs from the exchange buffer and apply the DIT twiddles.  All
+// offsets are multiples of 16 elements, so padi(t + c) = padi(t) + c + c/16 and
+// every shared-memory access is one base register plus an immediate.
 template <int F, int PASS>
 __device__ __forceinline__ void pass_load(const float2* buf, const float2* tq, const PassTw<F, PASS>* tw,
                                           float2* v, int t)
 {
     using PI = PassInfo<F, PASS>;
     constexpr int NT = FPlan<F>::NT;
+    constexpr int STEP = F / PI::R;
+    static_assert(STEP % 16 == 0 && NT % 16 == 0, "padded offsets must fold");
+    const float2* p0 = buf + padi(t);
 #pragma unroll
     for (int b = 0; b < PI::NB; b++) {
-        const int j = t + b * NT;
-        const int jm = j & (PI::NS - 1);
+        const int jm = (t + b * NT) & (PI::NS - 1);
+        const float2* p = p0 + b * (NT + NT / 16);
 #pragma unroll
         for (int r = 0; r < PI::R; r++) {
-            float2 x = buf[padi(j + r * (F / PI::R))];
+            float2 x = p[r * (STEP + STEP / 16)];
             if (r > 0) {
                 float2 w;
                 if constexpr (FPlan<F>::TWREG) w = tw->w[b * PI::R + r];
@@ -169,6 +175,7 @@ __device__ __forceinline__ void pass_dft(float2* v)
     for (int b = 0; b < PI::NB; b++) dft<PI::R>(v + b * PI::R);
 }
 
+// Stockham store: element r of butterfly j goes to (j / NS) * NS * R + j % NS + r * NS.
 template <int F, int PASS>
 __device__ __forceinline__ void pass_store(float2* buf, const float2* v, int t)
 {
@@ -177,9 +184,12 @@ __device__ __forceinline__ void pass_store(float2* buf, const float2* v, int t)
 #pragma unroll
     for (int b = 0; b < PI::NB; b++) {
         const int j = t + b * NT;
-        const int base = (j / PI::NS) * PI::NS * PI::R + (j & (PI::NS - 1));
+        float2* p;
+        constexpr int RS = (PI::NS == 1) ? 1 : PI::NS + PI::NS / 16;   // padded stride of r
+        if constexpr (PI::NS == 1) p = buf + 17 * j;                    // padi(16 j)
+        else p = buf + padi((j / PI::NS) * PI::NS * PI::R + (j & (PI::NS - 1)));
 #pragma unroll
-        for (int r = 0; r < PI::R; r++) buf[padi(base + r * PI::NS)] = v[b * PI::R + r];
+        for (int r = 0; r < PI::R; r++) p[r * RS] = v[b * PI::R + r];
     }
 }
 
@@ -215,21 +225,20 @@ __device__ __forceinline__ float2 rot_entry(int e, const DelayEntry& d, double l
     return make_float2(c, s);
 }
 
-template <int F, int MODE, int TB>
-__global__ void __launch_bounds__(FPlan<F>::NTHREADS)
+template <int F, int MODE, int TB, int NPOL>
+__global__ void __launch_bounds__(FPlan<F>::NTHREADS, FPlan<F>::MINB)
 k_fstage(FArgs args)
 {
     using P = FPlan<F>;
     constexpr int NT = P::NT;
     constexpr int C = P::C;
+    constexpr int INB = F / 2 + 16;                                    // staged bytes per slot
     extern __shared__ __align__(16) unsigned char smem[];
-    float2* bufs = reinterpret_cast<float2*>(smem);                 // [NSLOT][BUF]
-    float2* tq = bufs + P::NSLOT * P::BUF;                            // [TWQ]
-    float2* rtabs = tq + (P::TWREG ? 0 : P::TWQ);                    // [NSLOT][NROT]
-    int* otab = reinterpret_cast<int*>(rtabs + P::NSLOT * P::NROT);  // [NSLOT][2]
-    uint8_t* inbs = reinterpret_cast<uint8_t*>(otab + 4 * P::NSLOT); // [NSLOT][WIN]
-    const int npol = args.npol;
-    __half2* stage = reinterpret_cast<__half2*>(inbs + P::NSLOT * ((F / 2 + 16 + 15) & ~15));  // [npol][TB][C]
+    float2* bufs = reinterpret_cast<float2*>(smem);                   // [NSLOT][BUF]
+    float2* tq = bufs + P::NSLOT * P::BUF;                              // [TWQ]
+    float2* rtabs = tq + (P::TWREG ? 0 : P::TWQ);                      // [NSLOT][NROT]
+    uint8_t* inbs = reinterpret_cast<uint8_t*>(rtabs + P::NSLOT * P::NROT);  // [NSLOT][INB]
+    __half2* stage = reinterpret_cast<__half2*>(inbs + P::NSLOT * INB);       // [NPOL][TB][C]
 
     const int tid = threadIdx.x;
     const int slot = tid / NT;
@@ -239,11 +248,11 @@ k_fstage(FArgs args)
     const int tb0 = blockIdx.x * TB;
     float2* buf = bufs + slot * P::BUF;
     float2* rtab = rtabs + slot * P::NROT;
-    uint8_t* inb = inbs + slot * ((F / 2 + 16 + 15) & ~15);
+    uint8_t* inb = inbs + slot * INB;
 
     const double lo = args.sb_lo[sb];
     const double lofrac = dsub(lo, trunc(lo));
-    const bool fraclo = lofrac > 1e-11;                                // kernel.c:39
+    const bool fraclo = lofrac > 1e-11;                                  // kernel.c:39
 
     if constexpr (!P::TWREG) {
         for (int m = tid; m < P::TWQ; m += P::NTHREADS) tq[m] = twiddle_exact(m, F);
@@ -257,37 +266,92 @@ k_fstage(FArgs args)
     __syncthreads();
 
     const uint8_t* row = args.data + ((size_t)sb * args.nant + ant) * args.pitch;
-    const int nsig = args.nant * npol;
+    const int nsig = args.nant * NPOL;
+    constexpr int NITEM = TB * NPOL;
+    const DelayEntry* dtab = args.dtab + (size_t)ant * args.ld + args.t_base;
 
-    for (int item = slot; item < TB * npol; item += P::NSLOT) {
-        const int tl = item / npol;
-        const int pol = item - tl * npol;
+    // Input window of an item (kernel.c:402-409): 16-byte aligned start, one
+    // 128-bit vector per thread at most (F*NPOL/4 + 16 <= 16*NT).
+    auto window = [&](const DelayEntry& d, int& base, int& nvec) {
+        const int first = (NPOL == 2) ? (d.offset >> 1) : (d.offset >> 2);
+        base = first & ~15;
+        nvec = (F * NPOL / 4 + 1 + (first - base) + 15) >> 4;
+    };
+
+    // prefetch of the first item's delay entry and input vector
+    int item = slot;
+    DelayEntry dn;
+    bool vn = false;
+    int basen = 0, nvecn = 0;
+    uint4 pf = make_uint4(0, 0, 0, 0);
+    if (item < NITEM && tb0 + item / NPOL < args.nfft) {
+        dn = dtab[tb0 + item / NPOL];
+        vn = dn.valid != 0;
+    }
+    if (vn) {
+        window(dn, basen, nvecn);
+        if (t < nvecn) pf = __ldg(reinterpret_cast<const uint4*>(row + basen) + t);
+    }
+
+    for (; item < NITEM; item += P::NSLOT) {
+        const int tl = item / NPOL;
+        const int pol = item - tl * NPOL;
         const int tc = tb0 + tl;                    // FFT slot within the chunk
-        DelayEntry d;
-        bool valid = false;
-        if (tc < args.nfft) {
-            d = args.dtab[(size_t)ant * args.ld + args.t_base + tc];
-            valid = d.valid != 0;
+        const DelayEntry d = dn;
+        const bool valid = vn;
+        const int base_byte = basen;
+        if (valid && t < nvecn) reinterpret_cast<uint4*>(inb)[t] = pf;
+        // ---- prefetch the next item of this slot
+        {
+            const int ni = item + P::NSLOT;
+            vn = false;
+            if (ni < NITEM && tb0 + ni / NPOL < args.nfft) {
+                dn = dtab[tb0 + ni / NPOL];
+                vn = dn.valid != 0;
+            }
+            if (vn) {
+                window(dn, basen, nvecn);
+                if (t < nvecn) pf = __ldg(reinterpret_cast<const uint4*>(row + basen) + t);
+            }
         }
         // ---- rotator tables for this FFT (per slot)
         for (int e = t; e < P::NROT; e += NT)
             rtab[e] = valid ? rot_entry<F>(e, d, lo, lofrac, fraclo, args.chan_sub, args.chan_step)
                             : make_float2(0.f, 0.f);
-        // ---- stage packed bytes of this FFT
-        int base_byte = 0;
-        if (valid) base_byte = stage_fft_bytes(row, d.offset, npol, F, inb, t, NT);
         slot_sync<NT>(slot);
 
-        // ---- pass 0: unpack + fringe rotation + radix-16
+        // ---- pass 0: unpack + fringe rotation + radix-16 (samples n = t + r*NT)
         float2 v[16];
         {
+            const int s0 = d.offset + t;
+            const uint8_t* bp;
+            int sh;
+            if constexpr (NPOL == 2) {
+                bp = inb + ((s0 >> 1) - base_byte);
+                sh = 4 * (s0 & 1) + 2 * pol;
+            } else {
+                bp = inb + ((s0 >> 2) - base_byte);
+                sh = 2 * (s0 & 3);
+            }
             const float2* fr_sub = rtab;
             const float2* fr_step = rtab + P::S;
+            float2 sub_c = make_float2(0.f, 0.f);
+            const float2* stp = fr_step;
+            if constexpr (NT % P::S == 0) {
+                sub_c = fr_sub[t % P::S];   // j = n % S is the same for all r
+                stp = fr_step + t / P::S;
+            }
 #pragma unroll
             for (int r = 0; r < 16; r++) {
-                const int n = t + r * NT;
-                const float lv = valid ? decode_sample(inb, base_byte, d.offset + n, npol, pol) : 0.f;
-                const float2 rot = cmul(fr_sub[n % P::S], fr_step[n / P::S]);
+                const uint32_t byte = bp[r * (NT * NPOL / 4)];
+                const float lv = valid ? level2bit((byte >> sh) & 3u) : 0.f;
+                float2 rot;
+                if constexpr (NT % P::S == 0) {
+                    rot = cmul(sub_c, stp[r * (NT / P::S)]);
+                } else {
+                    const int n = t + r * NT;
+                    rot = cmul(fr_sub[n % P::S], fr_step[n / P::S]);
+                }
                 v[r] = make_float2(lv * rot.x, lv * rot.y);
             }
         }
@@ -318,24 +382,27 @@ k_fstage(FArgs args)
         else pass_load<F, 3>(buf, tq, nullptr, v, t);
         pass_dft<F, LP>(v);
 
-        // ---- fractional-sample correction + store of channels [0, C)
+        // ---- fractional-sample correction + store of channels k = j + r*F/R < C
+        constexpr int KSTEP = F / LI::R;
+        static_assert(KSTEP % P::FS == 0, "frac rotator index must fold");
         const float2* fc_sub = rtab + P::S + P::STRIDE;
         const float2* fc_step = fc_sub + P::FS;
-        const int sig = ant * npol + pol;
+        const int sig = ant * NPOL + pol;
 #pragma unroll
         for (int b = 0; b < LI::NB; b++) {
             const int j = t + b * NT;
+            const float2 fsub = fc_sub[j % P::FS];
+            const float2* fst = fc_step + j / P::FS;
 #pragma unroll
             for (int r = 0; r < LI::R / 2; r++) {
-                const int k = j + r * (F / LI::R);
-                const float2 fr = cmul(fc_sub[k % P::FS], fc_step[k / P::FS]);
+                const float2 fr = cmul(fsub, fst[r * (KSTEP / P::FS)]);
                 const float2 y = cmul(fr, v[b * LI::R + r]);
                 if constexpr (MODE == kSpecF32) {
                     float2* out = reinterpret_cast<float2*>(args.spec) +
-                                  (((size_t)sb * nsig + sig) * args.T + tc) * C;
-                    if (tc < args.T) out[k] = y;
+                                  (((size_t)sb * nsig + sig) * args.T + tc) * C + j;
+                    if (tc < args.T) out[r * KSTEP] = y;
                 } else {
-                    stage[(pol * TB + tl) * C + k] = __floats2half2_rn(y.x, y.y);
+                    stage[(pol * TB + tl) * C + j + r * KSTEP] = __floats2half2_rn(y.x, y.y);
                 }
             }
         }
@@ -346,10 +413,10 @@ k_fstage(FArgs args)
         __syncthreads();
         // flush: one (pol, channel) per thread -> Re row and Im row, TB halves each
         __half* spec = reinterpret_cast<__half*>(args.spec);
-        for (int e = tid; e < npol * C; e += P::NTHREADS) {
+        for (int e = tid; e < NPOL * C; e += P::NTHREADS) {
             const int pol = e / C;
             const int k = e - pol * C;
-            const int sig = ant * npol + pol;
+            const int sig = ant * NPOL + pol;
             uint32_t rw[TB / 2], iw[TB / 2];
 #pragma unroll
             for (int q = 0; q < TB / 2; q++) {
@@ -414,18 +481,17 @@ static size_t fstage_smem(int mode, int tb, int npol)
     size_t s = (size_t)P::NSLOT * P::BUF * sizeof(float2);
     if (!P::TWREG) s += (size_t)P::TWQ * sizeof(float2);
     s += (size_t)P::NSLOT * P::NROT * sizeof(float2);
-    s += 4 * P::NSLOT * sizeof(int);
-    s += (size_t)P::NSLOT * ((F / 2 + 16 + 15) & ~15);
+    s += (size_t)P::NSLOT * (F / 2 + 16);
     if (mode == kSpecF16) s += (size_t)npol * tb * P::C * sizeof(__half2);
     return s;
 }
 
-template <int F, int MODE, int TB>
+template <int F, int MODE, int TB, int NPOL>
 static cudaError_t launch_f(const FArgs& a, cudaStream_t st)
 {
     using P = FPlan<F>;
-    const size_t sm = fstage_smem<F>(MODE, TB, a.npol);
-    auto kern = k_fstage<F, MODE, TB>;
+    const size_t sm = fstage_smem<F>(MODE, TB, NPOL);
+    auto kern = k_fstage<F, MODE, TB, NPOL>;
     static unsigned configured = 0;  // per instantiation and device
     cudaError_t e = set_smem_once(kern, sm, &configured);
     if (e != cudaSuccess) return e;
@@ -434,13 +500,19 @@ static cudaError_t launch_f(const FArgs& a, cudaStream_t st)
     return cudaGetLastError();
 }
 
+template <int F, int MODE>
+static cudaError_t launch_fp(const FArgs& a, cudaStream_t st)
+{
+    return a.npol == 2 ? launch_f<F, MODE, 16, 2>(a, st) : launch_f<F, MODE, 16, 1>(a, st);
+}
+
 cudaError_t launch_fstage(int nchan, int mode, const FArgs& a, cudaStream_t st)
 {
     const int F = 2 * nchan;
 #define FX_CASE(FF)                                                            \
     case FF:                                                                   \
-        return mode == kSpecF32 ? launch_f<FF, kSpecF32, 16>(a, st)            \
-                                : launch_f<FF, kSpecF16, 16>(a, st);
+        return mode == kSpecF32 ? launch_fp<FF, kSpecF32>(a, st)               \
+                                : launch_fp<FF, kSpecF16>(a, st);
     switch (F) {
         FX_CASE(256)
         FX_CASE(512)

@@ -331,8 +331,8 @@ k_xtc(const __grid_constant__ CUtensorMap tmap, XArgs a, int* err)
                     const float val = odd ? (g0 - other) : (g0 + other);   // Im = c - b ; Re = a + d
                     if (j >= i && j < nsig) {
                         const int p = i * nsig - (i * (i - 1)) / 2 + (j - i);
-                        float* o = out + 2 * p + (odd ? 1 : 0);
-                        *o += val;
+                        // fire-and-forget reduction: one owner per (channel, pair) and launch
+                        atomicAdd(out + 2 * p + (odd ? 1 : 0), val);
                     }
                 }
             }
