@@ -141,6 +141,70 @@ __device__ __forceinline__ void dft<16>(float2* v)
     for (int i = 0; i < 16; i++) v[i] = t[i];
 }
 
+// Forward DFT of R points keeping only outputs [0, R/2) (in v[0 .. R/2)): the
+// last FFT pass needs channels below nchan = F/2 only.
+template <int R>
+__device__ __forceinline__ void dft_lo(float2* v);
+
+template <>
+__device__ __forceinline__ void dft_lo<2>(float2* v) { v[0] = cadd(v[0], v[1]); }
+
+template <>
+__device__ __forceinline__ void dft_lo<4>(float2* v)
+{
+    const float2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+    const float2 t2 = cadd(v[1], v[3]), t3 = cmul_mi(csub(v[1], v[3]));
+    v[0] = cadd(t0, t2);
+    v[1] = cadd(t1, t3);
+}
+
+template <>
+__device__ __forceinline__ void dft_lo<8>(float2* v)
+{
+    float2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+    float2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+    dft4(e0, e1, e2, e3);
+    dft4(o0, o1, o2, o3);
+    o1 = make_float2((o1.x + o1.y) * kSqrtHalf, (o1.y - o1.x) * kSqrtHalf);
+    o2 = cmul_mi(o2);
+    o3 = make_float2((o3.y - o3.x) * kSqrtHalf, -(o3.x + o3.y) * kSqrtHalf);
+    v[0] = cadd(e0, o0);
+    v[1] = cadd(e1, o1);
+    v[2] = cadd(e2, o2);
+    v[3] = cadd(e3, o3);
+}
+
+template <>
+__device__ __forceinline__ void dft_lo<16>(float2* v)
+{
+#pragma unroll
+    for (int n2 = 0; n2 < 4; n2++) dft4(v[n2], v[n2 + 4], v[n2 + 8], v[n2 + 12]);
+#pragma unroll
+    for (int n2 = 1; n2 < 4; n2++) {
+#pragma unroll
+        for (int k1 = 1; k1 < 4; k1++) {
+            const int m = n2 * k1;
+            if (m == 4) v[n2 + 4 * k1] = cmul_mi(v[n2 + 4 * k1]);
+            else v[n2 + 4 * k1] = cmul(v[n2 + 4 * k1], w16(m));
+        }
+    }
+    // X[k1 + 4*k2] for k2 in {0, 1}: outputs 0 and 1 of the 4-point DFT over n2
+    float2 lo[4], hi[4];
+#pragma unroll
+    for (int k1 = 0; k1 < 4; k1++) {
+        const float2 a0 = v[4 * k1 + 0], a1 = v[4 * k1 + 1], a2 = v[4 * k1 + 2], a3 = v[4 * k1 + 3];
+        const float2 t0 = cadd(a0, a2), t1 = csub(a0, a2);
+        const float2 t2 = cadd(a1, a3), t3 = cmul_mi(csub(a1, a3));
+        lo[k1] = cadd(t0, t2);
+        hi[k1] = cadd(t1, t3);
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < 4; k1++) {
+        v[k1] = lo[k1];
+        v[k1 + 4] = hi[k1];
+    }
+}
+
 // 2-bit code -> quantiser level {-HiMag, -1, +1, +HiMag} (kernel.c:191-200)
 __device__ __forceinline__ float level2bit(uint32_t c)
 {

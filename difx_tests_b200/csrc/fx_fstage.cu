@@ -193,36 +193,41 @@ __device__ __forceinline__ void pass_store(float2* buf, const float2* v, int t)
     }
 }
 
-// Rotator table of one FFT: [fr_sub S][fr_step STRIDE][fc_sub FS][fc_step FST]
+// Rotator table of one FFT: [fr_sub S][fr_step STRIDE][fc_sub FS][fc_step FST].
+// Entries are (cos, sin)(pi * x) with x in half-turns, which needs no
+// large-argument reduction: fringe x = -2 * frac(phase in turns), i.e. the
+// reference's argument -2pi*frac(phase) (kernel.c:463-470) divided by pi;
+// fractional-sample x = the reference's float32 argument (kernel.c:517-523) / pi.
+// Divisions by F are multiplications by the exact power-of-two reciprocal.
+constexpr float kInvPiF = 0.318309886183790671538f;
+
 template <int F>
 __device__ __forceinline__ float2 rot_entry(int e, const DelayEntry& d, double lo, double lofrac, bool fraclo,
-                                            const float* chan_sub, const float* chan_step)
+                                            const float* ctab)
 {
     using P = FPlan<F>;
-    float arg;
+    constexpr double kInvF = 1.0 / F;
+    float x;
     if (e < P::S) {
         // kernel.c:434-466: subphase[j] = lo * (j/F * a + b'), b' = b - (int)b
         const double intdelay = trunc(d.b);
         const double bp = dsub(d.b, intdelay);
-        const double xoff = ddiv((double)e, (double)F);
+        const double xoff = dmul((double)e, kInvF);
         double ph = dmul(dadd(dmul(xoff, d.a), bp), lo);
         if (fraclo) ph = dadd(ph, dmul(lofrac, intdelay));
-        arg = __double2float_rn(dmul(kNeg2Pi, dsub(ph, trunc(ph))));
+        x = __double2float_rn(-2.0 * dsub(ph, trunc(ph)));
     } else if (e < P::S + P::STRIDE) {
         // kernel.c:145, 452, 469: stepphase[i] = lo * (i*stride/F * a)
-        const int i = e - P::S;
-        const double xoff = ddiv(dmul((double)i, (double)P::STRIDE), (double)F);
+        const double xoff = dmul((double)((e - P::S) * P::STRIDE), kInvF);
         const double ph = dmul(dmul(xoff, d.a), lo);
-        arg = __double2float_rn(dmul(kNeg2Pi, dsub(ph, trunc(ph))));
+        x = __double2float_rn(-2.0 * dsub(ph, trunc(ph)));
     } else {
-        // kernel.c:517-523: f32 argument = channel angular frequency * (f32)fracdelay
-        const float fr = __double2float_rn(d.frac);
-        const int i = e - P::S - P::STRIDE;
-        arg = (i < P::FS) ? __fmul_rn(chan_sub[i], fr) : __fmul_rn(chan_step[i - P::FS], fr);
+        const float arg = __fmul_rn(ctab[e - P::S - P::STRIDE], __double2float_rn(d.frac));
+        x = __fmul_rn(arg, kInvPiF);
     }
-    float s, c;
-    sincosf(arg, &s, &c);
-    return make_float2(c, s);
+    float sn, cs;
+    sincospif(x, &sn, &cs);
+    return make_float2(cs, sn);
 }
 
 template <int F, int MODE, int TB, int NPOL>
@@ -237,7 +242,8 @@ k_fstage(FArgs args)
     float2* bufs = reinterpret_cast<float2*>(smem);                   // [NSLOT][BUF]
     float2* tq = bufs + P::NSLOT * P::BUF;                              // [TWQ]
     float2* rtabs = tq + (P::TWREG ? 0 : P::TWQ);                      // [NSLOT][NROT]
-    uint8_t* inbs = reinterpret_cast<uint8_t*>(rtabs + P::NSLOT * P::NROT);  // [NSLOT][INB]
+    float* ctab = reinterpret_cast<float*>(rtabs + P::NSLOT * P::NROT);     // [FS + FST] channel freqs
+    uint8_t* inbs = reinterpret_cast<uint8_t*>(ctab + P::FS + P::FST);      // [NSLOT][INB]
     __half2* stage = reinterpret_cast<__half2*>(inbs + P::NSLOT * INB);       // [NPOL][TB][C]
 
     const int tid = threadIdx.x;
@@ -257,6 +263,8 @@ k_fstage(FArgs args)
     if constexpr (!P::TWREG) {
         for (int m = tid; m < P::TWQ; m += P::NTHREADS) tq[m] = twiddle_exact(m, F);
     }
+    for (int i = tid; i < P::FS + P::FST; i += P::NTHREADS)
+        ctab[i] = i < P::FS ? args.chan_sub[i] : args.chan_step[i - P::FS];
     PassTw<F, 1> tw1;
     PassTw<F, (P::NPASS > 2 ? 2 : 1)> tw2;
     if constexpr (P::TWREG) {
@@ -316,21 +324,23 @@ k_fstage(FArgs args)
         }
         // ---- rotator tables for this FFT (per slot)
         for (int e = t; e < P::NROT; e += NT)
-            rtab[e] = valid ? rot_entry<F>(e, d, lo, lofrac, fraclo, args.chan_sub, args.chan_step)
-                            : make_float2(0.f, 0.f);
+            rtab[e] = valid ? rot_entry<F>(e, d, lo, lofrac, fraclo, ctab) : make_float2(0.f, 0.f);
         slot_sync<NT>(slot);
 
         // ---- pass 0: unpack + fringe rotation + radix-16 (samples n = t + r*NT)
         float2 v[16];
         {
-            const int s0 = d.offset + t;
+            // an invalid item reads from the start of the staging buffer (in range;
+            // its rotator is zero, so the levels do not matter)
+            const int s0 = valid ? d.offset + t : t;
+            const int b0 = valid ? base_byte : 0;
             const uint8_t* bp;
             int sh;
             if constexpr (NPOL == 2) {
-                bp = inb + ((s0 >> 1) - base_byte);
+                bp = inb + ((s0 >> 1) - b0);
                 sh = 4 * (s0 & 1) + 2 * pol;
             } else {
-                bp = inb + ((s0 >> 2) - base_byte);
+                bp = inb + ((s0 >> 2) - b0);
                 sh = 2 * (s0 & 3);
             }
             const float2* fr_sub = rtab;
@@ -344,7 +354,7 @@ k_fstage(FArgs args)
 #pragma unroll
             for (int r = 0; r < 16; r++) {
                 const uint32_t byte = bp[r * (NT * NPOL / 4)];
-                const float lv = valid ? level2bit((byte >> sh) & 3u) : 0.f;
+                const float lv = level2bit((byte >> sh) & 3u);
                 float2 rot;
                 if constexpr (NT % P::S == 0) {
                     rot = cmul(sub_c, stp[r * (NT / P::S)]);
@@ -380,7 +390,8 @@ k_fstage(FArgs args)
         if constexpr (LP == 1) pass_load<F, 1>(buf, tq, &tw1, v, t);
         else if constexpr (LP == 2) pass_load<F, 2>(buf, tq, &tw2, v, t);
         else pass_load<F, 3>(buf, tq, nullptr, v, t);
-        pass_dft<F, LP>(v);
+#pragma unroll
+        for (int b = 0; b < LI::NB; b++) dft_lo<LI::R>(v + b * LI::R);   // outputs r < R/2 only
 
         // ---- fractional-sample correction + store of channels k = j + r*F/R < C
         constexpr int KSTEP = F / LI::R;
@@ -454,8 +465,11 @@ __global__ void k_unpack_debug(FArgs args, float* out)
     __syncthreads();
     for (int pol = 0; pol < npol; pol++) {
         float* o = out + ((((size_t)sb * args.nant + ant) * npol + pol) * args.nfft + tc) * F;
-        for (int n = threadIdx.x; n < F; n += blockDim.x)
-            o[n] = d.valid ? decode_sample(inb, base_byte, d.offset + n, npol, pol) : 0.f;
+        for (int n = threadIdx.x; n < F; n += blockDim.x) {
+            float lv = 0.f;
+            if (d.valid) lv = decode_sample(inb, base_byte, d.offset + n, npol, pol);
+            o[n] = lv;
+        }
     }
 }
 
@@ -481,6 +495,7 @@ static size_t fstage_smem(int mode, int tb, int npol)
     size_t s = (size_t)P::NSLOT * P::BUF * sizeof(float2);
     if (!P::TWREG) s += (size_t)P::TWQ * sizeof(float2);
     s += (size_t)P::NSLOT * P::NROT * sizeof(float2);
+    s += (size_t)(P::FS + P::FST) * sizeof(float);
     s += (size_t)P::NSLOT * (F / 2 + 16);
     if (mode == kSpecF16) s += (size_t)npol * tb * P::C * sizeof(__half2);
     return s;
