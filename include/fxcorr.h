@@ -130,6 +130,28 @@ int fxc_synchronize(fxc_ctx* ctx);
 int fxc_host_alloc(void** p, size_t bytes);
 int fxc_host_free(void* p);
 
+/* One-shot correlation that allocates no memory.  No counterpart in the
+ * reference: it is for callers that cannot call cudaMalloc at the point where
+ * they correlate -- code inside a CUDA stream capture (allocation is not
+ * capturable), real-time paths that must not take the allocator's locks or
+ * latency, and hosts whose device memory another framework reserved up front.
+ * The caller passes the input (device rows as for fxc_process_device, host
+ * delay model) and the outputs it owns: d_vis (fxc_vis_count complex values,
+ * layout of fxc_get_visibilities) and optionally d_counts (nbl + nant ints).
+ * Every intermediate lives in one static device array of
+ * FXC_NOALLOC_SCRATCH_BYTES that each GPU loading this library holds until the
+ * process exits; a problem whose delay table, accumulators and at least 64 FFT
+ * slots of spectra do not fit returns FXC_ERR_INVALID.  Plain FP32 X stage only
+ * (FXC_ERR_UNSUPPORTED otherwise).  Work is queued on `stream` (a cudaStream_t,
+ * NULL = legacy default stream); the call returns before it completes.
+ * The first call on a device looks up the array's device address, so make it
+ * before any stream capture starts.  All calls share the array: calls that
+ * overlap on the GPU race, so order them (one stream, or events). */
+#define FXC_NOALLOC_SCRATCH_BYTES (64u << 20)
+int fxc_correlate_noalloc(const fxc_config* cfg, const uint8_t* d_data, size_t pitch, const double* delays,
+                          const double* fileoffsets, int first_fft, int nfft, float* d_vis, int* d_counts,
+                          int normalize, void* stream);
+
 /* Per-stage device timing (the counterpart of the reference's per-stage clock()
  * timers, kernel.c:720-821).  With enable != 0 every launch is bracketed by CUDA
  * events on the context's stream.  fxc_stage_times waits for the stream and
