@@ -7,7 +7,11 @@ subintegration = 31250 FFTs per subband at 128 MS/s, 2-bit real samples.
 One step = one subintegration (all subbands) through the whole hot path:
 delay table, fused unpack/shift/fringe/FFT/fractional-sample F stage, X stage.
 
-  python bench.py [--gpus N --steps K --warmup W] [--xmode tc|plain] [--impl reference]
+  python bench.py [--gpus N --steps K --warmup W] [--xmode both|tc|plain] [--impl reference]
+
+The headline `value` is the tensor-core form (FP32 F stage, FP16 X inputs with
+FP32 accumulation); the FP32 plain form runs on the same input in the same
+invocation and is reported under "plain".
 
 Under torchrun (N > 1) every rank correlates its own subintegration (weak
 scaling, no data-path collective) and rank 0 prints one JSON line; time is the
@@ -279,6 +283,66 @@ def run_reference_arm(args):
 
 
 # ------------------------------------------------------------------ GPU arm
+# DRAM bytes per input sample of the F stage's FP16 (tensor-core) variant,
+# dram__bytes_read.sum + dram__bytes_write.sum from one ncu capture of
+# k_fstage<2048,1,16,1> on the 64-antenna x 1024-channel profiling case, divided
+# by the samples of that launch (profiles/kernels_cfg2s_ncu_full.txt).
+FSTAGE_TC_DRAM_BYTES_PER_SAMPLE = 2.19
+
+
+def time_form(torch, dist, fx, w, xmode, data, pitch, delays, offs, steps, warmup, world, dev, stream):
+    """Warm up, then time `steps` subintegrations of one X form; returns a result dict."""
+    F = 2 * w["nchan"]
+    nsig = w["nant"] * w["npol"]
+    cfg = fx.make_config(w["nant"], w["nchan"], w["numffts"], w["bw"], w["lo"], npol=w["npol"], nsubband=w["nsb"],
+                         xmode=xmode)
+    corr = fx.Correlator(cfg)
+    corr.set_stream(stream.cuda_stream)
+    samples = w["nant"] * w["npol"] * w["nsb"] * w["numffts"] * F
+
+    def step():
+        corr.reset()
+        corr.process_device(data.data_ptr(), pitch, delays, offs)
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    corr.enable_stage_timing(True)
+    corr.stage_times(reset=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dev.index)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    stage_ms, launches = corr.stage_times(reset=True)
+    corr.enable_stage_timing(False)
+    ms_t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    f_launches = max(1, int(launches[1]))
+    x_launches = max(1, int(launches[2]))
+    ffts_per_launch = w["numffts"] * steps / f_launches
+    samples_per_launch = nsig * w["nsb"] * ffts_per_launch * F
+    x_flop_step = 8.0 * w["nchan"] * w["numffts"] * w["nsb"] * nsig * (nsig + 1) / 2   # Hermitian incl. autos
+    return dict(corr=corr, cfg=cfg, ms_max=ms_max, value=world * samples * steps / (ms_max / 1e3) / 1e9,
+                stage_ms=stage_ms, launches=launches, clocks=clk, samples=samples,
+                f_ms_launch=stage_ms[1] / f_launches, x_ms_launch=stage_ms[2] / x_launches,
+                samples_per_launch=samples_per_launch, ffts_per_launch=ffts_per_launch,
+                x_tflops=x_flop_step * steps / (stage_ms[2] / 1e3) / 1e12, x_flop_step=x_flop_step)
+
+
 def run_gpu_arm(args):
     import torch
     import torch.distributed as dist
@@ -295,126 +359,100 @@ def run_gpu_arm(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
 
     w = WORKLOADS[args.workload]
-    xmode = fx.FXC_X_TC_FP16 if args.xmode == "tc" else fx.FXC_X_PLAIN_FP32
     F = 2 * w["nchan"]
     nsig = w["nant"] * w["npol"]
-    cfg = fx.make_config(w["nant"], w["nchan"], w["numffts"], w["bw"], w["lo"], npol=w["npol"], nsubband=w["nsb"],
-                         xmode=xmode)
-    corr = fx.Correlator(cfg)
-    subint = corr.subint_bytes
-    dptr, pitch = corr.device_input()
+    probe = fx.make_config(w["nant"], w["nchan"], w["numffts"], w["bw"], w["lo"], npol=w["npol"], nsubband=w["nsb"])
+    subint = fx.lib().fxc_subint_bytes(probe)
+    pitch = (subint + 16 + 255) // 256 * 256
     delays, offs = delay_model(w["nant"], w["nchan"], w["bw"], seed=42 + rank)
-    data = gen_device_data(torch, w["nsb"], w["nant"], w["npol"], subint, pitch, w["rho"], seed=1000 + rank,
-                           device=dev)
-    # a dedicated (non-default) stream: the correlator's kernels and the timing
-    # events are then ordered on the same stream
+    # a dedicated (non-default) stream: the correlator's kernels and the timing events share it
     stream = torch.cuda.Stream(device=dev)
     torch.cuda.set_stream(stream)
+    data = gen_device_data(torch, w["nsb"], w["nant"], w["npol"], subint, pitch, w["rho"], seed=1000 + rank,
+                           device=dev)
     torch.cuda.synchronize()
-    corr.set_stream(stream.cuda_stream)
-    samples_per_step = w["nant"] * w["npol"] * w["nsb"] * w["numffts"] * F
 
-    def step():
-        corr.reset()
-        corr.process_device(data.data_ptr(), pitch, delays, offs)
+    forms = ["tc", "plain"] if args.xmode == "both" else [args.xmode]
+    res = {}
+    for form in forms:
+        xm = fx.FXC_X_TC_FP16 if form == "tc" else fx.FXC_X_PLAIN_FP32
+        res[form] = time_form(torch, dist, fx, w, xm, data, pitch, delays, offs, args.steps, args.warmup, world, dev,
+                              stream)
+        if form != forms[0]:
+            res[form]["corr"].close()
+    head = res[forms[0]]
+    xmode = fx.FXC_X_TC_FP16 if forms[0] == "tc" else fx.FXC_X_PLAIN_FP32
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    corr.enable_stage_timing(True)
-    corr.stage_times(reset=True)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    clocks = ClockSampler(local)
-    clocks.start()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        step()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    stage_ms, launches = corr.stage_times(reset=True)
-    corr.enable_stage_timing(False)
-    ms_t = torch.tensor([ms], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
-    value = world * samples_per_step * args.steps / (ms_max / 1e3) / 1e9
-
-    # ---- roofline of the dominant kernel (per-launch averages over the timed region)
+    # ---- roofline of the dominant kernel of the headline form (the F stage)
     hbm, tc_peak, peak_kind = peaks()
-    f_launches = max(1, int(launches[1]))
-    x_launches = max(1, int(launches[2]))
-    f_ms = stage_ms[1] / f_launches
-    x_ms = stage_ms[2] / x_launches
-    T = corr_T = int(math.ceil(w["numffts"] / f_launches * args.steps))  # FFT slots per launch (approx.)
-    ffts_per_launch = w["numffts"] * args.steps / f_launches
-    in_bytes = nsig * w["nsb"] * ffts_per_launch * F / 4.0            # 2-bit packed input
-    spec_bpc = 8 if xmode == fx.FXC_X_PLAIN_FP32 else 4                # bytes per complex spectrum value
-    out_bytes = nsig * w["nsb"] * ffts_per_launch * w["nchan"] * spec_bpc
-    f_gbs = (in_bytes + out_bytes) / (f_ms / 1e3) / 1e9
-    x_flop = 8.0 * w["nchan"] * ffts_per_launch * w["nsb"] * nsig * (nsig + 1) / 2   # Hermitian incl. autos
-    x_tflops = x_flop / (x_ms / 1e3) / 1e12
-    if stage_ms[1] >= stage_ms[2] or xmode == fx.FXC_X_PLAIN_FP32:
-        roof = {"kernel": "k_fstage (fused unpack/shift/fringe/FFT/frac)", "bound": "hbm", "achieved": f_gbs,
-                "peak": hbm, "unit": "GB/s", "frac": f_gbs / hbm, "traffic": None,
-                "peak_source": peak_kind, "share": stage_ms[1] / max(1e-9, stage_ms.sum())}
-    else:
-        roof = {"kernel": "k_xtc (tcgen05 X stage)", "bound": "tensor", "achieved": x_tflops, "peak": tc_peak,
-                "unit": "TFLOP/s", "frac": x_tflops / tc_peak, "traffic": None, "peak_source": peak_kind,
-                "share": stage_ms[2] / max(1e-9, stage_ms.sum())}
-    del T, corr_T
+    spec_bpc = 4 if xmode == fx.FXC_X_TC_FP16 else 8          # bytes per complex spectrum value written
+    f_bytes = head["samples_per_launch"] * (0.25 + 0.5 * spec_bpc)
+    f_gbs = f_bytes / (head["f_ms_launch"] / 1e3) / 1e9
+    sm = head["stage_ms"]
+    traffic = (FSTAGE_TC_DRAM_BYTES_PER_SAMPLE * head["samples_per_launch"]
+               if xmode == fx.FXC_X_TC_FP16 and args.workload.startswith("cfg2") else None)
+    roof = {"kernel": "k_fstage (fused unpack/shift/fringe/FFT/frac-delay)", "bound": "hbm", "achieved": f_gbs,
+            "peak": hbm, "unit": "GB/s", "frac": f_gbs / hbm, "traffic": traffic,
+            "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
+            "algorithmic_bytes_per_launch": f_bytes, "launch_ms": head["f_ms_launch"],
+            "share": sm[1] / max(1e-9, sm.sum()),
+            "note": "F stage is FP32-issue-bound; HBM fraction shown for its algorithmic bytes"}
 
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32" if xmode == fx.FXC_X_PLAIN_FP32 else "f32 F / f16 X",
-        "data": "synthetic (seeded, on device)",
-        "config": {"workload": w["desc"], "xmode": args.xmode, "parallelism": f"replicas x{world}",
-                   "l2": "inputs (8.2 GB packed at cfg2) larger than L2; no flush",
-                   "chunk_ffts": int(round(ffts_per_launch))},
-        "stages_ms_per_step": {"delay+counts": stage_ms[0] / args.steps, "F": stage_ms[1] / args.steps,
-                               "X": stage_ms[2] / args.steps},
-        "x_stage": {"tflops": x_tflops, "flop_per_step": 8.0 * w["nchan"] * w["numffts"] * w["nsb"] * nsig *
-                    (nsig + 1) / 2},
+        "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["ms_max"] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 F stage / f16 X inputs, f32 accumulate" if xmode == fx.FXC_X_TC_FP16 else "f32",
+        "data": "synthetic (seeded, generated on device)",
+        "config": {"workload": w["desc"], "form": forms[0], "parallelism": f"replicas x{world}",
+                   "l2": "inputs (8.2 GB packed per step at cfg2) exceed L2; no flush",
+                   "chunk_ffts": int(round(head["ffts_per_launch"]))},
+        "stages_ms_per_step": {"delay+counts": sm[0] / args.steps, "F": sm[1] / args.steps,
+                               "X": sm[2] / args.steps},
+        "x_stage": {"tflops": head["x_tflops"], "flop_per_step": head["x_flop_step"],
+                    "ms_per_step": sm[2] / args.steps},
         "roofline": roof,
-        "clocks": clk,
-        "gpu_launches": int(launches.sum()),
+        "clocks": head["clocks"],
+        "gpu_launches": int(head["launches"].sum()),
     }
+    if "plain" in res and forms[0] != "plain":
+        p = res["plain"]
+        line["plain"] = {"value": p["value"], "unit": UNIT, "ms_per_step": p["ms_max"] / args.steps,
+                         "stages_ms_per_step": {"F": p["stage_ms"][1] / args.steps, "X": p["stage_ms"][2] / args.steps},
+                         "x_tflops": p["x_tflops"], "clocks": p["clocks"]}
+        line["tc_vs_plain"] = {"gsamps": head["value"] / p["value"],
+                               "x_stage_only": (p["stage_ms"][2] / max(1e-9, sm[2]))}
 
+    corr = head["corr"]
     # ---- end to end through the C ABI with pinned host buffers (rank-local)
     if not args.no_e2e:
         host = torch.empty((w["nsb"] * w["nant"], subint), dtype=torch.uint8, pin_memory=True)
         host.copy_(data[:, :subint])
-        rows = host.numpy()
+        torch.cuda.synchronize()
+        rows = host.numpy().reshape(w["nsb"], w["nant"], subint)
         vis_n = w["nsb"] * (w["nant"] * (w["nant"] - 1) // 2 + w["nant"]) * w["npol"] ** 2 * w["nchan"]
         e2e_steps = max(1, min(args.steps, 3))
-        corr.process(rows.reshape(w["nsb"], w["nant"], subint), delays, offs)   # warm
+        corr.process(rows, delays, offs)   # warm
         corr.visibilities()
-        corr.reset()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(e2e_steps):
             corr.reset()
-            corr.process(rows.reshape(w["nsb"], w["nant"], subint), delays, offs)
+            corr.process(rows, delays, offs)
             corr.visibilities()
         t = (time.perf_counter() - t0) / e2e_steps
         t_t = torch.tensor([t], device=dev, dtype=torch.float64)
         if world > 1:
             dist.all_reduce(t_t, op=dist.ReduceOp.MAX)
-        line["e2e"] = {"value": world * samples_per_step / float(t_t.item()) / 1e9, "unit": UNIT,
+        line["e2e"] = {"value": world * head["samples"] / float(t_t.item()) / 1e9, "unit": UNIT,
                        "h2d_bytes_per_step": int(w["nsb"] * w["nant"] * subint),
-                       "d2h_bytes_per_step": int(vis_n * 8 + 4 * (w["nant"] * (w["nant"] + 1) // 2)),
-                       "steps": e2e_steps, "ms_per_step": 1e3 * float(t_t.item())}
+                       "d2h_bytes_per_step": int(vis_n * 8 + 4 * (w["nant"] * (w["nant"] - 1) // 2 + w["nant"])),
+                       "steps": e2e_steps, "ms_per_step": 1e3 * float(t_t.item()),
+                       "path": "fxc_process_host + fxc_get_visibilities, pinned host buffers"}
 
     if rank == 0 and not args.no_accuracy:
-        line["accuracy"] = accuracy_sample(w, xmode)
+        line["accuracy"] = {f: accuracy_sample(w, fx.FXC_X_TC_FP16 if f == "tc" else fx.FXC_X_PLAIN_FP32)
+                            for f in forms}
     if rank == 0 and world == 1 and not args.no_cpu:
         cb = cpu_baseline_one_core()
         if cb is not None:
@@ -435,7 +473,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS))
-    ap.add_argument("--xmode", default="plain", choices=["plain", "tc"])
+    ap.add_argument("--xmode", default="both", choices=["both", "tc", "plain"],
+                    help="both: the tensor-core form is the headline value, FP32 plain timed beside it")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
