@@ -76,7 +76,8 @@ SIGNATURES = {
     "fxc_synchronize": (_I, [_P]),
     "fxc_host_alloc": (_I, [C.POINTER(_P), C.c_size_t]),
     "fxc_host_free": (_I, [_P]),
-    "fxc_correlate_noalloc": (_I, [C.POINTER(FxcConfig), _P, C.c_size_t, _DP, _DP, _I, _I, _P, _P, _I, _P]),
+    "fxc_compat_last_error": (_I, []),
+    "fxc_correlate_noalloc":(_I, [C.POINTER(FxcConfig), _P, C.c_size_t, _DP, _DP, _I, _I, _P, _P, _I, _P]),
     "fxc_enable_stage_timing": (_I, [_P, _I]),
     "fxc_stage_times": (_I, [_P, _DP, C.POINTER(C.c_longlong), _I]),
     "fxc_strerror": (C.c_char_p, [_I]),
