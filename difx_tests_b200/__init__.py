@@ -80,6 +80,18 @@ SIGNATURES = {
     "fxc_correlate_noalloc":(_I, [C.POINTER(FxcConfig), _P, C.c_size_t, _DP, _DP, _I, _I, _P, _P, _I, _P]),
     "fxc_enable_stage_timing": (_I, [_P, _I]),
     "fxc_stage_times": (_I, [_P, _DP, C.POINTER(C.c_longlong), _I]),
+    "fxc_batch_create": (_I, [C.POINTER(FxcConfig), _I, C.POINTER(_P)]),
+    "fxc_batch_destroy": (None, [_P]),
+    "fxc_batch_upload": (_I, [_P, _I, C.POINTER(_P)]),
+    "fxc_batch_set_model": (_I, [_P, _I, _DP, _DP]),
+    "fxc_batch_process": (_I, [_P]),
+    "fxc_batch_reset": (_I, [_P]),
+    "fxc_batch_get_visibilities": (_I, [_P, _I, _FP, _IP, _I]),
+    "fxc_batch_autotune": (_I, [_P, _I]),
+    "fxc_batch_get_plan": (_I, [_P, _I, _IP, _IP]),
+    "fxc_batch_set_stream": (_I, [_P, _P]),
+    "fxc_batch_synchronize": (_I, [_P]),
+    "fxc_batch_use_graph": (_I, [_P, _I]),
     "fxc_strerror": (C.c_char_p, [_I]),
     "fxc_last_cuda_error": (_I, []),
     "fxc_last_device_error": (_I, []),
@@ -264,3 +276,78 @@ class Correlator:
         _check(_lib().fxc_debug_spectra(self._ctx, _dp(d), _dp(o), first_fft, nfft, out.ctypes.data_as(_FP)),
                "fxc_debug_spectra")
         return out.view(np.complex64)
+
+
+class Batch:
+    """Many independent correlation jobs (each its own FxcConfig, plain FP32 X
+    form) processed by grouped persistent launches, replayed as one CUDA graph
+    after the first call (fxc_batch_* of include/fxcorr.h)."""
+
+    def __init__(self, cfgs):
+        self.cfgs = list(cfgs)
+        arr = (FxcConfig * len(self.cfgs))(*self.cfgs)
+        self._b = _P()
+        _check(_lib().fxc_batch_create(arr, len(self.cfgs), C.byref(self._b)), "fxc_batch_create")
+
+    def close(self):
+        if self._b:
+            _lib().fxc_batch_destroy(self._b)
+            self._b = _P()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, job, data):
+        cfg = self.cfgs[job]
+        data = np.ascontiguousarray(data, dtype=np.uint8)
+        rows = [data[s, a] for s in range(cfg.nsubband) for a in range(cfg.nant)]
+        ptrs = (_P * len(rows))(*[r.ctypes.data for r in rows])
+        _check(_lib().fxc_batch_upload(self._b, job, ptrs), "fxc_batch_upload")
+
+    def set_model(self, job, delays, fileoffsets):
+        d = np.ascontiguousarray(delays, np.float64).reshape(-1)
+        o = np.ascontiguousarray(fileoffsets, np.float64)
+        _check(_lib().fxc_batch_set_model(self._b, job, _dp(d), _dp(o)), "fxc_batch_set_model")
+
+    def process(self):
+        _check(_lib().fxc_batch_process(self._b), "fxc_batch_process")
+
+    def reset(self):
+        _check(_lib().fxc_batch_reset(self._b), "fxc_batch_reset")
+
+    def synchronize(self):
+        _check(_lib().fxc_batch_synchronize(self._b), "fxc_batch_synchronize")
+
+    def set_stream(self, stream_ptr):
+        _check(_lib().fxc_batch_set_stream(self._b, _P(stream_ptr)), "fxc_batch_set_stream")
+
+    def use_graph(self, on=True):
+        _check(_lib().fxc_batch_use_graph(self._b, 1 if on else 0), "fxc_batch_use_graph")
+
+    def autotune(self, reps=3):
+        _check(_lib().fxc_batch_autotune(self._b, reps), "fxc_batch_autotune")
+
+    def plan(self, job):
+        tb, alt = C.c_int(), C.c_int()
+        _check(_lib().fxc_batch_get_plan(self._b, job, C.byref(tb), C.byref(alt)), "fxc_batch_get_plan")
+        return tb.value, alt.value
+
+    def visibilities(self, job, normalize=False):
+        cfg = self.cfgs[job]
+        nbl = cfg.nant * (cfg.nant - 1) // 2
+        n = cfg.nsubband * (nbl + cfg.nant) * cfg.npol ** 2 * cfg.nchan
+        out = np.empty(2 * n, dtype=np.float32)
+        counts = np.empty(nbl + cfg.nant, dtype=np.int32)
+        _check(_lib().fxc_batch_get_visibilities(self._b, job, out.ctypes.data_as(_FP), counts.ctypes.data_as(_IP),
+                                                 1 if normalize else 0), "fxc_batch_get_visibilities")
+        vis = out.view(np.complex64).reshape(cfg.nsubband, nbl + cfg.nant, cfg.npol ** 2, cfg.nchan)
+        return vis, counts

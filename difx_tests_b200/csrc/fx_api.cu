@@ -8,57 +8,12 @@
 #include <vector>
 
 #include "../../include/fxcorr.h"
+#include "fx_ctx.h"
 #include "fx_internal.h"
 #include "fx_kernels.h"
 
 using namespace fx;
 
-struct fxc_ctx {
-    fxc_config cfg;
-    int device = 0;
-    int F = 0, nsig = 0, npair = 0, npair_ant = 0, nbl = 0, nout = 0;
-    int ld = 0;            // delay-table leading dimension (FFTs, multiple of 128)
-    int T = 0;             // FFT slots per chunk (multiple of 64)
-    int rows = 0;          // F16 spectra rows per channel
-    size_t pitch = 0;      // input row pitch
-    size_t subint = 0;
-    cudaStream_t own_stream = nullptr;
-    cudaStream_t stream = nullptr;
-    uint8_t* d_in = nullptr;
-    double* d_delays = nullptr;
-    double* d_offs = nullptr;
-    double* d_sblo = nullptr;
-    float* d_chan_sub = nullptr;
-    float* d_chan_step = nullptr;
-    DelayEntry* d_dtab = nullptr;
-    uint32_t* d_vbits = nullptr;
-    void* d_spec = nullptr;
-    size_t spec_bytes = 0;
-    float2* d_acc = nullptr;
-    size_t acc_bytes = 0;
-    int* d_counts = nullptr;
-    int* d_err = nullptr;   // device-side wait expiry code of the tensor-core X stage
-    int nsm = 148;
-    // delay-model upload: [3*nant delays | nant file offsets], pinned ring
-    static constexpr int NRING = 4;
-    double* h_stage = nullptr;
-    cudaEvent_t stage_ev[NRING] = {};
-    int stage_next = 0;
-    std::vector<double> last_model;
-    bool model_valid = false;
-    float2* d_vis = nullptr;
-    size_t vis_bytes = 0;
-    // stage timing (fxc_enable_stage_timing / fxc_stage_times)
-    bool timing = false;
-    struct Pending {
-        int stage;
-        cudaEvent_t a, b;
-    };
-    std::vector<Pending> pending;
-    std::vector<cudaEvent_t> event_pool;
-    double stage_ms[FXC_NSTAGE] = {0, 0, 0, 0};
-    long long stage_launches[FXC_NSTAGE] = {0, 0, 0, 0};
-};
 
 namespace {
 
@@ -366,8 +321,10 @@ int fxc_host_free(void* p)
     return FXC_OK;
 }
 
+}  // extern "C"
+
 // delays / offsets to the device, then K0 over FFTs first..first+nfft-1
-static int run_delay_table(fxc_ctx* x, const double* delays, const double* offs, int first, int nfft, int* ld_out)
+int ctx_run_delay_table(fxc_ctx* x, const double* delays, const double* offs, int first, int nfft, int* ld_out)
 {
     const fxc_config& c = x->cfg;
     if (!delays || !offs || first < 0 || nfft < 1 || (long long)first + nfft > c.numffts) return FXC_ERR_INVALID;
@@ -403,7 +360,7 @@ static int run_delay_table(fxc_ctx* x, const double* delays, const double* offs,
     return FXC_OK;
 }
 
-static FArgs make_fargs(fxc_ctx* x, const uint8_t* d_data, size_t pitch, int ld)
+FArgs ctx_fargs(fxc_ctx* x, const uint8_t* d_data, size_t pitch, int ld)
 {
     FArgs a;
     std::memset(&a, 0, sizeof(a));
@@ -423,6 +380,8 @@ static FArgs make_fargs(fxc_ctx* x, const uint8_t* d_data, size_t pitch, int ld)
     return a;
 }
 
+extern "C" {
+
 int fxc_process_device(fxc_ctx* x, const uint8_t* d_data, size_t pitch, const double* delays,
                        const double* offs, int first, int nfft)
 {
@@ -431,12 +390,12 @@ int fxc_process_device(fxc_ctx* x, const uint8_t* d_data, size_t pitch, const do
     int ld = 0;
     {
         StageScope sc(x, 0, 2);
-        int st = run_delay_table(x, delays, offs, first, nfft, &ld);
+        int st = ctx_run_delay_table(x, delays, offs, first, nfft, &ld);
         if (st != FXC_OK) return st;
         FXC_CK(launch_counts(x->d_vbits, x->cfg.nant, ld / 32, x->d_counts, x->stream));
     }
     const bool tc = x->cfg.xmode == FXC_X_TC_FP16;
-    FArgs fa = make_fargs(x, d_data, pitch, ld);
+    FArgs fa = ctx_fargs(x, d_data, pitch, ld);
     XArgs xa;
     xa.spec = x->d_spec;
     xa.acc = x->d_acc;
@@ -552,7 +511,7 @@ int fxc_debug_delay_table(fxc_ctx* x, const double* delays, const double* offs, 
     if (!x) return FXC_ERR_INVALID;
     FXC_CK(cudaSetDevice(x->device));
     int ld = 0;
-    int st = run_delay_table(x, delays, offs, first, nfft, &ld);
+    int st = ctx_run_delay_table(x, delays, offs, first, nfft, &ld);
     if (st != FXC_OK) return st;
     const int A = x->cfg.nant;
     std::vector<DelayEntry> h((size_t)A * ld);
@@ -576,13 +535,13 @@ int fxc_debug_unpack(fxc_ctx* x, const double* delays, const double* offs, int f
     if (!x || !out) return FXC_ERR_INVALID;
     FXC_CK(cudaSetDevice(x->device));
     int ld = 0;
-    int st = run_delay_table(x, delays, offs, first, nfft, &ld);
+    int st = ctx_run_delay_table(x, delays, offs, first, nfft, &ld);
     if (st != FXC_OK) return st;
     const fxc_config& c = x->cfg;
     const size_t n = (size_t)c.nsubband * c.nant * c.npol * nfft * x->F;
     float* d = nullptr;
     FXC_CK(cudaMalloc(&d, n * sizeof(float)));
-    FArgs fa = make_fargs(x, x->d_in, x->pitch, ld);
+    FArgs fa = ctx_fargs(x, x->d_in, x->pitch, ld);
     fa.t_base = 0;
     fa.nfft = nfft;
     cudaError_t e = launch_unpack_debug(c.nchan, fa, d, x->stream);
@@ -598,14 +557,14 @@ int fxc_debug_spectra(fxc_ctx* x, const double* delays, const double* offs, int 
     if (!x || !out || nfft > x->T) return FXC_ERR_INVALID;
     FXC_CK(cudaSetDevice(x->device));
     int ld = 0;
-    int st = run_delay_table(x, delays, offs, first, nfft, &ld);
+    int st = ctx_run_delay_table(x, delays, offs, first, nfft, &ld);
     if (st != FXC_OK) return st;
     const fxc_config& c = x->cfg;
     const int T = (int)round_up((size_t)nfft, 64);
     const size_t n = (size_t)c.nsubband * x->nsig * T * c.nchan;
     float2* d = nullptr;
     FXC_CK(cudaMalloc(&d, n * sizeof(float2)));
-    FArgs fa = make_fargs(x, x->d_in, x->pitch, ld);
+    FArgs fa = ctx_fargs(x, x->d_in, x->pitch, ld);
     fa.t_base = 0;
     fa.nfft = nfft;
     fa.T = T;

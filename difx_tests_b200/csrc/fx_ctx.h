@@ -1,0 +1,62 @@
+// fx_ctx.h -- the correlation context behind the C ABI (internal; shared by
+// fx_api.cu and the multi-job batch in fx_batch.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "../../include/fxcorr.h"
+#include "fx_internal.h"
+
+struct fxc_ctx {
+    fxc_config cfg;
+    int device = 0;
+    int F = 0, nsig = 0, npair = 0, npair_ant = 0, nbl = 0, nout = 0;
+    int ld = 0;            // delay-table leading dimension (FFTs, multiple of 128)
+    int T = 0;             // FFT slots per chunk (multiple of 64)
+    int rows = 0;          // F16 spectra rows per channel
+    size_t pitch = 0;      // input row pitch
+    size_t subint = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    uint8_t* d_in = nullptr;
+    double* d_delays = nullptr;
+    double* d_offs = nullptr;
+    double* d_sblo = nullptr;
+    float* d_chan_sub = nullptr;
+    float* d_chan_step = nullptr;
+    fx::DelayEntry* d_dtab = nullptr;
+    uint32_t* d_vbits = nullptr;
+    void* d_spec = nullptr;
+    size_t spec_bytes = 0;
+    float2* d_acc = nullptr;
+    size_t acc_bytes = 0;
+    int* d_counts = nullptr;
+    int* d_err = nullptr;   // device-side wait expiry code of the tensor-core X stage
+    int nsm = 148;
+    // delay-model upload: [3*nant delays | nant file offsets], pinned ring
+    static constexpr int NRING = 4;
+    double* h_stage = nullptr;
+    cudaEvent_t stage_ev[NRING] = {};
+    int stage_next = 0;
+    std::vector<double> last_model;
+    bool model_valid = false;
+    float2* d_vis = nullptr;
+    size_t vis_bytes = 0;
+    // stage timing (fxc_enable_stage_timing / fxc_stage_times)
+    bool timing = false;
+    struct Pending {
+        int stage;
+        cudaEvent_t a, b;
+    };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> event_pool;
+    double stage_ms[FXC_NSTAGE] = {0, 0, 0, 0};
+    long long stage_launches[FXC_NSTAGE] = {0, 0, 0, 0};
+};
+
+// delay model to the device (only when it changed) + K0 over FFTs first..first+nfft-1
+int ctx_run_delay_table(fxc_ctx* x, const double* delays, const double* offs, int first, int nfft, int* ld_out);
+// F-stage arguments of this context for device input rows d_data of `pitch` bytes
+fx::FArgs ctx_fargs(fxc_ctx* x, const uint8_t* d_data, size_t pitch, int ld);

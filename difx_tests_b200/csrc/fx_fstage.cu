@@ -1,451 +1,71 @@
-// fx_fstage.cu -- fused F stage of the FX correlator for sm_100a.
-//
-// One CTA owns (subband, antenna, block of TB consecutive FFTs).  Per FFT and
-// polarisation it performs, without touching HBM in between:
-//   K0 lookup  : integer offset / validity / fractional delay from the delay
-//                table (kernel.c:733-756, produced by k_delay_table);
-//   unpack     : 2-bit decode of F samples starting at `offset` from bytes
-//                staged in shared memory by 128-bit loads (kernel.c:397-426);
-//   fringe     : multiply by rot[i*S + j] = sub[j] * step[i], the reference's
-//                two-level rotator with FP64 phase arguments (kernel.c:428-497);
-//   FFT        : forward, unnormalised, length F = 2*nchan (kernel.c:499-510),
-//                Stockham radix-16 passes (Govindaraju et al., SC'08) held in
-//                registers with padded shared-memory exchanges;
-//   frac       : channel c *= fsub[c % stride] * fstep[c / stride]
-//                (kernel.c:512-555), channels [0, nchan) only;
-//   store      : plain layout [sb][sig][T][nchan] (f32x2), or the FP16 K-major
-//                layout [sb][nchan][rows][T] for the tensor-core X stage.  The
-//                reference's conjugation (kernel.c:557-568) is folded into the X
-//                stage's arithmetic.
-#include <cstdio>
-
-#include "fx_common.cuh"
-#include "fx_kernels.h"
+// fx_fstage.cu -- dispatch of the fused F stage by FFT length (kernels in
+// fx_fstage.cuh, one translation unit per length) and the debug unpack export.
+#include "fx_fstage.cuh"
 
 namespace fx {
 
-constexpr int ilog2c(int x) { return x <= 1 ? 0 : 1 + ilog2c(x / 2); }
+cudaError_t launch_fstage_256(int mode, const FArgs& a, cudaStream_t st);
+cudaError_t launch_fstage_batch_256(int mode, int npol, int tb, const FArgs* d_jobs, const int4* d_tasks, int ntask,
+                                  cudaStream_t st);
+size_t fstage_smem_256(int mode, int tb, int npol);
+cudaError_t launch_fstage_512(int mode, const FArgs& a, cudaStream_t st);
+cudaError_t launch_fstage_batch_512(int mode, int npol, int tb, const FArgs* d_jobs, const int4* d_tasks, int ntask,
+                                  cudaStream_t st);
+size_t fstage_smem_512(int mode, int tb, int npol);
+cudaError_t launch_fstage_1024(int mode, const FArgs& a, cudaStream_t st);
+cudaError_t launch_fstage_batch_1024(int mode, int npol, int tb, const FArgs* d_jobs, const int4* d_tasks, int ntask,
+                                  cudaStream_t st);
+size_t fstage_smem_1024(int mode, int tb, int npol);
+cudaError_t launch_fstage_2048(int mode, const FArgs& a, cudaStream_t st);
+cudaError_t launch_fstage_batch_2048(int mode, int npol, int tb, const FArgs* d_jobs, const int4* d_tasks, int ntask,
+                                  cudaStream_t st);
+size_t fstage_smem_2048(int mode, int tb, int npol);
+cudaError_t launch_fstage_4096(int mode, const FArgs& a, cudaStream_t st);
+cudaError_t launch_fstage_batch_4096(int mode, int npol, int tb, const FArgs* d_jobs, const int4* d_tasks, int ntask,
+                                  cudaStream_t st);
+size_t fstage_smem_4096(int mode, int tb, int npol);
+cudaError_t launch_fstage_8192(int mode, const FArgs& a, cudaStream_t st);
+cudaError_t launch_fstage_batch_8192(int mode, int npol, int tb, const FArgs* d_jobs, const int4* d_tasks, int ntask,
+                                  cudaStream_t st);
+size_t fstage_smem_8192(int mode, int tb, int npol);
 
-template <int F>
-struct FPlan {
-    static constexpr int C = F / 2;
-    static constexpr int NT = F / 16;                        // threads per FFT
-    static constexpr int STRIDE = 1 << (ilog2c(C) / 2);      // kernel.c:31 generalised
-    static constexpr int S = F / STRIDE;                      // substride (kernel.c:36)
-    static constexpr int FS = STRIDE;                         // frac "sub" length
-    static constexpr int FST = C / STRIDE;                    // frac "step" length
-    static constexpr int NROT = S + STRIDE + FS + FST;        // rotator table entries
-    static constexpr int NPASS = (F == 256) ? 2 : (F <= 4096 ? 3 : 4);
-    static constexpr int LASTR = (F == 256) ? 16 : (F == 512) ? 2 : (F == 1024) ? 4 : (F == 2048) ? 8
-                               : (F == 4096) ? 16 : 2;
-    static constexpr int NSLOT = (NT >= 256) ? 1 : 256 / NT;
-    static constexpr int NTHREADS = NT * NSLOT;
-    static constexpr int BUF = F + F / 16;                    // padded exchange buffer (float2)
-    static constexpr bool TWREG = (F <= 2048);                // twiddles cached in registers
-    static constexpr int TWQ = F / 4;                         // quarter-wave twiddle table
-    static constexpr int MINB = (NTHREADS <= 256) ? 2 : 1;    // CTAs per SM the registers must allow
-};
-
-template <int F, int PASS>
-struct PassInfo {
-    static constexpr int R = (PASS == FPlan<F>::NPASS - 1) ? FPlan<F>::LASTR : 16;
-    static constexpr int NS = 1 << (4 * PASS);               // 16^PASS
-    static constexpr int NB = 16 / R;                         // butterflies per thread
-};
-
-__device__ __forceinline__ int padi(int i) { return i + (i >> 4); }
-
-// e^{-2 pi i m / F} from a quarter-wave table tq[m'] = e^{-2 pi i m'/F}, m' < F/4
-template <int F>
-__device__ __forceinline__ float2 twiddle_q(const float2* tq, int m)
+cudaError_t launch_fstage(int nchan, int mode, const FArgs& a, cudaStream_t st)
 {
-    const int q = m / (F / 4);
-    const float2 b = tq[m & (F / 4 - 1)];
-    switch (q & 3) {
-    case 0: return b;
-    case 1: return make_float2(b.y, -b.x);
-    case 2: return make_float2(-b.x, -b.y);
-    default: return make_float2(-b.y, b.x);
+    switch (2 * nchan) {
+    case 256: return launch_fstage_256(mode, a, st);
+    case 512: return launch_fstage_512(mode, a, st);
+    case 1024: return launch_fstage_1024(mode, a, st);
+    case 2048: return launch_fstage_2048(mode, a, st);
+    case 4096: return launch_fstage_4096(mode, a, st);
+    case 8192: return launch_fstage_8192(mode, a, st);
+    default: return cudaErrorInvalidValue;
     }
 }
 
-__device__ __forceinline__ float2 twiddle_exact(int m, int n)
+cudaError_t launch_fstage_batch(int nchan, int npol, int mode, int tb, const FArgs* d_jobs, const int4* d_tasks,
+                                int ntask, cudaStream_t st)
 {
-    float s, c;
-    sincospif(-2.0f * (float)m / (float)n, &s, &c);
-    return make_float2(c, s);
-}
-
-// Stage the packed bytes of one FFT into shared memory with 128-bit loads.  The
-// window starts at the 16-byte boundary at or below the FFT's first byte and
-// covers the F*npol/4 (+1 when the offset is not byte-aligned, kernel.c:402-409)
-// bytes the FFT spans; with the alignment slack that is <= F*npol/4 + 16 bytes.
-// Returns the window's base byte index in the antenna row.
-__device__ __forceinline__ int stage_fft_bytes(const uint8_t* row, int offset, int npol, int F, uint8_t* inb,
-                                               int t, int nthr)
-{
-    const int first_byte = (npol == 2) ? (offset >> 1) : (offset >> 2);
-    const int base_byte = first_byte & ~15;
-    const int nvec = (F * npol / 4 + 1 + (first_byte - base_byte) + 15) >> 4;
-    const uint4* src = reinterpret_cast<const uint4*>(row + base_byte);
-    uint4* dst = reinterpret_cast<uint4*>(inb);
-    for (int i = t; i < nvec; i += nthr) dst[i] = __ldg(src + i);
-    return base_byte;
-}
-
-// Quantiser level of absolute sample s, polarisation pol (kernel.c:397-426 bit
-// order for npol=2; 4 consecutive samples per byte, LSB first, for npol=1).
-__device__ __forceinline__ float decode_sample(const uint8_t* inb, int base_byte, int s, int npol, int pol)
-{
-    uint32_t code;
-    if (npol == 2) {
-        const uint32_t byte = inb[(s >> 1) - base_byte];
-        code = (byte >> (4 * (s & 1) + 2 * pol)) & 3u;
-    } else {
-        const uint32_t byte = inb[(s >> 2) - base_byte];
-        code = (byte >> (2 * (s & 3))) & 3u;
-    }
-    return level2bit(code);
-}
-
-template <int NT>
-__device__ __forceinline__ void slot_sync(int slot)
-{
-    if constexpr (NT >= 32) {
-        asm volatile("bar.sync %0, %1;" ::"r"(slot + 1), "r"(NT) : "memory");
-    } else {
-        __syncwarp();
+    switch (2 * nchan) {
+    case 256: return launch_fstage_batch_256(mode, npol, tb, d_jobs, d_tasks, ntask, st);
+    case 512: return launch_fstage_batch_512(mode, npol, tb, d_jobs, d_tasks, ntask, st);
+    case 1024: return launch_fstage_batch_1024(mode, npol, tb, d_jobs, d_tasks, ntask, st);
+    case 2048: return launch_fstage_batch_2048(mode, npol, tb, d_jobs, d_tasks, ntask, st);
+    case 4096: return launch_fstage_batch_4096(mode, npol, tb, d_jobs, d_tasks, ntask, st);
+    case 8192: return launch_fstage_batch_8192(mode, npol, tb, d_jobs, d_tasks, ntask, st);
+    default: return cudaErrorInvalidValue;
     }
 }
 
-// Twiddles a thread needs for pass PASS (r = 0..R-1 of each of its NB butterflies).
-template <int F, int PASS>
-struct PassTw {
-    float2 w[PassInfo<F, PASS>::NB * PassInfo<F, PASS>::R];
-};
-
-template <int F, int PASS>
-__device__ __forceinline__ void init_pass_tw(PassTw<F, PASS>& tw, int t)
+size_t fstage_smem_bytes(int nchan, int mode, int npol, int tb)
 {
-    using PI = PassInfo<F, PASS>;
-#pragma unroll
-    for (int b = 0; b < PI::NB; b++) {
-        const int j = t + b * FPlan<F>::NT;
-        const int jm = j & (PI::NS - 1);
-#pragma unroll
-        for (int r = 0; r < PI::R; r++) tw.w[b * PI::R + r] = twiddle_exact(r * jm, PI::NS * PI::R);
-    }
-}
-
-// Load pass inputs from the exchange buffer and apply the DIT twiddles.  All
-// offsets are multiples of 16 elements, so padi(t + c) = padi(t) + c + c/16 and
-// every shared-memory access is one base register plus an immediate.
-template <int F, int PASS>
-__device__ __forceinline__ void pass_load(const float2* buf, const float2* tq, const PassTw<F, PASS>* tw,
-                                          float2* v, int t)
-{
-    using PI = PassInfo<F, PASS>;
-    constexpr int NT = FPlan<F>::NT;
-    constexpr int STEP = F / PI::R;
-    static_assert(STEP % 16 == 0 && NT % 16 == 0, "padded offsets must fold");
-    const float2* p0 = buf + padi(t);
-#pragma unroll
-    for (int b = 0; b < PI::NB; b++) {
-        const int jm = (t + b * NT) & (PI::NS - 1);
-        const float2* p = p0 + b * (NT + NT / 16);
-#pragma unroll
-        for (int r = 0; r < PI::R; r++) {
-            float2 x = p[r * (STEP + STEP / 16)];
-            if (r > 0) {
-                float2 w;
-                if constexpr (FPlan<F>::TWREG) w = tw->w[b * PI::R + r];
-                else w = twiddle_q<F>(tq, r * jm * (F / (PI::NS * PI::R)));
-                x = cmul(x, w);
-            }
-            v[b * PI::R + r] = x;
-        }
-    }
-}
-
-template <int F, int PASS>
-__device__ __forceinline__ void pass_dft(float2* v)
-{
-    using PI = PassInfo<F, PASS>;
-#pragma unroll
-    for (int b = 0; b < PI::NB; b++) dft<PI::R>(v + b * PI::R);
-}
-
-// Stockham store: element r of butterfly j goes to (j / NS) * NS * R + j % NS + r * NS.
-template <int F, int PASS>
-__device__ __forceinline__ void pass_store(float2* buf, const float2* v, int t)
-{
-    using PI = PassInfo<F, PASS>;
-    constexpr int NT = FPlan<F>::NT;
-#pragma unroll
-    for (int b = 0; b < PI::NB; b++) {
-        const int j = t + b * NT;
-        float2* p;
-        constexpr int RS = (PI::NS == 1) ? 1 : PI::NS + PI::NS / 16;   // padded stride of r
-        if constexpr (PI::NS == 1) p = buf + 17 * j;                    // padi(16 j)
-        else p = buf + padi((j / PI::NS) * PI::NS * PI::R + (j & (PI::NS - 1)));
-#pragma unroll
-        for (int r = 0; r < PI::R; r++) p[r * RS] = v[b * PI::R + r];
-    }
-}
-
-// Rotator table of one FFT: [fr_sub S][fr_step STRIDE][fc_sub FS][fc_step FST].
-// Entries are (cos, sin)(pi * x) with x in half-turns, which needs no
-// large-argument reduction: fringe x = -2 * frac(phase in turns), i.e. the
-// reference's argument -2pi*frac(phase) (kernel.c:463-470) divided by pi;
-// fractional-sample x = the reference's float32 argument (kernel.c:517-523) / pi.
-// Divisions by F are multiplications by the exact power-of-two reciprocal.
-constexpr float kInvPiF = 0.318309886183790671538f;
-
-template <int F>
-__device__ __forceinline__ float2 rot_entry(int e, const DelayEntry& d, double lo, double lofrac, bool fraclo,
-                                            const float* ctab)
-{
-    using P = FPlan<F>;
-    constexpr double kInvF = 1.0 / F;
-    float x;
-    if (e < P::S) {
-        // kernel.c:434-466: subphase[j] = lo * (j/F * a + b'), b' = b - (int)b
-        const double intdelay = trunc(d.b);
-        const double bp = dsub(d.b, intdelay);
-        const double xoff = dmul((double)e, kInvF);
-        double ph = dmul(dadd(dmul(xoff, d.a), bp), lo);
-        if (fraclo) ph = dadd(ph, dmul(lofrac, intdelay));
-        x = __double2float_rn(-2.0 * dsub(ph, trunc(ph)));
-    } else if (e < P::S + P::STRIDE) {
-        // kernel.c:145, 452, 469: stepphase[i] = lo * (i*stride/F * a)
-        const double xoff = dmul((double)((e - P::S) * P::STRIDE), kInvF);
-        const double ph = dmul(dmul(xoff, d.a), lo);
-        x = __double2float_rn(-2.0 * dsub(ph, trunc(ph)));
-    } else {
-        const float arg = __fmul_rn(ctab[e - P::S - P::STRIDE], __double2float_rn(d.frac));
-        x = __fmul_rn(arg, kInvPiF);
-    }
-    float sn, cs;
-    sincospif(x, &sn, &cs);
-    return make_float2(cs, sn);
-}
-
-template <int F, int MODE, int TB, int NPOL>
-__global__ void __launch_bounds__(FPlan<F>::NTHREADS, FPlan<F>::MINB)
-k_fstage(FArgs args)
-{
-    using P = FPlan<F>;
-    constexpr int NT = P::NT;
-    constexpr int C = P::C;
-    constexpr int INB = F / 2 + 16;                                    // staged bytes per slot
-    extern __shared__ __align__(16) unsigned char smem[];
-    float2* bufs = reinterpret_cast<float2*>(smem);                   // [NSLOT][BUF]
-    float2* tq = bufs + P::NSLOT * P::BUF;                              // [TWQ]
-    float2* rtabs = tq + (P::TWREG ? 0 : P::TWQ);                      // [NSLOT][NROT]
-    float* ctab = reinterpret_cast<float*>(rtabs + P::NSLOT * P::NROT);     // [FS + FST] channel freqs
-    uint8_t* inbs = reinterpret_cast<uint8_t*>(ctab + P::FS + P::FST);      // [NSLOT][INB]
-    __half2* stage = reinterpret_cast<__half2*>(inbs + P::NSLOT * INB);       // [NPOL][TB][C]
-
-    const int tid = threadIdx.x;
-    const int slot = tid / NT;
-    const int t = tid - slot * NT;
-    const int sb = blockIdx.z;
-    const int ant = blockIdx.y;
-    const int tb0 = blockIdx.x * TB;
-    float2* buf = bufs + slot * P::BUF;
-    float2* rtab = rtabs + slot * P::NROT;
-    uint8_t* inb = inbs + slot * INB;
-
-    const double lo = args.sb_lo[sb];
-    const double lofrac = dsub(lo, trunc(lo));
-    const bool fraclo = lofrac > 1e-11;                                  // kernel.c:39
-
-    if constexpr (!P::TWREG) {
-        for (int m = tid; m < P::TWQ; m += P::NTHREADS) tq[m] = twiddle_exact(m, F);
-    }
-    for (int i = tid; i < P::FS + P::FST; i += P::NTHREADS)
-        ctab[i] = i < P::FS ? args.chan_sub[i] : args.chan_step[i - P::FS];
-    PassTw<F, 1> tw1;
-    PassTw<F, (P::NPASS > 2 ? 2 : 1)> tw2;
-    if constexpr (P::TWREG) {
-        init_pass_tw<F, 1>(tw1, t);
-        if constexpr (P::NPASS > 2) init_pass_tw<F, 2>(tw2, t);
-    }
-    __syncthreads();
-
-    const uint8_t* row = args.data + ((size_t)sb * args.nant + ant) * args.pitch;
-    const int nsig = args.nant * NPOL;
-    constexpr int NITEM = TB * NPOL;
-    const DelayEntry* dtab = args.dtab + (size_t)ant * args.ld + args.t_base;
-
-    // Input window of an item (kernel.c:402-409): 16-byte aligned start, one
-    // 128-bit vector per thread at most (F*NPOL/4 + 16 <= 16*NT).
-    auto window = [&](const DelayEntry& d, int& base, int& nvec) {
-        const int first = (NPOL == 2) ? (d.offset >> 1) : (d.offset >> 2);
-        base = first & ~15;
-        nvec = (F * NPOL / 4 + 1 + (first - base) + 15) >> 4;
-    };
-
-    // prefetch of the first item's delay entry and input vector
-    int item = slot;
-    DelayEntry dn;
-    bool vn = false;
-    int basen = 0, nvecn = 0;
-    uint4 pf = make_uint4(0, 0, 0, 0);
-    if (item < NITEM && tb0 + item / NPOL < args.nfft) {
-        dn = dtab[tb0 + item / NPOL];
-        vn = dn.valid != 0;
-    }
-    if (vn) {
-        window(dn, basen, nvecn);
-        if (t < nvecn) pf = __ldg(reinterpret_cast<const uint4*>(row + basen) + t);
-    }
-
-    for (; item < NITEM; item += P::NSLOT) {
-        const int tl = item / NPOL;
-        const int pol = item - tl * NPOL;
-        const int tc = tb0 + tl;                    // FFT slot within the chunk
-        const DelayEntry d = dn;
-        const bool valid = vn;
-        const int base_byte = basen;
-        if (valid && t < nvecn) reinterpret_cast<uint4*>(inb)[t] = pf;
-        // ---- prefetch the next item of this slot
-        {
-            const int ni = item + P::NSLOT;
-            vn = false;
-            if (ni < NITEM && tb0 + ni / NPOL < args.nfft) {
-                dn = dtab[tb0 + ni / NPOL];
-                vn = dn.valid != 0;
-            }
-            if (vn) {
-                window(dn, basen, nvecn);
-                if (t < nvecn) pf = __ldg(reinterpret_cast<const uint4*>(row + basen) + t);
-            }
-        }
-        // ---- rotator tables for this FFT (per slot)
-        for (int e = t; e < P::NROT; e += NT)
-            rtab[e] = valid ? rot_entry<F>(e, d, lo, lofrac, fraclo, ctab) : make_float2(0.f, 0.f);
-        slot_sync<NT>(slot);
-
-        // ---- pass 0: unpack + fringe rotation + radix-16 (samples n = t + r*NT)
-        float2 v[16];
-        {
-            // an invalid item reads from the start of the staging buffer (in range;
-            // its rotator is zero, so the levels do not matter)
-            const int s0 = valid ? d.offset + t : t;
-            const int b0 = valid ? base_byte : 0;
-            const uint8_t* bp;
-            int sh;
-            if constexpr (NPOL == 2) {
-                bp = inb + ((s0 >> 1) - b0);
-                sh = 4 * (s0 & 1) + 2 * pol;
-            } else {
-                bp = inb + ((s0 >> 2) - b0);
-                sh = 2 * (s0 & 3);
-            }
-            const float2* fr_sub = rtab;
-            const float2* fr_step = rtab + P::S;
-            float2 sub_c = make_float2(0.f, 0.f);
-            const float2* stp = fr_step;
-            if constexpr (NT % P::S == 0) {
-                sub_c = fr_sub[t % P::S];   // j = n % S is the same for all r
-                stp = fr_step + t / P::S;
-            }
-#pragma unroll
-            for (int r = 0; r < 16; r++) {
-                const uint32_t byte = bp[r * (NT * NPOL / 4)];
-                const float lv = level2bit((byte >> sh) & 3u);
-                float2 rot;
-                if constexpr (NT % P::S == 0) {
-                    rot = cmul(sub_c, stp[r * (NT / P::S)]);
-                } else {
-                    const int n = t + r * NT;
-                    rot = cmul(fr_sub[n % P::S], fr_step[n / P::S]);
-                }
-                v[r] = make_float2(lv * rot.x, lv * rot.y);
-            }
-        }
-        dft<16>(v);
-        pass_store<F, 0>(buf, v, t);
-        slot_sync<NT>(slot);
-
-        // ---- middle passes
-        if constexpr (P::NPASS > 2) {
-            pass_load<F, 1>(buf, tq, &tw1, v, t);
-            slot_sync<NT>(slot);
-            pass_dft<F, 1>(v);
-            pass_store<F, 1>(buf, v, t);
-            slot_sync<NT>(slot);
-        }
-        if constexpr (P::NPASS > 3) {
-            pass_load<F, 2>(buf, tq, nullptr, v, t);
-            slot_sync<NT>(slot);
-            pass_dft<F, 2>(v);
-            pass_store<F, 2>(buf, v, t);
-            slot_sync<NT>(slot);
-        }
-        // ---- last pass
-        constexpr int LP = P::NPASS - 1;
-        using LI = PassInfo<F, LP>;
-        if constexpr (LP == 1) pass_load<F, 1>(buf, tq, &tw1, v, t);
-        else if constexpr (LP == 2) pass_load<F, 2>(buf, tq, &tw2, v, t);
-        else pass_load<F, 3>(buf, tq, nullptr, v, t);
-#pragma unroll
-        for (int b = 0; b < LI::NB; b++) dft_lo<LI::R>(v + b * LI::R);   // outputs r < R/2 only
-
-        // ---- fractional-sample correction + store of channels k = j + r*F/R < C
-        constexpr int KSTEP = F / LI::R;
-        static_assert(KSTEP % P::FS == 0, "frac rotator index must fold");
-        const float2* fc_sub = rtab + P::S + P::STRIDE;
-        const float2* fc_step = fc_sub + P::FS;
-        const int sig = ant * NPOL + pol;
-#pragma unroll
-        for (int b = 0; b < LI::NB; b++) {
-            const int j = t + b * NT;
-            const float2 fsub = fc_sub[j % P::FS];
-            const float2* fst = fc_step + j / P::FS;
-#pragma unroll
-            for (int r = 0; r < LI::R / 2; r++) {
-                const float2 fr = cmul(fsub, fst[r * (KSTEP / P::FS)]);
-                const float2 y = cmul(fr, v[b * LI::R + r]);
-                if constexpr (MODE == kSpecF32) {
-                    float2* out = reinterpret_cast<float2*>(args.spec) +
-                                  (((size_t)sb * nsig + sig) * args.T + tc) * C + j;
-                    if (tc < args.T) out[r * KSTEP] = y;
-                } else {
-                    stage[(pol * TB + tl) * C + j + r * KSTEP] = __floats2half2_rn(y.x, y.y);
-                }
-            }
-        }
-        slot_sync<NT>(slot);   // buf / rtab / inb are reused by the next item
-    }
-
-    if constexpr (MODE == kSpecF16) {
-        __syncthreads();
-        // flush: one (pol, channel) per thread -> Re row and Im row, TB halves each
-        __half* spec = reinterpret_cast<__half*>(args.spec);
-        for (int e = tid; e < NPOL * C; e += P::NTHREADS) {
-            const int pol = e / C;
-            const int k = e - pol * C;
-            const int sig = ant * NPOL + pol;
-            uint32_t rw[TB / 2], iw[TB / 2];
-#pragma unroll
-            for (int q = 0; q < TB / 2; q++) {
-                const __half2 h0 = stage[(pol * TB + 2 * q) * C + k];
-                const __half2 h1 = stage[(pol * TB + 2 * q + 1) * C + k];
-                const __half2 r2 = __lows2half2(h0, h1);
-                const __half2 i2 = __highs2half2(h0, h1);
-                rw[q] = *reinterpret_cast<const uint32_t*>(&r2);
-                iw[q] = *reinterpret_cast<const uint32_t*>(&i2);
-            }
-            __half* dst = spec + (((size_t)sb * C + k) * args.rows + 2 * sig) * (size_t)args.T + tb0;
-#pragma unroll
-            for (int q = 0; q < TB / 8; q++) {
-                reinterpret_cast<uint4*>(dst)[q] = make_uint4(rw[4 * q], rw[4 * q + 1], rw[4 * q + 2], rw[4 * q + 3]);
-                reinterpret_cast<uint4*>(dst + args.T)[q] =
-                    make_uint4(iw[4 * q], iw[4 * q + 1], iw[4 * q + 2], iw[4 * q + 3]);
-            }
-        }
+    switch (2 * nchan) {
+    case 256: return fstage_smem_256(mode, tb ? tb : 16, npol);
+    case 512: return fstage_smem_512(mode, tb ? tb : 16, npol);
+    case 1024: return fstage_smem_1024(mode, tb ? tb : 16, npol);
+    case 2048: return fstage_smem_2048(mode, tb ? tb : 16, npol);
+    case 4096: return fstage_smem_4096(mode, tb ? tb : 16, npol);
+    case 8192: return fstage_smem_8192(mode, tb ? tb : 16, npol);
+    default: return 0;
     }
 }
 
@@ -488,69 +108,5 @@ cudaError_t launch_unpack_debug(int nchan, const FArgs& a, float* out, cudaStrea
     return cudaGetLastError();
 }
 
-template <int F>
-static size_t fstage_smem(int mode, int tb, int npol)
-{
-    using P = FPlan<F>;
-    size_t s = (size_t)P::NSLOT * P::BUF * sizeof(float2);
-    if (!P::TWREG) s += (size_t)P::TWQ * sizeof(float2);
-    s += (size_t)P::NSLOT * P::NROT * sizeof(float2);
-    s += (size_t)(P::FS + P::FST) * sizeof(float);
-    s += (size_t)P::NSLOT * (F / 2 + 16);
-    if (mode == kSpecF16) s += (size_t)npol * tb * P::C * sizeof(__half2);
-    return s;
-}
-
-template <int F, int MODE, int TB, int NPOL>
-static cudaError_t launch_f(const FArgs& a, cudaStream_t st)
-{
-    using P = FPlan<F>;
-    const size_t sm = fstage_smem<F>(MODE, TB, NPOL);
-    auto kern = k_fstage<F, MODE, TB, NPOL>;
-    static unsigned configured = 0;  // per instantiation and device
-    cudaError_t e = set_smem_once(kern, sm, &configured);
-    if (e != cudaSuccess) return e;
-    dim3 grid((a.T + TB - 1) / TB, a.nant, a.nsb);
-    kern<<<grid, P::NTHREADS, sm, st>>>(a);
-    return cudaGetLastError();
-}
-
-template <int F, int MODE>
-static cudaError_t launch_fp(const FArgs& a, cudaStream_t st)
-{
-    return a.npol == 2 ? launch_f<F, MODE, 16, 2>(a, st) : launch_f<F, MODE, 16, 1>(a, st);
-}
-
-cudaError_t launch_fstage(int nchan, int mode, const FArgs& a, cudaStream_t st)
-{
-    const int F = 2 * nchan;
-#define FX_CASE(FF)                                                            \
-    case FF:                                                                   \
-        return mode == kSpecF32 ? launch_fp<FF, kSpecF32>(a, st)               \
-                                : launch_fp<FF, kSpecF16>(a, st);
-    switch (F) {
-        FX_CASE(256)
-        FX_CASE(512)
-        FX_CASE(1024)
-        FX_CASE(2048)
-        FX_CASE(4096)
-        FX_CASE(8192)
-    default: return cudaErrorInvalidValue;
-    }
-#undef FX_CASE
-}
-
-size_t fstage_smem_bytes(int nchan, int mode, int npol)
-{
-    switch (2 * nchan) {
-    case 256: return fstage_smem<256>(mode, 16, npol);
-    case 512: return fstage_smem<512>(mode, 16, npol);
-    case 1024: return fstage_smem<1024>(mode, 16, npol);
-    case 2048: return fstage_smem<2048>(mode, 16, npol);
-    case 4096: return fstage_smem<4096>(mode, 16, npol);
-    case 8192: return fstage_smem<8192>(mode, 16, npol);
-    default: return 0;
-    }
-}
 
 }  // namespace fx

@@ -47,13 +47,16 @@ struct FArgs {
     const float* chan_step;     // [nchan/stride] (f32)(2 pi i stride bw / nchan) kernel.c:165
     void* spec;                 // spectra buffer (layout per SpecMode)
     int rows;                   // F16 layout: rows per channel (>= 2*nsig)
+    int tb;                     // FFTs per CTA (8, 16 or 32; 0 = 16), chosen by the plan / autotuner
 };
+
 
 struct XArgs {
     const void* spec;
     void* acc;
     int nsig, T, nchan, nsb;
     int rows;
+    int alt;     // plain-form tile variant: 0 = default, 1 = alternative (chosen by the plan / autotuner)
 };
 
 }  // namespace fx

@@ -14,8 +14,13 @@ cudaError_t launch_counts(const uint32_t* vbits, int nant, int nwords, int* coun
 cudaError_t launch_finalize(const float2* acc, int acc_layout, int nsig, int npol, int nant, int nchan, int nsb,
                             const int* counts, int normalize, float2* vis, cudaStream_t st);
 cudaError_t launch_fstage(int nchan, int mode, const FArgs& a, cudaStream_t st);
-size_t fstage_smem_bytes(int nchan, int mode, int npol);
+size_t fstage_smem_bytes(int nchan, int mode, int npol, int tb);
+cudaError_t launch_fstage_batch(int nchan, int npol, int mode, int tb, const FArgs* d_jobs, const int4* d_tasks,
+                                int ntask, cudaStream_t st);
 cudaError_t launch_xplain(const XArgs& a, cudaStream_t st);
+cudaError_t launch_xplain_batch(int nsig, int alt, const XArgs* d_jobs, const int4* d_tasks, int ntask,
+                                cudaStream_t st);
+int xplain_channel_group(int nsig, int alt);
 cudaError_t launch_xtc(const XArgs& a, int* d_err, int nsm, cudaStream_t st);
 size_t xtc_smem_bytes();
 cudaError_t launch_unpack_debug(int nchan, const FArgs& a, float* out, cudaStream_t st);

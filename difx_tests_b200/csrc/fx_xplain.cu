@@ -41,12 +41,11 @@ __device__ __forceinline__ int xoff(int s, int tk, int cl)
     return s * TK * CG + (s >> 3) * 8 + tk * CG + cl;
 }
 
+// One X-stage block: channels [c0, c0 + CG) of subband sb over all T FFT slots.
 template <int NB, int CG, int TK>
-__global__ void __launch_bounds__(XPlan<NB, CG, TK>::NTHREADS, 1)
-k_xplain(XArgs a)
+__device__ __forceinline__ void xplain_block(const XArgs& a, int sb, int c0, unsigned char* smem)
 {
     using P = XPlan<NB, CG, TK>;
-    extern __shared__ __align__(16) unsigned char smem[];
     float2* xs = reinterpret_cast<float2*>(smem);   // [2][STAGE]
 
     const int tid = threadIdx.x;
@@ -59,8 +58,6 @@ k_xplain(XArgs a)
     }
     const int J = I + rem;
 
-    const int c0 = blockIdx.x * CG;
-    const int sb = blockIdx.y;
     const int nsig = a.nsig;
     const int C = a.nchan;
     const float2* spec = reinterpret_cast<const float2*>(a.spec) + (size_t)sb * nsig * a.T * C;
@@ -140,9 +137,33 @@ k_xplain(XArgs a)
 }
 
 template <int NB, int CG, int TK>
+__global__ void __launch_bounds__(XPlan<NB, CG, TK>::NTHREADS, 1)
+k_xplain(XArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    xplain_block<NB, CG, TK>(a, blockIdx.y, blockIdx.x * CG, smem);
+}
+
+// Many jobs with the same tile plan in one persistent launch: CTAs stride over
+// a task table {job, subband, first channel}.
+template <int NB, int CG, int TK>
+__global__ void __launch_bounds__(XPlan<NB, CG, TK>::NTHREADS, 1)
+k_xplain_batch(const XArgs* __restrict__ jobs, const int4* __restrict__ tasks, int ntask)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    for (int i = blockIdx.x; i < ntask; i += gridDim.x) {
+        const int4 tk = tasks[i];
+        const XArgs a = jobs[tk.x];
+        xplain_block<NB, CG, TK>(a, tk.y, tk.z, smem);
+        __syncthreads();   // the next task refills the staging buffers
+    }
+}
+
+template <int NB, int CG, int TK>
 static cudaError_t launch_x(const XArgs& a, cudaStream_t st)
 {
     using P = XPlan<NB, CG, TK>;
+    if (a.nchan % CG) return cudaErrorInvalidValue;
     const size_t sm = 2 * (size_t)P::STAGE * sizeof(float2);
     auto kern = k_xplain<NB, CG, TK>;
     static unsigned configured = 0;  // per instantiation and device
@@ -153,23 +174,70 @@ static cudaError_t launch_x(const XArgs& a, cudaStream_t st)
     return cudaGetLastError();
 }
 
-// Tile shape per signal count: NB = ceil(nsig/8) blocks of 8 signals; CG
-// channels per CTA chosen so a CTA has 96..512 threads.
+template <int NB, int CG, int TK>
+static cudaError_t launch_xb(const XArgs* d_jobs, const int4* d_tasks, int ntask, cudaStream_t st)
+{
+    using P = XPlan<NB, CG, TK>;
+    const size_t sm = 2 * (size_t)P::STAGE * sizeof(float2);
+    auto kern = k_xplain_batch<NB, CG, TK>;
+    static unsigned configured = 0;
+    cudaError_t e = set_smem_once(kern, sm, &configured);
+    if (e != cudaSuccess) return e;
+    int dev = 0, nsm = 0, per_sm = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, P::NTHREADS, sm)) != cudaSuccess) return e;
+    int grid = nsm * (per_sm > 0 ? per_sm : 1);
+    if (grid > ntask) grid = ntask;
+    kern<<<grid, P::NTHREADS, sm, st>>>(d_jobs, d_tasks, ntask);
+    return cudaGetLastError();
+}
+
+// Tile plans per signal count: NB = ceil(nsig/8) blocks of 8 signals; CG
+// channels per CTA and TK FFTs per shared-memory stage.  Variant 0 is the
+// built-in choice, variant 1 the alternative the autotuner may pick.
+#define FX_XPLANS(OP)                                                           \
+    switch (nb * 2 + (alt ? 1 : 0)) {                                           \
+    case 2: OP(1, 32, 8); case 3: OP(1, 16, 16);                                \
+    case 4: OP(2, 32, 8); case 5: OP(2, 16, 16);                                \
+    case 6: OP(3, 32, 8); case 7: OP(3, 16, 16);                                \
+    case 8: OP(4, 32, 8); case 9: OP(4, 16, 16);                                \
+    case 10: OP(5, 16, 8); case 11: OP(5, 8, 16);                               \
+    case 12: OP(6, 16, 8); case 13: OP(6, 8, 16);                               \
+    case 14: OP(7, 8, 16); case 15: OP(7, 8, 8);                                \
+    case 16: OP(8, 8, 16); case 17: OP(8, 8, 8);                                \
+    default: return cudaErrorNotSupported;                                      \
+    }
+
+int xplain_channel_group(int nsig, int alt)
+{
+    const int nb = (nsig + 7) / 8;
+#define FX_CG(NB_, CG_, TK_) return CG_
+    switch (nb * 2 + (alt ? 1 : 0)) {
+    case 2: case 4: case 6: case 8: FX_CG(0, 32, 0);
+    case 3: case 5: case 7: case 9: case 10: case 12: FX_CG(0, 16, 0);
+    default: FX_CG(0, 8, 0);
+    }
+#undef FX_CG
+}
+
 cudaError_t launch_xplain(const XArgs& a, cudaStream_t st)
 {
     const int nb = (a.nsig + 7) / 8;
+    const int alt = a.alt;
     if (a.T % 16 != 0) return cudaErrorInvalidValue;  // T is a multiple of every TK
-    switch (nb) {
-    case 1: return a.nchan % 32 ? cudaErrorInvalidValue : launch_x<1, 32, 8>(a, st);
-    case 2: return a.nchan % 32 ? cudaErrorInvalidValue : launch_x<2, 32, 8>(a, st);
-    case 3: return a.nchan % 32 ? cudaErrorInvalidValue : launch_x<3, 32, 8>(a, st);
-    case 4: return a.nchan % 32 ? cudaErrorInvalidValue : launch_x<4, 32, 8>(a, st);
-    case 5: return a.nchan % 16 ? cudaErrorInvalidValue : launch_x<5, 16, 8>(a, st);
-    case 6: return a.nchan % 16 ? cudaErrorInvalidValue : launch_x<6, 16, 8>(a, st);
-    case 7: return a.nchan % 8 ? cudaErrorInvalidValue : launch_x<7, 8, 16>(a, st);
-    case 8: return a.nchan % 8 ? cudaErrorInvalidValue : launch_x<8, 8, 16>(a, st);
-    default: return cudaErrorNotSupported;
-    }
+#define FX_OP(NB_, CG_, TK_) return launch_x<NB_, CG_, TK_>(a, st)
+    FX_XPLANS(FX_OP)
+#undef FX_OP
+}
+
+cudaError_t launch_xplain_batch(int nsig, int alt, const XArgs* d_jobs, const int4* d_tasks, int ntask,
+                                cudaStream_t st)
+{
+    const int nb = (nsig + 7) / 8;
+#define FX_OP(NB_, CG_, TK_) return launch_xb<NB_, CG_, TK_>(d_jobs, d_tasks, ntask, st)
+    FX_XPLANS(FX_OP)
+#undef FX_OP
 }
 
 }  // namespace fx

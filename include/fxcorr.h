@@ -152,6 +152,38 @@ int fxc_correlate_noalloc(const fxc_config* cfg, const uint8_t* d_data, size_t p
                           const double* fileoffsets, int first_fft, int nfft, float* d_vis, int* d_counts,
                           int normalize, void* stream);
 
+/* ---- many independent jobs in grouped persistent launches -------------------
+ * A batch holds jobs of uneven geometry (antennas, polarisations, channels,
+ * subbands, subintegration length).  fxc_batch_process runs every job's whole
+ * subintegration: one persistent F-stage launch per group of jobs sharing FFT
+ * length and polarisation count, one persistent X-stage launch per group sharing
+ * an X tile plan (CTAs stride over a task table of {job, subband, antenna or
+ * channel block}), in rounds when a job needs several spectra chunks.  The first
+ * call runs eagerly; later calls replay one CUDA graph of the whole sequence.
+ * Plain FP32 X stage.  No counterpart in the reference (one job per run).
+ * fxc_batch_autotune times the FFT block size (8/16/32 FFTs per CTA) of every
+ * F group and the tile variant of every X group on the uploaded data, keeps the
+ * fastest, and zeroes the accumulators; with the environment variable
+ * FXC_PLAN_CACHE naming a file, chosen plans are appended to it and read back by
+ * later fxc_batch_create calls. */
+typedef struct fxc_batch fxc_batch;
+int fxc_batch_create(const fxc_config* cfgs, int njobs, fxc_batch** out);
+void fxc_batch_destroy(fxc_batch* b);
+/* host rows of job `job` (as fxc_upload_input) */
+int fxc_batch_upload(fxc_batch* b, int job, const uint8_t* const* data);
+/* delay model of job `job` (as fxc_process_host: delays[3*ant+k], fileoffsets[ant]) */
+int fxc_batch_set_model(fxc_batch* b, int job, const double* delays, const double* fileoffsets);
+int fxc_batch_process(fxc_batch* b);
+int fxc_batch_reset(fxc_batch* b);
+int fxc_batch_get_visibilities(fxc_batch* b, int job, float* vis, int* counts, int normalize);
+int fxc_batch_autotune(fxc_batch* b, int reps);
+/* plan of a job's groups: FFTs per F-stage CTA and X tile variant (0/1) */
+int fxc_batch_get_plan(fxc_batch* b, int job, int* fft_block, int* x_variant);
+int fxc_batch_set_stream(fxc_batch* b, void* stream);
+int fxc_batch_synchronize(fxc_batch* b);
+/* 0 disables graph capture (every call runs eagerly), non-zero enables it (default) */
+int fxc_batch_use_graph(fxc_batch* b, int enable);
+
 /* Per-stage device timing (the counterpart of the reference's per-stage clock()
  * timers, kernel.c:720-821).  With enable != 0 every launch is bracketed by CUDA
  * events on the context's stream.  fxc_stage_times waits for the stream and

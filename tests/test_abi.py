@@ -96,3 +96,23 @@ def test_null_arguments_rejected():
     assert L.fxc_process_host(None, None, None, None, 0, 1) == fx.FXC_ERR_INVALID
     assert L.fxc_get_visibilities(None, None, None, 0) == fx.FXC_ERR_INVALID
     assert L.fxc_strerror(fx.FXC_ERR_NOMEM).decode().startswith("out of")
+
+
+def test_batch_arguments_rejected():
+    L = fx.lib()
+    out = C.c_void_p()
+    cfg = fx.make_config(4, 256, 64, 32e6, 1.4e9)
+    assert L.fxc_batch_create(None, 1, C.byref(out)) == fx.FXC_ERR_INVALID
+    assert L.fxc_batch_create(C.byref(cfg), 0, C.byref(out)) == fx.FXC_ERR_INVALID
+    tc = fx.make_config(4, 256, 64, 32e6, 1.4e9, xmode=fx.FXC_X_TC_FP16)
+    assert L.fxc_batch_create(C.byref(tc), 1, C.byref(out)) == fx.FXC_ERR_UNSUPPORTED
+    bad = fx.make_config(4, 300, 64, 32e6, 1.4e9)
+    assert L.fxc_batch_create(C.byref(bad), 1, C.byref(out)) == fx.FXC_ERR_INVALID
+    assert not out.value
+    assert L.fxc_batch_process(None) == fx.FXC_ERR_INVALID
+    assert L.fxc_batch_reset(None) == fx.FXC_ERR_INVALID
+    assert L.fxc_batch_autotune(None, 1) == fx.FXC_ERR_INVALID
+    assert L.fxc_batch_get_visibilities(None, 0, None, None, 0) == fx.FXC_ERR_INVALID
+    assert L.fxc_batch_upload(None, 0, None) == fx.FXC_ERR_INVALID
+    assert L.fxc_batch_set_model(None, 0, None, None) == fx.FXC_ERR_INVALID
+    L.fxc_batch_destroy(None)
