@@ -7,11 +7,11 @@ subintegration = 31250 FFTs per subband at 128 MS/s, 2-bit real samples.
 One step = one subintegration (all subbands) through the whole hot path:
 delay table, fused unpack/shift/fringe/FFT/fractional-sample F stage, X stage.
 
-  python bench.py [--gpus N --steps K --warmup W] [--xmode both|tc|plain] [--impl reference]
+  python bench.py [--gpus N --steps K --warmup W] [--xmode all|both|tc|fp8|plain] [--impl reference]
 
 The headline `value` is the tensor-core form (FP32 F stage, FP16 X inputs with
-FP32 accumulation); the FP32 plain form runs on the same input in the same
-invocation and is reported under "plain".
+FP32 accumulation); the FP8-E4M3 tensor-core form and the FP32 plain form run on
+the same input in the same invocation and are reported under "fp8" and "plain".
 
 Under torchrun (N > 1) every rank correlates its own subintegration (weak
 scaling, no data-path collective) and rank 0 prints one JSON line; time is the
@@ -44,6 +44,24 @@ WORKLOADS = {
     "cfg2s": dict(nant=64, npol=1, nchan=1024, nsb=1, numffts=4096, bw=64e6, lo=1.4e9, rho=0.1,
                   desc="64 ant x 1 pol x 1 subband x 1024 ch, 4096 FFTs (profiling size)"),
 }
+
+# Batched uneven workload: 12 independent jobs, antenna counts fixed, FFT length, subband count and
+# subintegration length drawn (seed 3) from {256, 512, 1024, 4096, 8192} points, 1-8 subbands and
+# 5-200 ms at 64 MS/s (32 MHz, single polarisation); per-job data seed 1000 + job.
+BATCH_ANTS = [4, 6, 8, 10, 12, 16, 20, 24, 32, 40, 48, 56]
+
+
+def batch_jobs():
+    rng = np.random.default_rng(3)
+    jobs = []
+    for j, a in enumerate(BATCH_ANTS):
+        F = int(rng.choice([256, 512, 1024, 4096, 8192]))
+        nsb = int(rng.integers(1, 9))
+        dur = float(rng.uniform(5e-3, 200e-3))
+        jobs.append(dict(nant=a, npol=1, nchan=F // 2, nsb=nsb, numffts=int(round(dur * 64e6 / F)), bw=32e6,
+                         lo=1.4e9, rho=0.1, seed=1000 + j))
+    return jobs
+
 
 METRIC = "input Gsamp/s on 1 GPU & X TFLOP/s: TC form vs FP32 plain at stated visibility error"
 UNIT = "Gsamp/s"
@@ -290,6 +308,12 @@ def run_reference_arm(args):
 FSTAGE_TC_DRAM_BYTES_PER_SAMPLE = 2.19
 
 
+XMODES = {"plain": 0, "tc": 1, "fp8": 2}    # FXC_X_PLAIN_FP32, FXC_X_TC_FP16, FXC_X_TC_FP8
+DTYPES = {"plain": "f32",
+          "tc": "f32 F stage / f16 X inputs, f32 accumulate",
+          "fp8": "f32 F stage / e4m3 X inputs scaled per signal and channel, f32 accumulate"}
+
+
 def time_form(torch, dist, fx, w, xmode, data, pitch, delays, offs, steps, warmup, world, dev, stream):
     """Warm up, then time `steps` subintegrations of one X form; returns a result dict."""
     F = 2 * w["nchan"]
@@ -372,20 +396,20 @@ def run_gpu_arm(args):
                            device=dev)
     torch.cuda.synchronize()
 
-    forms = ["tc", "plain"] if args.xmode == "both" else [args.xmode]
+    forms = {"all": ["tc", "fp8", "plain"], "both": ["tc", "plain"]}.get(args.xmode, [args.xmode])
     res = {}
     for form in forms:
-        xm = fx.FXC_X_TC_FP16 if form == "tc" else fx.FXC_X_PLAIN_FP32
+        xm = XMODES[form]
         res[form] = time_form(torch, dist, fx, w, xm, data, pitch, delays, offs, args.steps, args.warmup, world, dev,
                               stream)
         if form != forms[0]:
             res[form]["corr"].close()
     head = res[forms[0]]
-    xmode = fx.FXC_X_TC_FP16 if forms[0] == "tc" else fx.FXC_X_PLAIN_FP32
+    xmode = XMODES[forms[0]]
 
     # ---- roofline of the dominant kernel of the headline form (the F stage)
     hbm, tc_peak, peak_kind = peaks()
-    spec_bpc = 4 if xmode == fx.FXC_X_TC_FP16 else 8          # bytes per complex spectrum value written
+    spec_bpc = 8 if xmode == fx.FXC_X_PLAIN_FP32 else 4       # bytes per complex spectrum value written
     f_bytes = head["samples_per_launch"] * (0.25 + 0.5 * spec_bpc)
     f_gbs = f_bytes / (head["f_ms_launch"] / 1e3) / 1e9
     sm = head["stage_ms"]
@@ -402,7 +426,7 @@ def run_gpu_arm(args):
         "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": head["ms_max"] / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32 F stage / f16 X inputs, f32 accumulate" if xmode == fx.FXC_X_TC_FP16 else "f32",
+        "dtype": DTYPES[forms[0]],
         "data": "synthetic (seeded, generated on device)",
         "config": {"workload": w["desc"], "form": forms[0], "parallelism": f"replicas x{world}",
                    "l2": "inputs (8.2 GB packed per step at cfg2) exceed L2; no flush",
@@ -415,13 +439,18 @@ def run_gpu_arm(args):
         "clocks": head["clocks"],
         "gpu_launches": int(head["launches"].sum()),
     }
+    for form in forms[1:]:
+        p = res[form]
+        line[form] = {"value": p["value"], "unit": UNIT, "ms_per_step": p["ms_max"] / args.steps, "dtype": DTYPES[form],
+                      "stages_ms_per_step": {"F": p["stage_ms"][1] / args.steps, "X": p["stage_ms"][2] / args.steps},
+                      "x_tflops": p["x_tflops"], "clocks": p["clocks"], "gpu_launches": int(p["launches"].sum())}
     if "plain" in res and forms[0] != "plain":
         p = res["plain"]
-        line["plain"] = {"value": p["value"], "unit": UNIT, "ms_per_step": p["ms_max"] / args.steps,
-                         "stages_ms_per_step": {"F": p["stage_ms"][1] / args.steps, "X": p["stage_ms"][2] / args.steps},
-                         "x_tflops": p["x_tflops"], "clocks": p["clocks"]}
         line["tc_vs_plain"] = {"gsamps": head["value"] / p["value"],
                                "x_stage_only": (p["stage_ms"][2] / max(1e-9, sm[2]))}
+        if "fp8" in res:
+            line["fp8_vs_plain"] = {"gsamps": res["fp8"]["value"] / p["value"],
+                                    "x_stage_only": p["stage_ms"][2] / max(1e-9, res["fp8"]["stage_ms"][2])}
 
     corr = head["corr"]
     # ---- end to end through the C ABI with pinned host buffers (rank-local)
@@ -451,8 +480,7 @@ def run_gpu_arm(args):
                        "path": "fxc_process_host + fxc_get_visibilities, pinned host buffers"}
 
     if rank == 0 and not args.no_accuracy:
-        line["accuracy"] = {f: accuracy_sample(w, fx.FXC_X_TC_FP16 if f == "tc" else fx.FXC_X_PLAIN_FP32)
-                            for f in forms}
+        line["accuracy"] = {f: accuracy_sample(w, XMODES[f]) for f in forms}
     if rank == 0 and world == 1 and not args.no_cpu:
         cb = cpu_baseline_one_core()
         if cb is not None:
@@ -466,15 +494,118 @@ def run_gpu_arm(args):
     return 0
 
 
+def run_batch_arm(args):
+    """12 uneven jobs through fxc_batch_* (grouped persistent launches, CUDA graph replay,
+    autotuned plans) against the same jobs run one after another through the single-job path."""
+    import torch
+
+    import difx_tests_b200 as fx
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+    jobs = batch_jobs()
+    cfgs, host, models = [], [], []
+    total = 0
+    for jb in jobs:
+        cfg = fx.make_config(jb["nant"], jb["nchan"], jb["numffts"], jb["bw"], jb["lo"], npol=1, nsubband=jb["nsb"],
+                             sb_spacing=jb["bw"])
+        subint = fx.lib().fxc_subint_bytes(cfg)
+        pitch = (subint + 16 + 255) // 256 * 256
+        d = gen_device_data(torch, jb["nsb"], jb["nant"], 1, subint, pitch, jb["rho"], jb["seed"], dev)
+        host.append(d[:, :subint].cpu().numpy().reshape(jb["nsb"], jb["nant"], subint))
+        del d
+        models.append(delay_model(jb["nant"], jb["nchan"], jb["bw"], seed=jb["seed"]))
+        cfgs.append(cfg)
+        total += jb["nant"] * jb["nsb"] * jb["numffts"] * 2 * jb["nchan"]
+    torch.cuda.synchronize()
+
+    def timed(step, steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    b = fx.Batch(cfgs)
+    b.set_stream(stream.cuda_stream)
+    for j in range(len(jobs)):
+        b.upload(j, host[j])
+        b.set_model(j, *models[j])
+    t0 = time.perf_counter()
+    b.autotune(reps=2)
+    tune_s = time.perf_counter() - t0
+
+    def bstep():
+        b.reset()
+        b.process()
+
+    for _ in range(args.warmup):   # the first call runs eagerly, the second records the graph
+        bstep()
+    clocks = ClockSampler(0)
+    clocks.start()
+    ms_batch = timed(bstep, args.steps)
+    clk = clocks.stop()
+    plans = [b.plan(j) for j in range(len(jobs))]
+    launches = b.launch_count()
+    b.use_graph(False)
+    ms_eager = timed(bstep, max(1, args.steps // 2))
+    b.close()
+
+    # the same jobs one after another through the single-job path (device-resident input)
+    corrs = []
+    for j, cfg in enumerate(cfgs):
+        c = fx.Correlator(cfg)
+        c.set_stream(stream.cuda_stream)
+        c.upload(host[j])
+        corrs.append(c)
+    ptrs = [c.device_input() for c in corrs]
+
+    def sstep():
+        for j, c in enumerate(corrs):
+            c.reset()
+            c.process_device(ptrs[j][0], ptrs[j][1], *models[j])
+
+    for _ in range(args.warmup):
+        sstep()
+    ms_seq = timed(sstep, max(1, args.steps // 2))
+    for c in corrs:
+        c.close()
+    line = {
+        "metric": METRIC, "value": total / (ms_batch / 1e3) / 1e9, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_batch, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, config-0 generator per job)",
+        "config": {"workload": "batch of 12 uneven jobs (fxc_batch, graph replay, autotuned plans)",
+                   "jobs": [dict(nant=jb["nant"], fft=2 * jb["nchan"], nsb=jb["nsb"], numffts=jb["numffts"])
+                            for jb in jobs],
+                   "total_samples": total, "l2": "1.6 GB packed input > L2; no flush"},
+        "batch_eager": {"ms_per_step": ms_eager, "value": total / (ms_eager / 1e3) / 1e9},
+        "sequential_single_job": {"ms_per_step": ms_seq, "value": total / (ms_seq / 1e3) / 1e9},
+        "batch_vs_sequential": ms_seq / ms_batch,
+        "plans": [{"fft_block": tb, "x_variant": alt} for tb, alt in plans],
+        "autotune_s": tune_s,
+        "clocks": clk,
+        "gpu_launches": launches * args.steps,
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS))
-    ap.add_argument("--xmode", default="both", choices=["both", "tc", "plain"],
-                    help="both: the tensor-core form is the headline value, FP32 plain timed beside it")
+    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS) + ["cfg3"],
+                    help="cfg3: the batched uneven workload (12 jobs through fxc_batch_*)")
+    ap.add_argument("--xmode", default="all", choices=["all", "both", "tc", "fp8", "plain"],
+                    help="all: the FP16 tensor-core form is the headline value, the FP8 tensor-core and FP32 "
+                         "plain forms are timed beside it; both: FP16 tensor-core and plain")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
@@ -483,6 +614,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "cfg3":
+        return run_batch_arm(args)
     return run_gpu_arm(args)
 
 

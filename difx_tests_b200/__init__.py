@@ -28,6 +28,7 @@ FXC_ERR_TIMEOUT = -6
 
 FXC_X_PLAIN_FP32 = 0
 FXC_X_TC_FP16 = 1
+FXC_X_TC_FP8 = 2
 
 
 class FxcConfig(C.Structure):
@@ -78,6 +79,9 @@ SIGNATURES = {
     "fxc_host_free": (_I, [_P]),
     "fxc_compat_last_error": (_I, []),
     "fxc_correlate_noalloc":(_I, [C.POINTER(FxcConfig), _P, C.c_size_t, _DP, _DP, _I, _I, _P, _P, _I, _P]),
+    "fxc_set_plan": (_I, [_P, _I, _I]),
+    "fxc_get_plan": (_I, [_P, _IP, _IP]),
+    "fxc_autotune": (_I, [_P, _I]),
     "fxc_enable_stage_timing": (_I, [_P, _I]),
     "fxc_stage_times": (_I, [_P, _DP, C.POINTER(C.c_longlong), _I]),
     "fxc_batch_create": (_I, [C.POINTER(FxcConfig), _I, C.POINTER(_P)]),
@@ -92,6 +96,7 @@ SIGNATURES = {
     "fxc_batch_set_stream": (_I, [_P, _P]),
     "fxc_batch_synchronize": (_I, [_P]),
     "fxc_batch_use_graph": (_I, [_P, _I]),
+    "fxc_batch_launch_count": (_I, [_P]),
     "fxc_strerror": (C.c_char_p, [_I]),
     "fxc_last_cuda_error": (_I, []),
     "fxc_last_device_error": (_I, []),
@@ -221,6 +226,19 @@ class Correlator:
     def set_stream(self, stream_ptr):
         _check(_lib().fxc_set_stream(self._ctx, _P(stream_ptr)), "fxc_set_stream")
 
+    def set_plan(self, fft_block, x_variant=0):
+        _check(_lib().fxc_set_plan(self._ctx, fft_block, x_variant), "fxc_set_plan")
+
+    def plan(self):
+        tb, alt = C.c_int(), C.c_int()
+        _check(_lib().fxc_get_plan(self._ctx, C.byref(tb), C.byref(alt)), "fxc_get_plan")
+        return tb.value, alt.value
+
+    def autotune(self, reps=3):
+        """Pick the fastest F-stage FFT block and plain X tile variant on the current input and
+        delay model (needs one earlier process call); clears the accumulators."""
+        _check(_lib().fxc_autotune(self._ctx, reps), "fxc_autotune")
+
     def enable_stage_timing(self, on=True):
         _check(_lib().fxc_enable_stage_timing(self._ctx, 1 if on else 0), "fxc_enable_stage_timing")
 
@@ -335,6 +353,12 @@ class Batch:
 
     def autotune(self, reps=3):
         _check(_lib().fxc_batch_autotune(self._b, reps), "fxc_batch_autotune")
+
+    def launch_count(self):
+        n = _lib().fxc_batch_launch_count(self._b)
+        if n < 0:
+            raise FxcError(n, "fxc_batch_launch_count")
+        return n
 
     def plan(self, job):
         tb, alt = C.c_int(), C.c_int()

@@ -1,6 +1,7 @@
 // fx_api.cu -- C ABI (include/fxcorr.h): context lifetime, buffer layout and
 // the per-call launch sequence  K0 delay table -> counts -> [F stage -> X stage]
 // per chunk of FFTs -> finalise on demand.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -120,14 +121,58 @@ static int validate(const fxc_config* c)
     if (c->nchan < 128 || c->nchan > 4096 || (c->nchan & (c->nchan - 1))) return FXC_ERR_INVALID;
     if (c->nbit != 2 || c->iscomplex != 0) return FXC_ERR_UNSUPPORTED;
     if (!(c->bw > 0.0) || !std::isfinite(c->lo) || !std::isfinite(c->sb_spacing)) return FXC_ERR_INVALID;
-    if (c->xmode != FXC_X_PLAIN_FP32 && c->xmode != FXC_X_TC_FP16) return FXC_ERR_INVALID;
-    if (c->chunk_ffts < 0 || c->chunk_ffts % 64) return FXC_ERR_INVALID;
+    if (c->xmode != FXC_X_PLAIN_FP32 && c->xmode != FXC_X_TC_FP16 && c->xmode != FXC_X_TC_FP8)
+        return FXC_ERR_INVALID;
+    if (c->chunk_ffts < 0 || c->chunk_ffts % (c->xmode == FXC_X_TC_FP8 ? 128 : 64)) return FXC_ERR_INVALID;
     if ((long long)(c->numffts + 1) * 2 * c->nchan > 0x7fffffffLL) return FXC_ERR_INVALID;  // int sample offsets
     if (c->nant * c->npol > 64) return FXC_ERR_UNSUPPORTED;
     // tensor-core form: the F stage stages 16 FFTs x npol x nchan FP16 pairs in shared memory
-    if (c->xmode == FXC_X_TC_FP16 && c->npol * c->nchan > 2048) return FXC_ERR_UNSUPPORTED;
+    if (c->xmode != FXC_X_PLAIN_FP32 && c->npol * c->nchan > 2048) return FXC_ERR_UNSUPPORTED;
     return FXC_OK;
 }
+
+}  // extern "C"
+
+std::map<std::string, int> plan_cache_load()
+{
+    std::map<std::string, int> m;
+    const char* path = std::getenv("FXC_PLAN_CACHE");
+    if (!path) return m;
+    FILE* f = std::fopen(path, "r");
+    if (!f) return m;
+    char line[256];
+    while (std::fgets(line, sizeof line, f)) {
+        std::string l(line);
+        while (!l.empty() && (l.back() == '\n' || l.back() == '\r' || l.back() == ' ')) l.pop_back();
+        const size_t sp = l.rfind(' ');
+        if (sp == std::string::npos || sp == 0) continue;
+        char* end = nullptr;
+        const long v = std::strtol(l.c_str() + sp + 1, &end, 10);
+        if (end && *end == '\0') m[l.substr(0, sp)] = (int)v;
+    }
+    std::fclose(f);
+    return m;
+}
+
+void plan_cache_append(const std::vector<std::string>& lines)
+{
+    const char* path = std::getenv("FXC_PLAN_CACHE");
+    if (!path) return;
+    if (FILE* f = std::fopen(path, "a")) {
+        for (const auto& l : lines) std::fprintf(f, "%s\n", l.c_str());
+        std::fclose(f);
+    }
+}
+
+static std::string fplan_key(const fxc_config& c)
+{
+    return std::string(c.xmode == FXC_X_PLAIN_FP32 ? "F " : "H ") + std::to_string(2 * c.nchan) + " " +
+           std::to_string(c.npol);
+}
+
+static std::string xplan_key(int nsig) { return "X " + std::to_string((nsig + 7) / 8); }
+
+extern "C" {
 
 static void free_ctx(fxc_ctx* x)
 {
@@ -143,6 +188,9 @@ static void free_ctx(fxc_ctx* x)
     cudaFree(x->d_dtab);
     cudaFree(x->d_vbits);
     cudaFree(x->d_spec);
+    cudaFree(x->d_spec8);
+    cudaFree(x->d_amax);
+    cudaFree(x->d_inv);
     cudaFree(x->d_acc);
     cudaFree(x->d_counts);
     cudaFree(x->d_err);
@@ -186,17 +234,20 @@ int fxc_create(const fxc_config* cfg, fxc_ctx** out)
 
     // chunk length: spectra buffer <= ~1 GiB
     // bytes per FFT slot of the spectra buffer: plain f32x2 [sb][sig][T][chan]; TC f16 [sb][chan][rows][T]
-    const bool tc = c.xmode == FXC_X_TC_FP16;
+    // (the FP8 form adds an e4m3 copy of half that size; its chunk is a multiple of 128 FFTs)
+    const bool tc = c.xmode != FXC_X_PLAIN_FP32;
+    const bool fp8 = c.xmode == FXC_X_TC_FP8;
+    const size_t tq = fp8 ? 128 : 64;
     const size_t per_slot = tc ? (size_t)c.nsubband * c.nchan * x->rows * sizeof(uint16_t)
                                : (size_t)c.nsubband * x->nsig * c.nchan * sizeof(float2);
     size_t T = c.chunk_ffts;
     if (T == 0) {
         T = ((size_t)(tc ? 6 : 1) << 30) / per_slot;
-        T = T / 64 * 64;
-        if (T < 64) T = 64;
+        T = T / tq * tq;
+        if (T < tq) T = tq;
         if (T > 4096) T = 4096;
     }
-    T = std::min(T, round_up((size_t)c.numffts, 64));
+    T = std::min(T, round_up((size_t)c.numffts, tq));
     x->T = (int)T;
     x->spec_bytes = per_slot * T;
 
@@ -229,6 +280,13 @@ int fxc_create(const fxc_config* cfg, fxc_ctx** out)
     if ((e = cudaMalloc(&x->d_vbits, sizeof(uint32_t) * (size_t)c.nant * (x->ld / 32))) != cudaSuccess) return fail(e);
     if ((e = cudaMalloc(&x->d_spec, x->spec_bytes)) != cudaSuccess) return fail(e);
     if ((e = cudaMemset(x->d_spec, 0, x->spec_bytes)) != cudaSuccess) return fail(e);
+    if (fp8) {
+        const size_t n8 = x->spec_bytes / 2, nsc = (size_t)c.nsubband * c.nchan * x->nsig;
+        if ((e = cudaMalloc(&x->d_spec8, n8)) != cudaSuccess) return fail(e);
+        if ((e = cudaMemset(x->d_spec8, 0, n8)) != cudaSuccess) return fail(e);   // padding rows stay zero
+        if ((e = cudaMalloc(&x->d_amax, nsc * sizeof(unsigned))) != cudaSuccess) return fail(e);
+        if ((e = cudaMalloc(&x->d_inv, nsc * sizeof(float))) != cudaSuccess) return fail(e);
+    }
     if ((e = cudaMalloc(&x->d_acc, x->acc_bytes)) != cudaSuccess) return fail(e);
     if ((e = cudaMalloc(&x->d_counts, sizeof(int) * x->npair_ant)) != cudaSuccess) return fail(e);
     if ((e = cudaMalloc(&x->d_err, sizeof(int))) != cudaSuccess) return fail(e);
@@ -251,6 +309,13 @@ int fxc_create(const fxc_config* cfg, fxc_ctx** out)
         return fail(e);
     if ((e = cudaMemset(x->d_acc, 0, x->acc_bytes)) != cudaSuccess) return fail(e);
     if ((e = cudaMemset(x->d_counts, 0, sizeof(int) * x->npair_ant)) != cudaSuccess) return fail(e);
+    {
+        const auto plans = plan_cache_load();
+        auto it = plans.find(fplan_key(c));
+        if (it != plans.end() && (it->second == 8 || it->second == 16 || it->second == 32)) x->plan_tb = it->second;
+        it = plans.find(xplan_key(x->nsig));
+        if (it != plans.end() && (it->second == 0 || it->second == 1)) x->plan_alt = it->second;
+    }
     *out = x;
     return FXC_OK;
 }
@@ -377,6 +442,7 @@ FArgs ctx_fargs(fxc_ctx* x, const uint8_t* d_data, size_t pitch, int ld)
     a.spec = x->d_spec;
     a.rows = x->rows;
     a.T = x->T;
+    a.tb = x->plan_tb;
     return a;
 }
 
@@ -394,9 +460,11 @@ int fxc_process_device(fxc_ctx* x, const uint8_t* d_data, size_t pitch, const do
         if (st != FXC_OK) return st;
         FXC_CK(launch_counts(x->d_vbits, x->cfg.nant, ld / 32, x->d_counts, x->stream));
     }
-    const bool tc = x->cfg.xmode == FXC_X_TC_FP16;
+    const bool tc = x->cfg.xmode != FXC_X_PLAIN_FP32;
+    const bool fp8 = x->cfg.xmode == FXC_X_TC_FP8;
     FArgs fa = ctx_fargs(x, d_data, pitch, ld);
-    XArgs xa;
+    fa.amax = x->d_amax;
+    XArgs xa{};
     xa.spec = x->d_spec;
     xa.acc = x->d_acc;
     xa.nsig = x->nsig;
@@ -404,16 +472,28 @@ int fxc_process_device(fxc_ctx* x, const uint8_t* d_data, size_t pitch, const do
     xa.nchan = x->cfg.nchan;
     xa.nsb = x->cfg.nsubband;
     xa.rows = x->rows;
+    xa.alt = x->plan_alt;
     for (int c0 = 0; c0 < nfft; c0 += x->T) {
         fa.t_base = c0;
         fa.nfft = std::min(x->T, nfft - c0);
         {
             StageScope sc(x, 1, 1);
+            if (fp8) FXC_CK(cudaMemsetAsync(x->d_amax, 0, sizeof(unsigned) * xa.nsb * xa.nchan * xa.nsig, x->stream));
             FXC_CK(launch_fstage(x->cfg.nchan, tc ? kSpecF16 : kSpecF32, fa, x->stream));
         }
         {
-            StageScope sc(x, 2, 1);
-            FXC_CK(tc ? launch_xtc(xa, x->d_err, x->nsm, x->stream) : launch_xplain(xa, x->stream));
+            StageScope sc(x, 2, fp8 ? 2 : 1);
+            if (fp8) {
+                // the e4m3 cast of the chunk belongs to the X operand: counted with the X stage
+                FXC_CK(launch_cast_fp8(x->d_spec, x->d_amax, x->rows, x->nsig, x->T, xa.nsb * xa.nchan, x->d_spec8,
+                                       x->d_inv, x->stream));
+                XArgs x8 = xa;
+                x8.spec = x->d_spec8;
+                x8.inv_scale = x->d_inv;
+                FXC_CK(launch_xtc8(x8, x->d_err, x->nsm, x->stream));
+            } else {
+                FXC_CK(tc ? launch_xtc(xa, x->d_err, x->nsm, x->stream) : launch_xplain(xa, x->stream));
+            }
         }
     }
     return FXC_OK;
@@ -456,7 +536,7 @@ int fxc_get_visibilities_device(fxc_ctx* x, float* d_vis, int normalize)
     FXC_CK(cudaSetDevice(x->device));
     const fxc_config& c = x->cfg;
     StageScope sc(x, 3, 1);
-    FXC_CK(launch_finalize(x->d_acc, c.xmode == FXC_X_TC_FP16 ? 1 : 0, x->nsig, c.npol, c.nant, c.nchan, c.nsubband, x->d_counts, normalize,
+    FXC_CK(launch_finalize(x->d_acc, c.xmode != FXC_X_PLAIN_FP32 ? 1 : 0, x->nsig, c.npol, c.nant, c.nchan, c.nsubband, x->d_counts, normalize,
                            reinterpret_cast<float2*>(d_vis), x->stream));
     return FXC_OK;
 }
@@ -472,6 +552,99 @@ int fxc_get_visibilities(fxc_ctx* x, float* vis, int* counts, int normalize)
     FXC_CK(cudaStreamSynchronize(x->stream));
     if (counts) counts_out(x, pc, counts);
     return device_status(x);
+}
+
+int fxc_set_plan(fxc_ctx* x, int fft_block, int x_variant)
+{
+    if (!x || (fft_block != 8 && fft_block != 16 && fft_block != 32) || (x_variant != 0 && x_variant != 1))
+        return FXC_ERR_INVALID;
+    x->plan_tb = fft_block;
+    x->plan_alt = x_variant;
+    return FXC_OK;
+}
+
+int fxc_get_plan(fxc_ctx* x, int* fft_block, int* x_variant)
+{
+    if (!x) return FXC_ERR_INVALID;
+    if (fft_block) *fft_block = x->plan_tb;
+    if (x_variant) *x_variant = x->plan_alt;
+    return FXC_OK;
+}
+
+int fxc_autotune(fxc_ctx* x, int reps)
+{
+    if (!x || reps < 1) return FXC_ERR_INVALID;
+    if (!x->model_valid) return FXC_ERR_INVALID;   // needs the input and delay model of an earlier call
+    FXC_CK(cudaSetDevice(x->device));
+    const fxc_config& c = x->cfg;
+    const int nfft = std::min(x->T, c.numffts);
+    int ld = 0;
+    const std::vector<double> model = x->last_model;
+    int st = ctx_run_delay_table(x, model.data(), model.data() + 3 * c.nant, 0, nfft, &ld);
+    if (st != FXC_OK) return st;
+    const bool tc = c.xmode != FXC_X_PLAIN_FP32;
+    FArgs fa = ctx_fargs(x, x->d_in, x->pitch, ld);
+    fa.t_base = 0;
+    fa.nfft = nfft;
+    fa.amax = x->d_amax;
+    cudaEvent_t e0, e1;
+    FXC_CK(cudaEventCreate(&e0));
+    FXC_CK(cudaEventCreate(&e1));
+    auto timeit = [&](auto&& launch, float* ms) -> cudaError_t {
+        cudaError_t e = launch();   // warm-up (also sets the kernel's shared-memory limit)
+        if (e != cudaSuccess) return e;
+        if ((e = cudaEventRecord(e0, x->stream)) != cudaSuccess) return e;
+        for (int i = 0; i < reps; i++)
+            if ((e = launch()) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(e1, x->stream)) != cudaSuccess) return e;
+        if ((e = cudaEventSynchronize(e1)) != cudaSuccess) return e;
+        return cudaEventElapsedTime(ms, e0, e1);
+    };
+    cudaError_t err = cudaSuccess;
+    float best = 1e30f;
+    int best_tb = x->plan_tb;
+    for (int tb : {8, 16, 32}) {
+        fa.tb = tb;
+        float ms = 0.f;
+        err = timeit([&] { return launch_fstage(c.nchan, tc ? kSpecF16 : kSpecF32, fa, x->stream); }, &ms);
+        if (err != cudaSuccess) break;
+        if (ms < best) {
+            best = ms;
+            best_tb = tb;
+        }
+    }
+    int best_alt = x->plan_alt;
+    if (err == cudaSuccess && !tc) {
+        XArgs xa{};
+        xa.spec = x->d_spec;
+        xa.acc = x->d_acc;
+        xa.nsig = x->nsig;
+        xa.T = x->T;
+        xa.nchan = c.nchan;
+        xa.nsb = c.nsubband;
+        xa.rows = x->rows;
+        best = 1e30f;
+        for (int alt : {0, 1}) {
+            xa.alt = alt;
+            float ms = 0.f;
+            err = timeit([&] { return launch_xplain(xa, x->stream); }, &ms);
+            if (err != cudaSuccess) break;
+            if (ms < best) {
+                best = ms;
+                best_alt = alt;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (err != cudaSuccess) {
+        g_last_cuda = (int)err;
+        return FXC_ERR_CUDA;
+    }
+    x->plan_tb = best_tb;
+    x->plan_alt = best_alt;
+    plan_cache_append({fplan_key(c) + " " + std::to_string(best_tb), xplan_key(x->nsig) + " " + std::to_string(best_alt)});
+    return fxc_reset(x);   // the timing launches accumulated into the visibilities
 }
 
 int fxc_enable_stage_timing(fxc_ctx* x, int enable)

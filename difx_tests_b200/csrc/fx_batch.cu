@@ -55,24 +55,6 @@ thread_local int g_batch_cuda = 0;
 std::string fkey(int nchan, int npol) { return "F " + std::to_string(2 * nchan) + " " + std::to_string(npol); }
 std::string xkey(int nsig8) { return "X " + std::to_string(nsig8); }
 
-std::map<std::string, int> load_plans()
-{
-    std::map<std::string, int> m;
-    const char* path = std::getenv("FXC_PLAN_CACHE");
-    if (!path) return m;
-    FILE* f = std::fopen(path, "r");
-    if (!f) return m;
-    char kind[8];
-    int a = 0, b = 0, v = 0;
-    while (std::fscanf(f, "%7s", kind) == 1) {
-        if (kind[0] == 'F' && std::fscanf(f, "%d %d %d", &a, &b, &v) == 3) m["F " + std::to_string(a) + " " + std::to_string(b)] = v;
-        else if (kind[0] == 'X' && std::fscanf(f, "%d %d", &a, &v) == 2) m["X " + std::to_string(a)] = v;
-        else break;
-    }
-    std::fclose(f);
-    return m;
-}
-
 }  // namespace
 
 struct fxc_batch {
@@ -125,7 +107,7 @@ static int build_tables(fxc_batch* b)
             a.tb = b->fg[b->job_fg[j]].tb;
             fa[(size_t)r * J + j] = a;
         }
-        XArgs x;
+        XArgs x{};
         x.spec = c->d_spec;
         x.acc = c->d_acc;
         x.nsig = c->nsig;
@@ -237,7 +219,7 @@ int fxc_batch_create(const fxc_config* cfgs, int njobs, fxc_batch** out)
         return st;
     }
     // groups (plans from the cache file when present)
-    const auto plans = load_plans();
+    const auto plans = plan_cache_load();
     for (int j = 0; j < njobs; j++) {
         const fxc_ctx* c = b->ctx[j];
         int g = -1;
@@ -378,6 +360,17 @@ int fxc_batch_use_graph(fxc_batch* b, int enable)
     return FXC_OK;
 }
 
+int fxc_batch_launch_count(fxc_batch* b)
+{
+    if (!b) return FXC_ERR_INVALID;
+    if (!b->tables_valid) {
+        FB_CK(cudaSetDevice(b->device));
+        const int st = build_tables(b);
+        if (st != FXC_OK) return st;
+    }
+    return 2 * (int)b->ctx.size() + (int)b->launches.size();
+}
+
 int fxc_batch_get_plan(fxc_batch* b, int job, int* fft_block, int* x_variant)
 {
     if (!b || job < 0 || job >= (int)b->ctx.size()) return FXC_ERR_INVALID;
@@ -447,12 +440,11 @@ int fxc_batch_autotune(fxc_batch* b, int reps)
     drop_graph(b);
     b->warmed = false;
     if (st != FXC_OK) return st;
-    if (const char* path = std::getenv("FXC_PLAN_CACHE")) {
-        if (FILE* f = std::fopen(path, "a")) {
-            for (const auto& g : b->fg) std::fprintf(f, "F %d %d %d\n", 2 * g.nchan, g.npol, g.tb);
-            for (const auto& g : b->xg) std::fprintf(f, "X %d %d\n", g.nsig8, g.alt);
-            std::fclose(f);
-        }
+    {
+        std::vector<std::string> lines;
+        for (const auto& g : b->fg) lines.push_back(fkey(g.nchan, g.npol) + " " + std::to_string(g.tb));
+        for (const auto& g : b->xg) lines.push_back(xkey(g.nsig8) + " " + std::to_string(g.alt));
+        plan_cache_append(lines);
     }
     return fxc_batch_reset(b);
 }

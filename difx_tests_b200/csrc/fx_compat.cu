@@ -158,7 +158,9 @@ void processAntennasAndBaselinePara(int* nant, int* numffts, int* fftchannels, d
     cfg.bw = *bw;
     cfg.sb_spacing = *bw;
     const char* xm = std::getenv("FXC_COMPAT_XMODE");
-    cfg.xmode = (xm && std::strcmp(xm, "tc") == 0) ? FXC_X_TC_FP16 : FXC_X_PLAIN_FP32;
+    cfg.xmode = !xm ? FXC_X_PLAIN_FP32
+              : std::strcmp(xm, "tc") == 0 ? FXC_X_TC_FP16
+              : std::strcmp(xm, "fp8") == 0 ? FXC_X_TC_FP8 : FXC_X_PLAIN_FP32;
     int st;
     if (!g.ctx || !same_cfg(g.cfg, cfg)) {
         if (g.ctx) fxc_destroy(g.ctx);

@@ -4,6 +4,8 @@
 
 #include <cuda_runtime.h>
 
+#include <map>
+#include <string>
 #include <vector>
 
 #include "../../include/fxcorr.h"
@@ -30,6 +32,9 @@ struct fxc_ctx {
     uint32_t* d_vbits = nullptr;
     void* d_spec = nullptr;
     size_t spec_bytes = 0;
+    uint8_t* d_spec8 = nullptr;   // FP8 form: e4m3 spectra [nsb][nchan][rows][T]
+    unsigned* d_amax = nullptr;   // FP8 form: [nsb*nchan][nsig] absmax bits of the chunk
+    float* d_inv = nullptr;       // FP8 form: [nsb*nchan][nsig] inverse scales
     float2* d_acc = nullptr;
     size_t acc_bytes = 0;
     int* d_counts = nullptr;
@@ -54,7 +59,16 @@ struct fxc_ctx {
     std::vector<cudaEvent_t> event_pool;
     double stage_ms[FXC_NSTAGE] = {0, 0, 0, 0};
     long long stage_launches[FXC_NSTAGE] = {0, 0, 0, 0};
+    // launch plan (fxc_set_plan / fxc_autotune / plan cache): FFTs per F-stage CTA, plain X tile variant
+    int plan_tb = 16;
+    int plan_alt = 0;
 };
+
+// Plan cache (file named by FXC_PLAN_CACHE): lines "<key...> <value>", later lines win.
+// Keys: "F <fft> <npol>" FFTs per CTA of the FP32-output F stage, "H <fft> <npol>" of the
+// F16-output F stage, "X <signal blocks of 8>" plain X tile variant.
+std::map<std::string, int> plan_cache_load();
+void plan_cache_append(const std::vector<std::string>& lines);
 
 // delay model to the device (only when it changed) + K0 over FFTs first..first+nfft-1
 int ctx_run_delay_table(fxc_ctx* x, const double* delays, const double* offs, int first, int nfft, int* ld_out);

@@ -425,6 +425,7 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
             const int k = e - pol * C;
             const int sig = ant * NPOL + pol;
             uint32_t rw[TB / 2], iw[TB / 2];
+            __half2 mx = __float2half2_rn(0.f);
 #pragma unroll
             for (int q = 0; q < TB / 2; q++) {
                 const __half2 h0 = stage[(pol * TB + 2 * q) * C + k];
@@ -433,6 +434,13 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
                 const __half2 i2 = __highs2half2(h0, h1);
                 rw[q] = *reinterpret_cast<const uint32_t*>(&r2);
                 iw[q] = *reinterpret_cast<const uint32_t*>(&i2);
+                mx = __hmax2(mx, __hmax2(__habs2(h0), __habs2(h1)));
+            }
+            if (args.amax) {
+                // FP8 form: running max(|Re|, |Im|) of the F16 values over the chunk; non-negative
+                // floats order like their bit patterns
+                const float m = fmaxf(__low2float(mx), __high2float(mx));
+                if (m > 0.f) atomicMax(args.amax + ((size_t)sb * C + k) * (args.nant * NPOL) + sig, __float_as_uint(m));
             }
             __half* dst = spec + (((size_t)sb * C + k) * args.rows + 2 * sig) * (size_t)args.T + tb0;
 #pragma unroll

@@ -8,6 +8,10 @@
 //   spectra (F32)  f32x2 [nsb][nsig][T][nchan]     plain X stage input, channel-contiguous
 //   spectra (F16)  f16  [nsb][nchan][rows][T]      tensor-core X stage input, K(=time)-major;
 //                                                  row 2*sig = Re, 2*sig+1 = Im, rows padded
+//   spectra (F8)   e4m3 [nsb][nchan][rows][T]      FP8 form: the F16 spectra times 448/absmax
+//   absmax         u32  [nsb*nchan][nsig]          FP8 form: float bits of max(|Re|,|Im|) over
+//                                                  the chunk, per signal and channel
+//   inverse scale  f32  [nsb*nchan][nsig]          FP8 form: absmax/448 (1 when absmax = 0)
 //   accumulators   f32x2 [nsb][npair][nchan]       plain form, pair = upper-triangle (i<=j)
 //                  f32x2 [nsb][nchan][npair]       tensor-core form
 //   counts         i32  [npair_ant]                antenna pairs (a1<=a2) incl. autos
@@ -48,6 +52,7 @@ struct FArgs {
     void* spec;                 // spectra buffer (layout per SpecMode)
     int rows;                   // F16 layout: rows per channel (>= 2*nsig)
     int tb;                     // FFTs per CTA (8, 16 or 32; 0 = 16), chosen by the plan / autotuner
+    unsigned* amax;             // F16 layout, FP8 form: running absmax per (sb*nchan + chan, sig), or null
 };
 
 
@@ -57,6 +62,7 @@ struct XArgs {
     int nsig, T, nchan, nsb;
     int rows;
     int alt;     // plain-form tile variant: 0 = default, 1 = alternative (chosen by the plan / autotuner)
+    const float* inv_scale;   // FP8 form: [nsb*nchan][nsig] factors applied to each Gram product
 };
 
 }  // namespace fx

@@ -22,6 +22,11 @@ cudaError_t launch_xplain_batch(int nsig, int alt, const XArgs* d_jobs, const in
                                 cudaStream_t st);
 int xplain_channel_group(int nsig, int alt);
 cudaError_t launch_xtc(const XArgs& a, int* d_err, int nsm, cudaStream_t st);
+// FP8 form: e4m3 copy of the F16 spectra scaled by 448/absmax per (item = sb*nchan + chan, signal),
+// then the e4m3 Gram with the inverse scales applied per product
+cudaError_t launch_cast_fp8(const void* spec16, const unsigned* amax, int rows, int nsig, int T, int nitems,
+                            uint8_t* spec8, float* inv_scale, cudaStream_t st);
+cudaError_t launch_xtc8(const XArgs& a, int* d_err, int nsm, cudaStream_t st);
 size_t xtc_smem_bytes();
 cudaError_t launch_unpack_debug(int nchan, const FArgs& a, float* out, cudaStream_t st);
 

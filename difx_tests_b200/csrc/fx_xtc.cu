@@ -1,4 +1,4 @@
-// fx_xtc.cu -- tensor-core X stage (tcgen05, FP16 inputs, FP32 accumulation).
+// fx_xtc.cu -- tensor-core X stage (tcgen05, FP16 or FP8-E4M3 inputs, FP32 accumulation).
 //
 // Per channel c the visibility matrix V = sum_t X_t X_t^H over signals is a
 // Hermitian rank-T update.  With the spectra stored real-ified and K(=time)-major,
@@ -7,6 +7,12 @@
 //   Re V[i][j] = G[2i][2j] + G[2i+1][2j+1],   Im V[i][j] = G[2i+1][2j] - G[2i][2j+1]
 // (V[i][j] = X_i conj(X_j), kernel.c:846 with the conjugation of kernel.c:557-568).
 // One 128x128 FP32 accumulator covers up to 64 signals per channel.
+//
+// FP8 form: the F16 spectra of a chunk are cast to e4m3 after scaling every
+// (signal, channel) row pair by k = 448/absmax (absmax over the chunk, Re and Im,
+// gathered by the F stage); the Gram of the scaled rows is multiplied back by
+// 1/(k_i k_j) in the epilogue.  Same 128-byte swizzle rows, so a stage holds 128
+// FFTs and each tcgen05.mma.kind::f8f6f4 consumes K = 32.
 //
 // Persistent, warp-specialised CTA per SM; work item = (subband, channel):
 //   warp 0     TMA producer: 128-row x 64-FFT FP16 boxes (SWIZZLE_128B) into an
@@ -22,6 +28,8 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <cuda_fp8.h>
+
 #include <cstdio>
 
 #include "fx_common.cuh"
@@ -32,9 +40,9 @@ namespace fx {
 namespace tc {
 
 constexpr int BM = 128;                    // rows per channel tile (2 x 64 signals)
-constexpr int BK = 64;                     // FFTs per stage (128 B of FP16 = one swizzle row)
+constexpr int ROWB = 128;                  // bytes per stage row (one 128-byte swizzle row)
 constexpr int NSTAGE = 8;
-constexpr int STAGE_BYTES = BM * BK * 2;   // 16 KB
+constexpr int STAGE_BYTES = BM * ROWB;     // 16 KB
 constexpr int NTHREADS = 192;              // 6 warps
 constexpr int TMEM_COLS = 256;             // two 128-column FP32 accumulators
 constexpr unsigned long long WAIT_NS = 1000000000ull;   // 1 s per wait
@@ -124,14 +132,25 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr)
 constexpr uint32_t kIdesc = (1u << 4) | (0u << 7) | (0u << 10) | ((uint32_t)(128 >> 3) << 17) |
                             ((uint32_t)(128 >> 4) << 24);
 
-__device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t accumulate)
+// kind::f8f6f4 with A and B both E4M3 (format code 0) uses the same descriptor bits.
+template <bool F8>
+__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t accumulate)
 {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-        ::"r"(tmem_d), "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate)
-        : "memory");
+    if constexpr (F8) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}"
+            ::"r"(tmem_d), "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate)
+            : "memory");
+    } else {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+            ::"r"(tmem_d), "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate)
+            : "memory");
+    }
 }
 
 __device__ __forceinline__ void umma_commit(uint64_t* bar)
@@ -161,10 +180,12 @@ __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::
 
 // err: 0 ok; 1 TMA wait expired; 2 stage-free wait expired; 3 accumulator wait expired;
 //      4 epilogue wait expired; 5 drain expired
+template <bool F8>
 __global__ void __launch_bounds__(tc::NTHREADS, 1)
 k_xtc(const __grid_constant__ CUtensorMap tmap, XArgs a, int* err)
 {
     using namespace tc;
+    constexpr int BK = F8 ? ROWB : ROWB / 2;   // FFTs per stage
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     Smem& sm = *reinterpret_cast<Smem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
     const int warp = threadIdx.x >> 5;
@@ -264,9 +285,9 @@ k_xtc(const __grid_constant__ CUtensorMap tmap, XArgs a, int* err)
                     tc_fence_after();
                     const uint32_t s0 = smem_u32(sm.stage[stage]);
 #pragma unroll
-                    for (int k = 0; k < BK / 16; k++) {
+                    for (int k = 0; k < 4; k++) {   // 32 bytes of K per MMA: K16 for f16, K32 for e4m3
                         const uint64_t desc = umma_desc(s0 + k * 32);
-                        umma_f16(d, desc, desc, (kb > 0 || k > 0) ? 1u : 0u);
+                        umma<F8>(d, desc, desc, (kb > 0 || k > 0) ? 1u : 0u);
                     }
                     umma_commit(&sm.empty[stage]);
                     if (++stage == NSTAGE) {
@@ -310,6 +331,8 @@ k_xtc(const __grid_constant__ CUtensorMap tmap, XArgs a, int* err)
             }
             tc_fence_after();
             float* out = reinterpret_cast<float*>(acc + (size_t)item * npair);
+            const float* inv = F8 ? a.inv_scale + (size_t)item * nsig : nullptr;
+            const float inv_i = F8 ? inv[i < nsig ? i : 0] : 1.f;
             const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + buf * 128;
 #pragma unroll 1
             for (int cq = 0; cq < 4; cq++) {      // 32 columns = 16 signal pairs j per chunk
@@ -328,8 +351,9 @@ k_xtc(const __grid_constant__ CUtensorMap tmap, XArgs a, int* err)
                     // even row 2i holds (a, b) = (G[2i][2j], G[2i][2j+1]); odd row holds (c, d) =
                     // (G[2i+1][2j], G[2i+1][2j+1]).  Both send column 2j+1: even receives d, odd b.
                     const float other = __shfl_xor_sync(0xffffffffu, g1, 1);
-                    const float val = odd ? (g0 - other) : (g0 + other);   // Im = c - b ; Re = a + d
+                    float val = odd ? (g0 - other) : (g0 + other);   // Im = c - b ; Re = a + d
                     if (j >= i && j < nsig) {
+                        if constexpr (F8) val *= inv_i * inv[j];
                         const int p = i * nsig - (i * (i - 1)) / 2 + (j - i);
                         // fire-and-forget reduction: one owner per (channel, pair) and launch
                         atomicAdd(out + 2 * p + (odd ? 1 : 0), val);
@@ -365,27 +389,91 @@ static PFN_cuTensorMapEncodeTiled_v12000 get_encode()
 
 size_t xtc_smem_bytes() { return sizeof(tc::Smem) + 1024; }
 
-cudaError_t launch_xtc(const XArgs& a, int* d_err, int nsm, cudaStream_t st)
+template <bool F8>
+static cudaError_t launch_xtc_t(const XArgs& a, int* d_err, int nsm, cudaStream_t st)
 {
-    if (a.rows != tc::BM || a.T % tc::BK != 0 || a.nsig > 64) return cudaErrorInvalidValue;
+    constexpr int BK = F8 ? tc::ROWB : tc::ROWB / 2;
+    if (a.rows != tc::BM || a.T % BK != 0 || a.nsig > 64) return cudaErrorInvalidValue;
+    if (F8 && !a.inv_scale) return cudaErrorInvalidValue;
     auto enc = get_encode();
     if (!enc) return cudaErrorNotSupported;
     CUtensorMap map;
     const cuuint64_t dims[2] = {(cuuint64_t)a.T, (cuuint64_t)a.nsb * a.nchan * a.rows};
-    const cuuint64_t strides[1] = {(cuuint64_t)a.T * 2};
-    const cuuint32_t box[2] = {(cuuint32_t)tc::BK, (cuuint32_t)tc::BM};
+    const cuuint64_t strides[1] = {(cuuint64_t)a.T * (F8 ? 1 : 2)};
+    const cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)tc::BM};
     const cuuint32_t estr[2] = {1, 1};
-    CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, const_cast<void*>(a.spec), dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    CUresult r = enc(&map, F8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2,
+                     const_cast<void*>(a.spec), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
     const size_t sm = xtc_smem_bytes();
     static unsigned configured = 0;
-    cudaError_t e = set_smem_once(k_xtc, sm, &configured);
+    cudaError_t e = set_smem_once(k_xtc<F8>, sm, &configured);
     if (e != cudaSuccess) return e;
     const int nitems = a.nsb * a.nchan;
     const int grid = nitems < nsm ? nitems : nsm;
-    k_xtc<<<grid, tc::NTHREADS, sm, st>>>(map, a, d_err);
+    k_xtc<F8><<<grid, tc::NTHREADS, sm, st>>>(map, a, d_err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_xtc(const XArgs& a, int* d_err, int nsm, cudaStream_t st)
+{
+    return launch_xtc_t<false>(a, d_err, nsm, st);
+}
+
+cudaError_t launch_xtc8(const XArgs& a, int* d_err, int nsm, cudaStream_t st)
+{
+    return launch_xtc_t<true>(a, d_err, nsm, st);
+}
+
+// FP8 cast: one thread per 8 FFTs of one (item, row); rows >= 2*nsig stay zero.
+// The scale of signal s in item it is k = 448/absmax (1 when the rows are all zero);
+// inv_scale receives 1/k.
+__global__ void k_cast_fp8(const __half* __restrict__ spec16, const unsigned* __restrict__ amax, int rows, int nsig,
+                           int T, long long nvec, uint8_t* __restrict__ spec8, float* __restrict__ inv_scale)
+{
+    const int vpr = T / 8;                      // 8-FFT vectors per row
+    const long long per_item = (long long)2 * nsig * vpr;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nvec;
+         v += (long long)gridDim.x * blockDim.x) {
+        const long long it = v / per_item;
+        const int rem = (int)(v - it * per_item);
+        const int row = rem / vpr;
+        const int q = rem - row * vpr;
+        const int sig = row >> 1;
+        const float m = __uint_as_float(amax[it * nsig + sig]);
+        const float k = m > 0.f ? 448.f / m : 1.f;
+        if (q == 0 && (row & 1) == 0) inv_scale[it * nsig + sig] = m > 0.f ? m / 448.f : 1.f;
+        const size_t off = ((size_t)it * rows + row) * T + (size_t)q * 8;
+        const uint4 h = *reinterpret_cast<const uint4*>(spec16 + off);
+        const __half2* hp = reinterpret_cast<const __half2*>(&h);
+        uint32_t lo = 0, hi = 0;
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            float2 f = __half22float2(hp[e]);
+            f.x *= k;
+            f.y *= k;
+            const uint32_t b = (uint32_t)__nv_cvt_float2_to_fp8x2(f, __NV_SATFINITE, __NV_E4M3);
+            if (e < 2) lo |= b << (16 * e);
+            else hi |= b << (16 * (e - 2));
+        }
+        *reinterpret_cast<uint2*>(spec8 + off) = make_uint2(lo, hi);
+    }
+}
+
+cudaError_t launch_cast_fp8(const void* spec16, const unsigned* amax, int rows, int nsig, int T, int nitems,
+                            uint8_t* spec8, float* inv_scale, cudaStream_t st)
+{
+    if (T % 8 != 0 || 2 * nsig > rows) return cudaErrorInvalidValue;
+    const long long nvec = (long long)nitems * 2 * nsig * (T / 8);
+    int dev = 0, nsm = 0;
+    cudaError_t e;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    const long long want = (nvec + 255) / 256;
+    const int grid = (int)(want < (long long)nsm * 8 ? want : (long long)nsm * 8);
+    k_cast_fp8<<<grid > 0 ? grid : 1, 256, 0, st>>>(reinterpret_cast<const __half*>(spec16), amax, rows, nsig, T,
+                                                    nvec, spec8, inv_scale);
     return cudaGetLastError();
 }
 

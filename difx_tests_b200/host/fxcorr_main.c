@@ -7,10 +7,10 @@
  * COMPLEX 0, NBIT 2 -- the grammar of the reference's main.c:14-129), reads one
  * subintegration per antenna file, correlates it on the GPU and writes vis.out
  * in the reference's text format (kernel.c:570-630).  Additional keyword
- * XMODE PLAIN|TC selects the X stage; the reference host reports unknown
+ * XMODE PLAIN|TC|FP8 selects the X stage; the reference host reports unknown
  * keywords and carries on, so such files stay readable by it.
  *
- * usage: fxcorr_main [config.conf] [-o vis.out] [-b vis.bin] [-x plain|tc] [-n]
+ * usage: fxcorr_main [config.conf] [-o vis.out] [-b vis.bin] [-x plain|tc|fp8] [-n]
  *   -b  also write all visibilities (crosses then autos) and counts in binary:
  *       int32 header {nsub, nbl+nant, npol*npol, nchan}, counts int32[nbl+nant],
  *       complex float32 [nsub][nbl+nant][npol*npol][nchan]
@@ -26,6 +26,14 @@
 #include <strings.h>
 
 #include "fxcorr.h"
+
+/* X-stage form by name: TC (FP16 tensor cores), FP8 (E4M3 tensor cores), anything else plain FP32 */
+static int parse_xmode(const char* v)
+{
+    if (!strcasecmp(v, "TC")) return FXC_X_TC_FP16;
+    if (!strcasecmp(v, "FP8")) return FXC_X_TC_FP8;
+    return FXC_X_PLAIN_FP32;
+}
 
 typedef struct {
     int nbit, npol, iscomplex, nchan, nant, numffts, xmode;
@@ -102,7 +110,7 @@ static int parse_conf(const char* path, conf_t* c)
         } else if (!strcasecmp(tok, "NUMFFTS")) {
             c->numffts = atoi(val);
         } else if (!strcasecmp(tok, "XMODE")) {
-            c->xmode = !strcasecmp(val, "TC") ? FXC_X_TC_FP16 : FXC_X_PLAIN_FP32;
+            c->xmode = parse_xmode(val);
         } else {
             fprintf(stderr, "Error: Unknown keyword \"%s\"\n", tok);
         }
@@ -147,11 +155,11 @@ int main(int argc, char** argv)
         else if (!strcmp(argv[i], "-b") && i + 1 < argc) bin_path = argv[++i];
         else if (!strcmp(argv[i], "-x") && i + 1 < argc) {
             i++;
-            xmode_cli = !strcasecmp(argv[i], "tc") ? FXC_X_TC_FP16 : FXC_X_PLAIN_FP32;
+            xmode_cli = parse_xmode(argv[i]);
         } else if (!strcmp(argv[i], "-n")) normalize = 0;
         else if (argv[i][0] != '-') conf_path = argv[i];
         else {
-            fprintf(stderr, "usage: %s [config.conf] [-o vis.out] [-b vis.bin] [-x plain|tc] [-n]\n", argv[0]);
+            fprintf(stderr, "usage: %s [config.conf] [-o vis.out] [-b vis.bin] [-x plain|tc|fp8] [-n]\n", argv[0]);
             return 1;
         }
     }

@@ -45,6 +45,8 @@ extern "C" {
 /* X-stage arithmetic */
 #define FXC_X_PLAIN_FP32 0        /* FP32 CUDA-core cross-multiply-accumulate */
 #define FXC_X_TC_FP16    1        /* tcgen05 tensor cores, FP16 inputs, FP32 accumulation */
+#define FXC_X_TC_FP8     2        /* tcgen05 tensor cores, FP8-E4M3 inputs scaled per antenna, polarisation and
+                                     channel by 448/absmax over each spectra chunk, FP32 accumulation */
 
 typedef struct fxc_config {
     int nant;          /* antennas, >= 2 */
@@ -54,7 +56,7 @@ typedef struct fxc_config {
     int iscomplex;     /* 0: real sampling (kernel.c:15) */
     int numffts;       /* FFTs per subintegration; sets the maximum sample offset (kernel.c:730) */
     int nsubband;      /* independent subbands sharing the antennas' delay model, >= 1 */
-    int xmode;         /* FXC_X_PLAIN_FP32 or FXC_X_TC_FP16 */
+    int xmode;         /* FXC_X_PLAIN_FP32, FXC_X_TC_FP16 or FXC_X_TC_FP8 */
     double lo;         /* LO (sky) frequency of subband 0, Hz; |lo| < 2^31 for reference-identical phases */
     double bw;         /* bandwidth per subband, Hz; sampling interval 1/(2 bw) (kernel.c:14) */
     double sb_spacing; /* LO step between consecutive subbands, Hz */
@@ -183,6 +185,19 @@ int fxc_batch_set_stream(fxc_batch* b, void* stream);
 int fxc_batch_synchronize(fxc_batch* b);
 /* 0 disables graph capture (every call runs eagerly), non-zero enables it (default) */
 int fxc_batch_use_graph(fxc_batch* b, int enable);
+/* kernels one fxc_batch_process call launches (delay tables, counts, grouped F and X launches);
+ * builds the task tables if needed; < 0 on error */
+int fxc_batch_launch_count(fxc_batch* b);
+
+/* Launch plan of a context: FFTs per F-stage CTA (8, 16 or 32) and plain X tile variant (0 or 1).
+ * Defaults 16 / 0, or the entries of the plan-cache file named by the environment variable
+ * FXC_PLAN_CACHE when the context is created.  Plans change speed only, never results. */
+int fxc_set_plan(fxc_ctx* ctx, int fft_block, int x_variant);
+int fxc_get_plan(fxc_ctx* ctx, int* fft_block, int* x_variant);
+/* Times every plan on the context's current input and delay model (at least one earlier
+ * fxc_process_* call) with `reps` launches each, keeps the fastest, appends it to the plan cache
+ * (when FXC_PLAN_CACHE is set) and clears the accumulators as fxc_reset does. */
+int fxc_autotune(fxc_ctx* ctx, int reps);
 
 /* Per-stage device timing (the counterpart of the reference's per-stage clock()
  * timers, kernel.c:720-821).  With enable != 0 every launch is bracketed by CUDA

@@ -16,7 +16,7 @@
  *   - nchan may be any power of two in [128, 4096] (kernel.c:31-35 requires a
  *     perfect square); stridesize is still reported as (int)sqrt(nchan);
  *   - the X stage is FP32 (1e-5 parity with kernel.c); setting the environment
- *     variable FXC_COMPAT_XMODE=tc selects the tensor-core form;
+ *     variable FXC_COMPAT_XMODE=tc (or fp8) selects the FP16 (or FP8) tensor-core form;
  *   - single-threaded like the reference (one cached GPU context per process).
  */
 #ifndef FXKERNEL_COMPAT_H

@@ -116,3 +116,22 @@ def test_batch_arguments_rejected():
     assert L.fxc_batch_upload(None, 0, None) == fx.FXC_ERR_INVALID
     assert L.fxc_batch_set_model(None, 0, None, None) == fx.FXC_ERR_INVALID
     L.fxc_batch_destroy(None)
+
+
+def test_fp8_form_config_rules():
+    L = fx.lib()
+    ctx = C.c_void_p()
+    cfg = fx.make_config(4, 256, 64, 32e6, 1.4e9, xmode=fx.FXC_X_TC_FP8, chunk_ffts=64)
+    assert L.fxc_create(C.byref(cfg), C.byref(ctx)) == fx.FXC_ERR_INVALID      # FP8 chunks are 128-FFT multiples
+    cfg = fx.make_config(4, 4096, 64, 32e6, 1.4e9, npol=1, xmode=fx.FXC_X_TC_FP8)
+    assert L.fxc_create(C.byref(cfg), C.byref(ctx)) == fx.FXC_ERR_UNSUPPORTED  # npol*nchan > 2048
+    cfg = fx.make_config(4, 256, 64, 32e6, 1.4e9, xmode=3)
+    assert L.fxc_create(C.byref(cfg), C.byref(ctx)) == fx.FXC_ERR_INVALID
+    assert not ctx.value
+
+
+def test_plan_arguments_rejected():
+    L = fx.lib()
+    assert L.fxc_set_plan(None, 16, 0) == fx.FXC_ERR_INVALID
+    assert L.fxc_get_plan(None, None, None) == fx.FXC_ERR_INVALID
+    assert L.fxc_autotune(None, 1) == fx.FXC_ERR_INVALID

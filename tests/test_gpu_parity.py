@@ -229,3 +229,103 @@ def test_tc_matches_plain_and_accumulates_over_chunks():
     np.testing.assert_array_equal(out[0][1], out[1][1])
     mx, rms = fo.vis_error(out[1][0][0], out[0][0][0])
     assert rms.max() < TC_RMS_TOL and mx.max() < TC_MAX_TOL
+
+
+# ---------------------------------------------------------------- FP8-E4M3 tensor-core form
+E4M3_U = 2.0 ** -4 + 2.0 ** -11   # e4m3 unit roundoff, compounded with the F16 rounding before the cast
+E4M3_SUB = 2.0 ** -10             # absolute rounding of e4m3 subnormals, in scaled units
+
+
+def fp8_error_bound(job, sb, T):
+    """Worst-case |V_fp8 - V| per product and channel from the quantisation model.
+
+    Every spectrum value x of signal s, channel c in chunk k is stored as
+    q = e4m3(x * 448 / amax[k][s][c]) with amax = max(|Re|, |Im|) over the chunk,
+    so each component carries |err| <= u |x| + 2^-10 amax / 448 and the product
+    x_i conj(x_j) carries |err| <= e_i |x_j| + |x_i| e_j + e_i e_j with
+    e = u |x| + sqrt(2) 2^-10 amax / 448.  Returned in the visibility layout
+    [nbl + nant][npol^2][nchan].
+    """
+    spec, _ = fo.channelise(job.data[sb], job.delays, job.fileoffsets, job.bw, float(job.sb_lo[sb]), job.nchan,
+                            job.npol, np.arange(job.numffts), job.numffts)
+    nsig = job.nant * job.npol
+    X = spec.reshape(nsig, job.numffts, job.nchan)
+    ax = np.abs(X)
+    B = np.zeros((job.nchan, nsig, nsig))
+    for t0 in range(0, job.numffts, T):
+        xs = X[:, t0:t0 + T]
+        a = ax[:, t0:t0 + T]
+        amax = np.maximum(np.abs(xs.real), np.abs(xs.imag)).max(axis=1)        # [sig][chan]
+        e = E4M3_U * a + np.sqrt(2.0) * E4M3_SUB * (amax / 448.0)[:, None, :]
+        At, Et = a.transpose(2, 0, 1), e.transpose(2, 0, 1)                    # [chan][sig][t]
+        B += Et @ At.transpose(0, 2, 1) + At @ Et.transpose(0, 2, 1) + Et @ Et.transpose(0, 2, 1)
+    bls = fo.baseline_order(job.nant) + [(k, k) for k in range(job.nant)]
+    out = np.zeros((len(bls), job.npol ** 2, job.nchan))
+    for bi, (j, k) in enumerate(bls):
+        for l in range(job.npol):
+            for m in range(job.npol):
+                out[bi, l * job.npol + m] = B[:, j * job.npol + l, k * job.npol + m]
+    return out
+
+
+@pytest.mark.parametrize("nant,npol,nchan,nsb,numffts,chunk", [(4, 1, 256, 1, 128, 0), (16, 2, 512, 2, 300, 128),
+                                                                (64, 1, 1024, 1, 128, 0), (33, 1, 128, 2, 200, 128),
+                                                                (8, 2, 1024, 1, 256, 256)])
+def test_fp8_vis_within_quantisation_bound(nant, npol, nchan, nsb, numffts, chunk):
+    job = synth.make_job(nant=nant, npol=npol, nchan=nchan, numffts=numffts, bw=64e6, lo=1.4e9, rho=0.1,
+                         seed=nant * 11 + nchan, nsubband=nsb)
+    with corr_for(job, xmode=fx.FXC_X_TC_FP8, chunk_ffts=chunk) as c:
+        c.process(job.data, job.delays, job.fileoffsets)
+        vis, counts = c.visibilities()
+    T = chunk if chunk else int(np.ceil(numffts / 128) * 128)
+    for sb in range(nsb):
+        ref, rc = oracle_vis(job, sb)
+        np.testing.assert_array_equal(counts, rc)
+        bound = fp8_error_bound(job, sb, T)
+        err = np.abs(vis[sb] - ref)
+        # the bound is a worst case; FP32 F-stage and accumulation rounding add ~1e-6 relative
+        slack = 1e-5 * np.abs(ref).max(axis=-1, keepdims=True)
+        assert (err <= 1.01 * bound + slack).all(), f"sb {sb}: max err/bound {(err / (bound + slack)).max():.3f}"
+        mx, rms = fo.vis_error(vis[sb], ref)
+        assert rms.max() < 0.05       # loose sanity bound; the per-product bound above is the contract
+
+
+def test_fp8_accumulates_over_calls_like_plain():
+    job = synth.make_job(nant=24, npol=1, nchan=1024, numffts=512, bw=64e6, lo=1.4e9, rho=0.1, seed=37)
+    out = {}
+    for mode in (fx.FXC_X_PLAIN_FP32, fx.FXC_X_TC_FP8):
+        with corr_for(job, xmode=mode, chunk_ffts=256) as c:
+            c.process(job.data, job.delays, job.fileoffsets, 0, 256)
+            c.process(job.data, job.delays, job.fileoffsets, 256, 256)
+            out[mode] = c.visibilities(normalize=True)
+    np.testing.assert_array_equal(out[0][1], out[2][1])
+    mx, rms = fo.vis_error(out[2][0][0], out[0][0][0])
+    assert rms.max() < 0.05
+
+
+@pytest.mark.parametrize("xmode", [fx.FXC_X_PLAIN_FP32, fx.FXC_X_TC_FP16])
+def test_plans_change_speed_not_results(xmode, tmp_path, monkeypatch):
+    job = synth.make_job(nant=12, npol=2, nchan=512, numffts=256, bw=64e6, lo=1.4e9, rho=0.1, seed=77)
+    ref = None
+    with corr_for(job, xmode=xmode) as c:
+        for tb, alt in [(16, 0), (8, 1), (32, 0)]:
+            c.set_plan(tb, alt)
+            c.reset()
+            c.process(job.data, job.delays, job.fileoffsets)
+            vis = c.visibilities()[0]
+            if ref is None:
+                ref = vis
+            else:
+                np.testing.assert_array_equal(vis, ref)
+        with pytest.raises(fx.FxcError):
+            c.set_plan(12, 0)
+        cache = tmp_path / "plans.txt"
+        monkeypatch.setenv("FXC_PLAN_CACHE", str(cache))
+        c.autotune(reps=2)
+        tuned = c.plan()
+        c.process(job.data, job.delays, job.fileoffsets)
+        np.testing.assert_array_equal(c.visibilities()[0], ref)
+    key = ("F " if xmode == fx.FXC_X_PLAIN_FP32 else "H ") + "1024 2 "
+    assert any(line.startswith(key) for line in cache.read_text().splitlines())
+    with corr_for(job, xmode=xmode) as c2:
+        assert c2.plan() == tuned
