@@ -233,6 +233,46 @@ __device__ __forceinline__ float2 rot_entry(int e, const DelayEntry& d, double l
     return make_float2(cs, sn);
 }
 
+// One (polarisation, channel) row pair of the F16 layout: NR consecutive FFTs from
+// the stage (element q at src[q * C], Re/Im half2) to the Re row at dst and
+// the Im row at dst + T; for the FP8 form also the running absmax.
+template <int NR, int NPOL, int C>
+__device__ __forceinline__ void flush_row(const FArgs& args, const __half2* src, int sb, int ant, int pol, int k,
+                                          __half* dst)
+{
+    static_assert(NR >= 4 && NR % 4 == 0, "row segments of 8 bytes or more");
+    uint32_t rw[NR / 2], iw[NR / 2];
+    __half2 mx = __float2half2_rn(0.f);
+#pragma unroll
+    for (int q = 0; q < NR / 2; q++) {
+        const __half2 h0 = src[(2 * q) * C];
+        const __half2 h1 = src[(2 * q + 1) * C];
+        const __half2 r2 = __lows2half2(h0, h1);
+        const __half2 i2 = __highs2half2(h0, h1);
+        rw[q] = *reinterpret_cast<const uint32_t*>(&r2);
+        iw[q] = *reinterpret_cast<const uint32_t*>(&i2);
+        mx = __hmax2(mx, __hmax2(__habs2(h0), __habs2(h1)));
+    }
+    if (args.amax) {
+        // FP8 form: running max(|Re|, |Im|) of the F16 values over the chunk; non-negative
+        // floats order like their bit patterns
+        const float m = fmaxf(__low2float(mx), __high2float(mx));
+        if (m > 0.f) atomicMax(args.amax + ((size_t)sb * C + k) * (args.nant * NPOL) + ant * NPOL + pol,
+                               __float_as_uint(m));
+    }
+    if constexpr (NR == 4) {
+        *reinterpret_cast<uint2*>(dst) = make_uint2(rw[0], rw[1]);
+        *reinterpret_cast<uint2*>(dst + args.T) = make_uint2(iw[0], iw[1]);
+    } else {
+#pragma unroll
+        for (int q = 0; q < NR / 8; q++) {
+            reinterpret_cast<uint4*>(dst)[q] = make_uint4(rw[4 * q], rw[4 * q + 1], rw[4 * q + 2], rw[4 * q + 3]);
+            reinterpret_cast<uint4*>(dst + args.T)[q] =
+                make_uint4(iw[4 * q], iw[4 * q + 1], iw[4 * q + 2], iw[4 * q + 3]);
+        }
+    }
+}
+
 template <int F>
 using Tw2Of = PassTw<F, (FPlan<F>::NPASS > 2 ? 2 : 1)>;
 
@@ -282,14 +322,20 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
         nvec = (F * NPOL / 4 + 1 + (first - base) + 15) >> 4;
     };
 
+    // Items (polarisation-major: item = pol * TB + FFT) are dealt to the slots in
+    // contiguous runs of SEG, so with SEG >= 4 every slot owns whole row segments
+    // of the F16 layout and flushes them itself, without a CTA-wide barrier.
+    constexpr int SEG = (NITEM >= P::NSLOT) ? NITEM / P::NSLOT : 1;
+    const int item_end = min(slot * SEG + SEG, NITEM);
+
     // prefetch of the first item's delay entry and input vector
-    int item = slot;
+    int item = slot * SEG;
     DelayEntry dn;
     bool vn = false;
     int basen = 0, nvecn = 0;
     uint4 pf = make_uint4(0, 0, 0, 0);
-    if (item < NITEM && tb0 + item / NPOL < args.nfft) {
-        dn = dtab[tb0 + item / NPOL];
+    if (item < item_end && tb0 + item % TB < args.nfft) {
+        dn = dtab[tb0 + item % TB];
         vn = dn.valid != 0;
     }
     if (vn) {
@@ -297,9 +343,9 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
         if (t < nvecn) pf = __ldg(reinterpret_cast<const uint4*>(row + basen) + t);
     }
 
-    for (; item < NITEM; item += P::NSLOT) {
-        const int tl = item / NPOL;
-        const int pol = item - tl * NPOL;
+    for (; item < item_end; item++) {
+        const int pol = item / TB;
+        const int tl = item - pol * TB;
         const int tc = tb0 + tl;                    // FFT slot within the chunk
         const DelayEntry d = dn;
         const bool valid = vn;
@@ -307,10 +353,10 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
         if (valid && t < nvecn) reinterpret_cast<uint4*>(inb)[t] = pf;
         // ---- prefetch the next item of this slot
         {
-            const int ni = item + P::NSLOT;
+            const int ni = item + 1;
             vn = false;
-            if (ni < NITEM && tb0 + ni / NPOL < args.nfft) {
-                dn = dtab[tb0 + ni / NPOL];
+            if (ni < item_end && tb0 + ni % TB < args.nfft) {
+                dn = dtab[tb0 + ni % TB];
                 vn = dn.valid != 0;
             }
             if (vn) {
@@ -417,37 +463,30 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
     }
 
     if constexpr (MODE == kSpecF16) {
-        __syncthreads();
-        // flush: one (pol, channel) per thread -> Re row and Im row, TB halves each
         __half* spec = reinterpret_cast<__half*>(args.spec);
-        for (int e = tid; e < NPOL * C; e += P::NTHREADS) {
-            const int pol = e / C;
-            const int k = e - pol * C;
-            const int sig = ant * NPOL + pol;
-            uint32_t rw[TB / 2], iw[TB / 2];
-            __half2 mx = __float2half2_rn(0.f);
-#pragma unroll
-            for (int q = 0; q < TB / 2; q++) {
-                const __half2 h0 = stage[(pol * TB + 2 * q) * C + k];
-                const __half2 h1 = stage[(pol * TB + 2 * q + 1) * C + k];
-                const __half2 r2 = __lows2half2(h0, h1);
-                const __half2 i2 = __highs2half2(h0, h1);
-                rw[q] = *reinterpret_cast<const uint32_t*>(&r2);
-                iw[q] = *reinterpret_cast<const uint32_t*>(&i2);
-                mx = __hmax2(mx, __hmax2(__habs2(h0), __habs2(h1)));
+        if constexpr (SEG >= 4) {
+            // flush of this slot's rows: FFTs [tl0, tl0 + NR) of NPS polarisations (the slot's
+            // last slot_sync made its stage entries visible to all its threads)
+            constexpr int NR = SEG < TB ? SEG : TB;
+            constexpr int NPS = SEG / NR;
+            const int pol0 = (slot * SEG) / TB;
+            const int tl0 = (slot * SEG) % TB;
+            for (int e = t; e < NPS * C; e += NT) {
+                const int pol = pol0 + e / C;
+                const int k = e % C;
+                flush_row<NR, NPOL, C>(args, stage + (pol * TB + tl0) * C + k, sb, ant, pol, k,
+                                    spec + (((size_t)sb * C + k) * args.rows + 2 * (ant * NPOL + pol)) *
+                                               (size_t)args.T + tb0 + tl0);
             }
-            if (args.amax) {
-                // FP8 form: running max(|Re|, |Im|) of the F16 values over the chunk; non-negative
-                // floats order like their bit patterns
-                const float m = fmaxf(__low2float(mx), __high2float(mx));
-                if (m > 0.f) atomicMax(args.amax + ((size_t)sb * C + k) * (args.nant * NPOL) + sig, __float_as_uint(m));
-            }
-            __half* dst = spec + (((size_t)sb * C + k) * args.rows + 2 * sig) * (size_t)args.T + tb0;
-#pragma unroll
-            for (int q = 0; q < TB / 8; q++) {
-                reinterpret_cast<uint4*>(dst)[q] = make_uint4(rw[4 * q], rw[4 * q + 1], rw[4 * q + 2], rw[4 * q + 3]);
-                reinterpret_cast<uint4*>(dst + args.T)[q] =
-                    make_uint4(iw[4 * q], iw[4 * q + 1], iw[4 * q + 2], iw[4 * q + 3]);
+        } else {
+            __syncthreads();
+            // flush: one (pol, channel) per thread -> Re row and Im row, TB halves each
+            for (int e = tid; e < NPOL * C; e += P::NTHREADS) {
+                const int pol = e / C;
+                const int k = e - pol * C;
+                flush_row<TB, NPOL, C>(args, stage + (pol * TB) * C + k, sb, ant, pol, k,
+                                    spec + (((size_t)sb * C + k) * args.rows + 2 * (ant * NPOL + pol)) *
+                                               (size_t)args.T + tb0);
             }
         }
     }
