@@ -41,16 +41,20 @@ namespace tc {
 
 constexpr int BM = 128;                    // rows per channel tile (2 x 64 signals)
 constexpr int ROWB = 128;                  // bytes per stage row (one 128-byte swizzle row)
-constexpr int NSTAGE = 8;
+constexpr int NSTAGE = 8;                  // single-block Gram (up to 64 signals)
+constexpr int NSTAGE_MB = 6;               // multi-block Gram: 6 x 32 KB
 constexpr int STAGE_BYTES = BM * ROWB;     // 16 KB
 constexpr int NTHREADS = 192;              // 6 warps
 constexpr int TMEM_COLS = 256;             // two 128-column FP32 accumulators
 constexpr unsigned long long WAIT_NS = 1000000000ull;   // 1 s per wait
 
+// NST stages of SLOTS 16-KB tiles (one tile: the single-block Gram; two: tiles I and J of a
+// block pair of a multi-block Gram)
+template <int NST, int SLOTS>
 struct Smem {
-    alignas(1024) uint8_t stage[NSTAGE][STAGE_BYTES];
-    alignas(8) uint64_t full[NSTAGE];
-    uint64_t empty[NSTAGE];
+    alignas(1024) uint8_t stage[NST][SLOTS][STAGE_BYTES];
+    alignas(8) uint64_t full[NST];
+    uint64_t empty[NST];
     uint64_t acc_full[2];
     uint64_t acc_empty[2];
     uint64_t drain;          // final tcgen05.commit: every MMA of this CTA retired
@@ -178,27 +182,45 @@ __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::
 
 }  // namespace tc
 
+// Block pair bp of an nb x nb upper block triangle, row-major: (0,0), (0,1) .. (0,nb-1), (1,1) ..
+__device__ __forceinline__ void block_pair(int bp, int nb, int& I, int& J)
+{
+    I = 0;
+    while (bp >= nb - I) {
+        bp -= nb - I;
+        I++;
+    }
+    J = I + bp;
+}
+
 // err: 0 ok; 1 TMA wait expired; 2 stage-free wait expired; 3 accumulator wait expired;
 //      4 epilogue wait expired; 5 drain expired
-template <bool F8>
+//
+// Work item = (sb * nchan + c, block pair (I, J), I <= J) of the channel's Gram
+// over rows = 128 * nb (nb = 1 when MB is false: up to 64 signals, one tile per stage).
+template <bool F8, bool MB>
 __global__ void __launch_bounds__(tc::NTHREADS, 1)
 k_xtc(const __grid_constant__ CUtensorMap tmap, XArgs a, int* err)
 {
     using namespace tc;
     constexpr int BK = F8 ? ROWB : ROWB / 2;   // FFTs per stage
+    constexpr int NST = MB ? NSTAGE_MB : NSTAGE;
+    using SM = Smem<NST, MB ? 2 : 1>;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    Smem& sm = *reinterpret_cast<Smem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    SM& sm = *reinterpret_cast<SM*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     volatile int* abort_flag = &sm.abort;
 
-    const int nitems = a.nsb * a.nchan;
+    const int nb = MB ? a.rows / BM : 1;
+    const int nbp = nb * (nb + 1) / 2;
+    const int nitems = a.nsb * a.nchan * nbp;
     const int nk = a.T / BK;
     const int nsig = a.nsig;
     const int npair = nsig * (nsig + 1) / 2;
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < NSTAGE; s++) {
+        for (int s = 0; s < NST; s++) {
             mbar_init(&sm.full[s], 1);
             mbar_init(&sm.empty[s], 1);
         }
@@ -227,29 +249,36 @@ k_xtc(const __grid_constant__ CUtensorMap tmap, XArgs a, int* err)
             uint32_t phase = 0;
             long long issued = 0;
             for (int item = blockIdx.x; item < nitems && !*abort_flag; item += gridDim.x) {
-                const int row0 = item * a.rows;   // (sb * nchan + c) * rows
+                const int ic = item / nbp;
+                int I = 0, J = 0;
+                if (MB) block_pair(item - ic * nbp, nb, I, J);
+                const int rowA = ic * a.rows + I * BM;   // (sb * nchan + c) * rows + 128 I
+                const int rowB = ic * a.rows + J * BM;
+                const uint32_t bytes = (I == J) ? STAGE_BYTES : 2 * STAGE_BYTES;
                 for (int kb = 0; kb < nk; kb++) {
                     if (!mbar_wait(&sm.empty[stage], phase ^ 1, abort_flag)) {
                         if (!*abort_flag) atomicCAS(err, 0, 2);
                         *abort_flag = 1;
                         break;
                     }
-                    mbar_expect_tx(&sm.full[stage], STAGE_BYTES);
-                    tma_load_2d(&tmap, &sm.full[stage], sm.stage[stage], kb * BK, row0);
+                    mbar_expect_tx(&sm.full[stage], bytes);
+                    tma_load_2d(&tmap, &sm.full[stage], sm.stage[stage][0], kb * BK, rowA);
+                    if constexpr (MB)
+                        if (I != J) tma_load_2d(&tmap, &sm.full[stage], sm.stage[stage][1], kb * BK, rowB);
                     issued++;
-                    if (++stage == NSTAGE) {
+                    if (++stage == NST) {
                         stage = 0;
                         phase ^= 1;
                     }
                 }
             }
             // drain: every stage issued must have landed before the CTA exits
-            for (int s = 0; s < NSTAGE && issued > 0; s++) {
-                // the last NSTAGE issues are the only ones that may still be in flight
+            for (int s = 0; s < NST && issued > 0; s++) {
+                // the last NST stage fills are the only ones that may still be in flight
                 const long long idx = issued - 1 - s;
                 if (idx < 0) break;
-                const int st = (int)(idx % NSTAGE);
-                const uint32_t ph = (uint32_t)((idx / NSTAGE) & 1);
+                const int st = (int)(idx % NST);
+                const uint32_t ph = (uint32_t)((idx / NST) & 1);
                 const unsigned long long t0 = globaltimer();
                 while (!mbar_try(&sm.full[st], ph)) {
                     if (globaltimer() - t0 > WAIT_NS) {
@@ -267,6 +296,8 @@ k_xtc(const __grid_constant__ CUtensorMap tmap, XArgs a, int* err)
             int buf = 0;
             uint32_t acc_phase = 0;
             for (int item = blockIdx.x; item < nitems && !*abort_flag; item += gridDim.x) {
+                int I = 0, J = 0;
+                if (MB) block_pair(item % nbp, nb, I, J);
                 if (!mbar_wait(&sm.acc_empty[buf], acc_phase ^ 1, abort_flag)) {
                     if (!*abort_flag) atomicCAS(err, 0, 3);
                     *abort_flag = 1;
@@ -283,14 +314,14 @@ k_xtc(const __grid_constant__ CUtensorMap tmap, XArgs a, int* err)
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t s0 = smem_u32(sm.stage[stage]);
+                    const uint32_t sa = smem_u32(sm.stage[stage][0]);
+                    const uint32_t sb = (MB && I != J) ? smem_u32(sm.stage[stage][MB ? 1 : 0]) : sa;
 #pragma unroll
                     for (int k = 0; k < 4; k++) {   // 32 bytes of K per MMA: K16 for f16, K32 for e4m3
-                        const uint64_t desc = umma_desc(s0 + k * 32);
-                        umma<F8>(d, desc, desc, (kb > 0 || k > 0) ? 1u : 0u);
+                        umma<F8>(d, umma_desc(sa + k * 32), umma_desc(sb + k * 32), (kb > 0 || k > 0) ? 1u : 0u);
                     }
                     umma_commit(&sm.empty[stage]);
-                    if (++stage == NSTAGE) {
+                    if (++stage == NST) {
                         stage = 0;
                         phase ^= 1;
                     }
@@ -317,22 +348,26 @@ k_xtc(const __grid_constant__ CUtensorMap tmap, XArgs a, int* err)
     } else {
         // ------------------------------------------------------------ epilogue
         const int q = warp & 3;                  // TMEM lane quadrant of this warp
-        const int r = q * 32 + lane;             // accumulator row
-        const int i = r >> 1;                    // signal of this row
+        const int r = q * 32 + lane;             // accumulator row within the block
         const bool odd = (r & 1) != 0;
         int buf = 0;
         uint32_t acc_phase = 0;
         float2* acc = reinterpret_cast<float2*>(a.acc);
         for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+            const int ic = item / nbp;
+            int I = 0, J = 0;
+            if (MB) block_pair(item - ic * nbp, nb, I, J);
+            const int i = (I * BM + r) >> 1;        // signal of this row
             if (!mbar_wait(&sm.acc_full[buf], acc_phase, abort_flag)) {
                 if (!*abort_flag) atomicCAS(err, 0, 4);
                 *abort_flag = 1;
                 break;
             }
             tc_fence_after();
-            float* out = reinterpret_cast<float*>(acc + (size_t)item * npair);
-            const float* inv = F8 ? a.inv_scale + (size_t)item * nsig : nullptr;
+            float* out = reinterpret_cast<float*>(acc + (size_t)ic * npair);
+            const float* inv = F8 ? a.inv_scale + (size_t)ic * nsig : nullptr;
             const float inv_i = F8 ? inv[i < nsig ? i : 0] : 1.f;
+            const int pbase = i * nsig - (i * (i - 1)) / 2 - i;   // pair(i, j) = pbase + j
             const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + buf * 128;
 #pragma unroll 1
             for (int cq = 0; cq < 4; cq++) {      // 32 columns = 16 signal pairs j per chunk
@@ -345,7 +380,7 @@ k_xtc(const __grid_constant__ CUtensorMap tmap, XArgs a, int* err)
                 }
 #pragma unroll
                 for (int jj = 0; jj < 16; jj++) {
-                    const int j = cq * 16 + jj;
+                    const int j = J * (BM / 2) + cq * 16 + jj;
                     const float g0 = __uint_as_float(v[2 * jj]);      // G[r][2j]
                     const float g1 = __uint_as_float(v[2 * jj + 1]);  // G[r][2j+1]
                     // even row 2i holds (a, b) = (G[2i][2j], G[2i][2j+1]); odd row holds (c, d) =
@@ -354,9 +389,8 @@ k_xtc(const __grid_constant__ CUtensorMap tmap, XArgs a, int* err)
                     float val = odd ? (g0 - other) : (g0 + other);   // Im = c - b ; Re = a + d
                     if (j >= i && j < nsig) {
                         if constexpr (F8) val *= inv_i * inv[j];
-                        const int p = i * nsig - (i * (i - 1)) / 2 + (j - i);
                         // fire-and-forget reduction: one owner per (channel, pair) and launch
-                        atomicAdd(out + 2 * p + (odd ? 1 : 0), val);
+                        atomicAdd(out + 2 * (pbase + j) + (odd ? 1 : 0), val);
                     }
                 }
             }
@@ -387,13 +421,34 @@ static PFN_cuTensorMapEncodeTiled_v12000 get_encode()
     return fn;
 }
 
-size_t xtc_smem_bytes() { return sizeof(tc::Smem) + 1024; }
+template <bool MB>
+static size_t xtc_smem_t()
+{
+    return sizeof(tc::Smem<MB ? tc::NSTAGE_MB : tc::NSTAGE, MB ? 2 : 1>) + 1024;
+}
+
+size_t xtc_smem_bytes() { return xtc_smem_t<true>(); }
+
+template <bool F8, bool MB>
+static cudaError_t launch_xtc_t(const XArgs& a, const CUtensorMap& map, int* d_err, int nsm, cudaStream_t st)
+{
+    const size_t sm = xtc_smem_t<MB>();
+    static unsigned configured = 0;
+    cudaError_t e = set_smem_once(k_xtc<F8, MB>, sm, &configured);
+    if (e != cudaSuccess) return e;
+    const int nb = a.rows / tc::BM;
+    const long long nitems = (long long)a.nsb * a.nchan * (MB ? nb * (nb + 1) / 2 : 1);
+    const int grid = nitems < nsm ? (int)nitems : nsm;
+    k_xtc<F8, MB><<<grid, tc::NTHREADS, sm, st>>>(map, a, d_err);
+    return cudaGetLastError();
+}
 
 template <bool F8>
-static cudaError_t launch_xtc_t(const XArgs& a, int* d_err, int nsm, cudaStream_t st)
+static cudaError_t launch_xtc_f(const XArgs& a, int* d_err, int nsm, cudaStream_t st)
 {
     constexpr int BK = F8 ? tc::ROWB : tc::ROWB / 2;
-    if (a.rows != tc::BM || a.T % BK != 0 || a.nsig > 64) return cudaErrorInvalidValue;
+    if (a.rows % tc::BM != 0 || a.rows < 2 * a.nsig || a.T % BK != 0 || a.nsig > 512) return cudaErrorInvalidValue;
+    if ((long long)a.nsb * a.nchan * a.rows > 0x7fffffffLL) return cudaErrorInvalidValue;   // int TMA row coordinate
     if (F8 && !a.inv_scale) return cudaErrorInvalidValue;
     auto enc = get_encode();
     if (!enc) return cudaErrorNotSupported;
@@ -406,24 +461,18 @@ static cudaError_t launch_xtc_t(const XArgs& a, int* d_err, int nsm, cudaStream_
                      const_cast<void*>(a.spec), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                      CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
-    const size_t sm = xtc_smem_bytes();
-    static unsigned configured = 0;
-    cudaError_t e = set_smem_once(k_xtc<F8>, sm, &configured);
-    if (e != cudaSuccess) return e;
-    const int nitems = a.nsb * a.nchan;
-    const int grid = nitems < nsm ? nitems : nsm;
-    k_xtc<F8><<<grid, tc::NTHREADS, sm, st>>>(map, a, d_err);
-    return cudaGetLastError();
+    return a.rows == tc::BM ? launch_xtc_t<F8, false>(a, map, d_err, nsm, st)
+                            : launch_xtc_t<F8, true>(a, map, d_err, nsm, st);
 }
 
 cudaError_t launch_xtc(const XArgs& a, int* d_err, int nsm, cudaStream_t st)
 {
-    return launch_xtc_t<false>(a, d_err, nsm, st);
+    return launch_xtc_f<false>(a, d_err, nsm, st);
 }
 
 cudaError_t launch_xtc8(const XArgs& a, int* d_err, int nsm, cudaStream_t st)
 {
-    return launch_xtc_t<true>(a, d_err, nsm, st);
+    return launch_xtc_f<true>(a, d_err, nsm, st);
 }
 
 // FP8 cast: one thread per 8 FFTs of one (item, row); rows >= 2*nsig stay zero.

@@ -49,7 +49,7 @@ extern "C" {
                                      channel by 448/absmax over each spectra chunk, FP32 accumulation */
 
 typedef struct fxc_config {
-    int nant;          /* antennas, >= 2 */
+    int nant;          /* antennas, >= 2; nant * npol <= 64 (plain X) or <= 512 (tensor-core X) */
     int npol;          /* 1, or 2 = the reference's interleaved dual-polarisation format */
     int nchan;         /* channels per subband: power of two in [128, 4096]; FFT length 2*nchan */
     int nbit;          /* bits per sample: 2 (the reference's only unpacker, kernel.c:388-395) */

@@ -329,3 +329,29 @@ def test_plans_change_speed_not_results(xmode, tmp_path, monkeypatch):
     assert any(line.startswith(key) for line in cache.read_text().splitlines())
     with corr_for(job, xmode=xmode) as c2:
         assert c2.plan() == tuned
+
+
+# ---------------------------------------------------------------- multi-block Gram (65..512 signals)
+@pytest.mark.parametrize("nant,npol,nchan,numffts,xmode", [
+    (48, 2, 512, 64, fx.FXC_X_TC_FP16),     # 96 signals: 1 x 128-row block + padding
+    (65, 2, 256, 64, fx.FXC_X_TC_FP16),     # 130 signals: 3 blocks, odd padding
+    (200, 1, 128, 128, fx.FXC_X_TC_FP16),   # 4 blocks
+    (256, 2, 128, 64, fx.FXC_X_TC_FP16),    # 512 signals: 8 blocks, 36 block pairs per channel
+    (80, 2, 256, 128, fx.FXC_X_TC_FP8),
+])
+def test_tc_multiblock_vs_fp64_oracle(nant, npol, nchan, numffts, xmode):
+    job = synth.make_job(nant=nant, npol=npol, nchan=nchan, numffts=numffts, bw=64e6, lo=1.4e9, rho=0.1,
+                         seed=nant + nchan)
+    with corr_for(job, xmode=xmode) as c:
+        c.process(job.data, job.delays, job.fileoffsets)
+        vis, counts = c.visibilities()
+    ref, rc = oracle_vis(job)
+    np.testing.assert_array_equal(counts, rc)
+    if xmode == fx.FXC_X_TC_FP16:
+        mx, rms = fo.vis_error(vis[0], ref)
+        assert rms.max() < TC_RMS_TOL and mx.max() < TC_MAX_TOL, f"rms {rms.max():.3e} max {mx.max():.3e}"
+    else:
+        bound = fp8_error_bound(job, 0, int(np.ceil(numffts / 128) * 128))
+        err = np.abs(vis[0] - ref)
+        slack = 1e-5 * np.abs(ref).max(axis=-1, keepdims=True)
+        assert (err <= 1.01 * bound + slack).all()
