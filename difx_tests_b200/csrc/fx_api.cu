@@ -125,9 +125,9 @@ static int validate(const fxc_config* c)
         return FXC_ERR_INVALID;
     if (c->chunk_ffts < 0 || c->chunk_ffts % (c->xmode == FXC_X_TC_FP8 ? 128 : 64)) return FXC_ERR_INVALID;
     if ((long long)(c->numffts + 1) * 2 * c->nchan > 0x7fffffffLL) return FXC_ERR_INVALID;  // int sample offsets
-    // plain X: one CTA covers every 8x8 signal tile of its channels (<= 64 signals);
-    // tensor-core X: 128x128 block pairs of the Gram over up to 512 signals
-    if (c->nant * c->npol > (c->xmode == FXC_X_PLAIN_FP32 ? 64 : 512)) return FXC_ERR_UNSUPPORTED;
+    // plain X: 8x8 register tiles, one CTA per channel group (<= 64 signals) or per pair of
+    // 64-signal super-blocks; tensor-core X: 128x128 block pairs of the Gram
+    if (c->nant * c->npol > 512) return FXC_ERR_UNSUPPORTED;
     // tensor-core form: the F stage stages 16 FFTs x npol x nchan FP16 pairs in shared memory
     if (c->xmode != FXC_X_PLAIN_FP32 && c->npol * c->nchan > 2048) return FXC_ERR_UNSUPPORTED;
     return FXC_OK;

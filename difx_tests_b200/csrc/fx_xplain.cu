@@ -193,6 +193,143 @@ static cudaError_t launch_xb(const XArgs* d_jobs, const int4* d_tasks, int ntask
     return cudaGetLastError();
 }
 
+// ------------------------------------------------------------------------------
+// More than 64 signals: the signal range is cut into super-blocks of 64 and a CTA
+// owns one super-block pair (P, Q), P <= Q, for CG channels: 8 x 8 register
+// tiles of 8 x 8 signal pairs, one per thread and channel (tiles below the
+// diagonal of a diagonal pair idle).  Both super-blocks are staged per TK FFTs.
+namespace big {
+constexpr int CG = 4;            // channels per CTA
+constexpr int TK = 16;           // FFTs per stage
+constexpr int NTHREADS = 64 * CG;
+constexpr int NS = 128;          // staged signals: 64 rows (P) + 64 columns (Q)
+// element (s, tk, cl) at s*TK*CG + (s/8)*4 + tk*CG + cl: the 4-element skew per 8 signals
+// spreads the column operands of a warp's 8 tiles over the banks (2 wavefronts per load)
+constexpr int STAGE = NS * TK * CG + (NS / 8) * 4;
+__device__ __forceinline__ int off(int s, int tk, int cl) { return s * TK * CG + (s >> 3) * 4 + tk * CG + cl; }
+}  // namespace big
+
+__device__ __forceinline__ void super_pair(int bp, int nb, int& P, int& Q)
+{
+    P = 0;
+    while (bp >= nb - P) {
+        bp -= nb - P;
+        P++;
+    }
+    Q = P + bp;
+}
+
+__global__ void __launch_bounds__(big::NTHREADS, 1)
+k_xplain_big(XArgs a)
+{
+    using namespace big;
+    extern __shared__ __align__(16) unsigned char smem[];
+    float2* xs = reinterpret_cast<float2*>(smem);   // [2][STAGE]
+    const int sb = blockIdx.z;
+    const int c0 = blockIdx.x * CG;
+    const int nsig = a.nsig;
+    const int nsup = (nsig + 63) / 64;
+    int P, Q;
+    super_pair(blockIdx.y, nsup, P, Q);
+
+    const int tid = threadIdx.x;
+    const int tile = tid / CG;
+    const int cl = tid - tile * CG;
+    const int ti = tile >> 3, tj = tile & 7;
+    const bool active = !(P == Q && ti > tj);
+
+    const int C = a.nchan;
+    const float2* spec = reinterpret_cast<const float2*>(a.spec) + (size_t)sb * nsig * a.T * C;
+
+    for (int e = tid; e < 2 * STAGE; e += NTHREADS) xs[e] = make_float2(0.f, 0.f);
+    __syncthreads();
+
+    constexpr int VPR = CG / 2;   // 16-byte vectors per (s, tk)
+    auto issue = [&](int buf, int t0) {
+        float2* dst = xs + buf * STAGE;
+        for (int v = tid; v < NS * TK * VPR; v += NTHREADS) {
+            const int s = v / (TK * VPR);
+            const int r = v - s * (TK * VPR);
+            const int tk = r / VPR;
+            const int q = r - tk * VPR;
+            const int sig = (s < 64) ? P * 64 + s : Q * 64 + (s - 64);
+            if (sig < nsig) {
+                const float2* src = spec + ((size_t)sig * a.T + t0 + tk) * C + c0 + 2 * q;
+                cp_async16(dst + off(s, tk, 2 * q), src);
+            }
+        }
+        cp_async_commit();
+    };
+
+    float2 acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[i][j] = make_float2(0.f, 0.f);
+
+    const int nblk = a.T / TK;
+    issue(0, 0);
+    for (int blk = 0; blk < nblk; blk++) {
+        if (blk + 1 < nblk) {
+            issue((blk + 1) & 1, (blk + 1) * TK);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const float2* x = xs + (blk & 1) * STAGE;
+        if (active) {
+            for (int tk = 0; tk < TK; tk++) {
+                float2 xi[8];
+#pragma unroll
+                for (int ii = 0; ii < 8; ii++) xi[ii] = x[off(ti * 8 + ii, tk, cl)];
+#pragma unroll
+                for (int jj = 0; jj < 8; jj++) {
+                    const float2 xj = x[off(64 + tj * 8 + jj, tk, cl)];
+#pragma unroll
+                    for (int ii = 0; ii < 8; ii++) {
+                        acc[ii][jj].x = fmaf(xi[ii].x, xj.x, fmaf(xi[ii].y, xj.y, acc[ii][jj].x));
+                        acc[ii][jj].y = fmaf(xi[ii].y, xj.x, fmaf(-xi[ii].x, xj.y, acc[ii][jj].y));
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (!active) return;
+    float2* out = reinterpret_cast<float2*>(a.acc);
+    const size_t npair = (size_t)nsig * (nsig + 1) / 2;
+#pragma unroll
+    for (int ii = 0; ii < 8; ii++) {
+        const int i = P * 64 + ti * 8 + ii;
+#pragma unroll
+        for (int jj = 0; jj < 8; jj++) {
+            const int j = Q * 64 + tj * 8 + jj;
+            if (i <= j && j < nsig) {
+                const size_t p = (size_t)i * nsig - ((size_t)i * (i - 1)) / 2 + (j - i);
+                float2* o = out + ((size_t)sb * npair + p) * C + c0 + cl;
+                float2 cur = *o;
+                cur.x += acc[ii][jj].x;
+                cur.y += acc[ii][jj].y;
+                *o = cur;
+            }
+        }
+    }
+}
+
+static cudaError_t launch_xbig(const XArgs& a, cudaStream_t st)
+{
+    if (a.nchan % big::CG || a.T % big::TK || a.nsig > 512) return cudaErrorInvalidValue;
+    const size_t sm = 2 * (size_t)big::STAGE * sizeof(float2);
+    static unsigned configured = 0;
+    cudaError_t e = set_smem_once(k_xplain_big, sm, &configured);
+    if (e != cudaSuccess) return e;
+    const int nsup = (a.nsig + 63) / 64;
+    dim3 grid(a.nchan / big::CG, nsup * (nsup + 1) / 2, a.nsb);
+    k_xplain_big<<<grid, big::NTHREADS, sm, st>>>(a);
+    return cudaGetLastError();
+}
+
 // Tile plans per signal count: NB = ceil(nsig/8) blocks of 8 signals; CG
 // channels per CTA and TK FFTs per shared-memory stage.  Variant 0 is the
 // built-in choice, variant 1 the alternative the autotuner may pick.
@@ -223,6 +360,7 @@ int xplain_channel_group(int nsig, int alt)
 
 cudaError_t launch_xplain(const XArgs& a, cudaStream_t st)
 {
+    if (a.nsig > 64) return launch_xbig(a, st);
     const int nb = (a.nsig + 7) / 8;
     const int alt = a.alt;
     if (a.T % 16 != 0) return cudaErrorInvalidValue;  // T is a multiple of every TK

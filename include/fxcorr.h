@@ -49,7 +49,7 @@ extern "C" {
                                      channel by 448/absmax over each spectra chunk, FP32 accumulation */
 
 typedef struct fxc_config {
-    int nant;          /* antennas, >= 2; nant * npol <= 64 (plain X) or <= 512 (tensor-core X) */
+    int nant;          /* antennas, >= 2; nant * npol <= 512 (the multi-job batch: <= 64) */
     int npol;          /* 1, or 2 = the reference's interleaved dual-polarisation format */
     int nchan;         /* channels per subband: power of two in [128, 4096]; FFT length 2*nchan */
     int nbit;          /* bits per sample: 2 (the reference's only unpacker, kernel.c:388-395) */
@@ -162,7 +162,8 @@ int fxc_correlate_noalloc(const fxc_config* cfg, const uint8_t* d_data, size_t p
  * an X tile plan (CTAs stride over a task table of {job, subband, antenna or
  * channel block}), in rounds when a job needs several spectra chunks.  The first
  * call runs eagerly; later calls replay one CUDA graph of the whole sequence.
- * Plain FP32 X stage.  No counterpart in the reference (one job per run).
+ * Plain FP32 X stage, up to 64 signals per job (FXC_ERR_UNSUPPORTED otherwise).
+ * No counterpart in the reference (one job per run).
  * fxc_batch_autotune times the FFT block size (8/16/32 FFTs per CTA) of every
  * F group and the tile variant of every X group on the uploaded data, keeps the
  * fastest, and zeroes the accumulators; with the environment variable

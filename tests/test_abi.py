@@ -57,6 +57,7 @@ def test_config_helpers():
 
 @pytest.mark.parametrize("field,value,status", [
     ("nant", 1, fx.FXC_ERR_INVALID),
+    ("nant", 257, fx.FXC_ERR_UNSUPPORTED),    # 514 signals at npol 2
     ("nchan", 300, fx.FXC_ERR_INVALID),
     ("nchan", 64, fx.FXC_ERR_INVALID),
     ("npol", 3, fx.FXC_ERR_INVALID),
@@ -106,6 +107,8 @@ def test_batch_arguments_rejected():
     assert L.fxc_batch_create(C.byref(cfg), 0, C.byref(out)) == fx.FXC_ERR_INVALID
     tc = fx.make_config(4, 256, 64, 32e6, 1.4e9, xmode=fx.FXC_X_TC_FP16)
     assert L.fxc_batch_create(C.byref(tc), 1, C.byref(out)) == fx.FXC_ERR_UNSUPPORTED
+    big = fx.make_config(40, 256, 64, 32e6, 1.4e9)   # 80 signals: single-job path only
+    assert L.fxc_batch_create(C.byref(big), 1, C.byref(out)) == fx.FXC_ERR_UNSUPPORTED
     bad = fx.make_config(4, 300, 64, 32e6, 1.4e9)
     assert L.fxc_batch_create(C.byref(bad), 1, C.byref(out)) == fx.FXC_ERR_INVALID
     assert not out.value

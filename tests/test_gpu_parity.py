@@ -355,3 +355,29 @@ def test_tc_multiblock_vs_fp64_oracle(nant, npol, nchan, numffts, xmode):
         err = np.abs(vis[0] - ref)
         slack = 1e-5 * np.abs(ref).max(axis=-1, keepdims=True)
         assert (err <= 1.01 * bound + slack).all()
+
+
+@pytest.mark.parametrize("nant,npol,nchan,numffts,nsb", [(48, 2, 256, 64, 1), (65, 2, 128, 64, 2),
+                                                          (200, 1, 128, 64, 1)])
+def test_plain_multiblock_vs_fp64_oracle(nant, npol, nchan, numffts, nsb):
+    job = synth.make_job(nant=nant, npol=npol, nchan=nchan, numffts=numffts, bw=64e6, lo=1.4e9, rho=0.1,
+                         seed=3 * nant + nchan, nsubband=nsb)
+    with corr_for(job) as c:
+        c.process(job.data, job.delays, job.fileoffsets)
+        vis, counts = c.visibilities()
+    for sb in range(nsb):
+        ref, rc = oracle_vis(job, sb)
+        np.testing.assert_array_equal(counts, rc)
+        assert_vis_close(vis[sb], ref)
+
+
+def test_tc_matches_plain_multiblock():
+    job = synth.make_job(nant=70, npol=2, nchan=256, numffts=256, bw=64e6, lo=1.4e9, rho=0.1, seed=71)
+    out = {}
+    for mode in (fx.FXC_X_PLAIN_FP32, fx.FXC_X_TC_FP16):
+        with corr_for(job, xmode=mode, chunk_ffts=128) as c:
+            c.process(job.data, job.delays, job.fileoffsets)
+            out[mode] = c.visibilities(normalize=True)
+    np.testing.assert_array_equal(out[0][1], out[1][1])
+    mx, rms = fo.vis_error(out[1][0][0], out[0][0][0])
+    assert rms.max() < TC_RMS_TOL and mx.max() < TC_MAX_TOL
