@@ -37,6 +37,7 @@ class FxcConfig(C.Structure):
         ("nant", C.c_int), ("npol", C.c_int), ("nchan", C.c_int), ("nbit", C.c_int),
         ("iscomplex", C.c_int), ("numffts", C.c_int), ("nsubband", C.c_int), ("xmode", C.c_int),
         ("lo", C.c_double), ("bw", C.c_double), ("sb_spacing", C.c_double), ("chunk_ffts", C.c_int),
+        ("window_ffts", C.c_int),
     ]
 
 
@@ -70,6 +71,8 @@ SIGNATURES = {
     "fxc_process_host": (_I, [_P, C.POINTER(_P), _DP, _DP, _I, _I]),
     "fxc_process_device": (_I, [_P, _P, C.c_size_t, _DP, _DP, _I, _I]),
     "fxc_upload_input": (_I, [_P, C.POINTER(_P)]),
+    "fxc_process_device_window": (_I, [_P, _P, C.c_size_t, C.POINTER(C.c_longlong), C.c_size_t, _DP, _DP, _I, _I]),
+    "fxc_process_host_window": (_I, [_P, C.POINTER(_P), _DP, _DP, _I, _I]),
     "fxc_device_input": (_I, [_P, C.POINTER(_P), C.POINTER(C.c_size_t)]),
     "fxc_get_visibilities": (_I, [_P, _FP, _IP, _I]),
     "fxc_get_visibilities_device": (_I, [_P, _P, _I]),
@@ -136,7 +139,7 @@ def _dp(a):
 
 
 def make_config(nant, nchan, numffts, bw, lo, npol=2, nsubband=1, sb_spacing=None, xmode=FXC_X_PLAIN_FP32,
-                chunk_ffts=0) -> FxcConfig:
+                chunk_ffts=0, window_ffts=0) -> FxcConfig:
     cfg = FxcConfig()
     _lib().fxc_config_default(C.byref(cfg))
     cfg.nant, cfg.npol, cfg.nchan, cfg.numffts = nant, npol, nchan, numffts
@@ -145,6 +148,7 @@ def make_config(nant, nchan, numffts, bw, lo, npol=2, nsubband=1, sb_spacing=Non
     cfg.sb_spacing = float(bw if sb_spacing is None else sb_spacing)
     cfg.xmode = xmode
     cfg.chunk_ffts = chunk_ffts
+    cfg.window_ffts = window_ffts
     return cfg
 
 
@@ -204,6 +208,24 @@ class Correlator:
         o = np.ascontiguousarray(fileoffsets, dtype=np.float64)
         _check(_lib().fxc_process_device(self._ctx, _P(d_ptr), pitch, _dp(d), _dp(o), first_fft, nfft),
                "fxc_process_device")
+
+    def process_window(self, data, delays, fileoffsets, first_fft, nfft):
+        """Host rows of the whole subintegration; copies only the bytes of FFTs
+        [first_fft, first_fft + nfft) through the double-buffered device windows."""
+        data, ptrs = self._row_ptrs(data)
+        d = np.ascontiguousarray(delays, dtype=np.float64).reshape(-1)
+        o = np.ascontiguousarray(fileoffsets, dtype=np.float64)
+        _check(_lib().fxc_process_host_window(self._ctx, ptrs, _dp(d), _dp(o), first_fft, nfft),
+               "fxc_process_host_window")
+
+    def process_device_window(self, d_ptr, pitch, base_samples, row_bytes, delays, fileoffsets, first_fft, nfft):
+        """Device rows [nsb * nant] holding each antenna's samples from base_samples[ant]."""
+        b = np.ascontiguousarray(base_samples, dtype=np.int64)
+        d = np.ascontiguousarray(delays, dtype=np.float64).reshape(-1)
+        o = np.ascontiguousarray(fileoffsets, dtype=np.float64)
+        _check(_lib().fxc_process_device_window(self._ctx, _P(d_ptr), pitch,
+                                                b.ctypes.data_as(C.POINTER(C.c_longlong)), row_bytes, _dp(d), _dp(o),
+                                                first_fft, nfft), "fxc_process_device_window")
 
     def device_input(self):
         p, pitch = _P(), C.c_size_t()

@@ -124,6 +124,7 @@ static int validate(const fxc_config* c)
     if (c->xmode != FXC_X_PLAIN_FP32 && c->xmode != FXC_X_TC_FP16 && c->xmode != FXC_X_TC_FP8)
         return FXC_ERR_INVALID;
     if (c->chunk_ffts < 0 || c->chunk_ffts % (c->xmode == FXC_X_TC_FP8 ? 128 : 64)) return FXC_ERR_INVALID;
+    if (c->window_ffts < 0) return FXC_ERR_INVALID;
     if ((long long)(c->numffts + 1) * 2 * c->nchan > 0x7fffffffLL) return FXC_ERR_INVALID;  // int sample offsets
     // plain X: 8x8 register tiles, one CTA per channel group (<= 64 signals) or per pair of
     // 64-signal super-blocks; tensor-core X: 128x128 block pairs of the Gram
@@ -181,6 +182,12 @@ static void free_ctx(fxc_ctx* x)
     if (!x) return;
     cudaFree(x->d_in);
     cudaFree(x->d_delays);
+    for (int s = 0; s < 2; s++) {
+        cudaFree(x->d_win[s]);
+        if (x->win_ready[s]) cudaEventDestroy(x->win_ready[s]);
+        if (x->win_free[s]) cudaEventDestroy(x->win_free[s]);
+    }
+    if (x->copy_stream) cudaStreamDestroy(x->copy_stream);
     for (auto& ev : x->stage_ev)
         if (ev) cudaEventDestroy(ev);
     if (x->h_stage) cudaFreeHost(x->h_stage);
@@ -265,13 +272,17 @@ int fxc_create(const fxc_config* cfg, fxc_ctx** out)
     x->acc_bytes = (size_t)c.nsubband * x->npair * c.nchan * sizeof(float2);
     x->vis_bytes = fxc_vis_count(cfg) * sizeof(float2);
     const int stride = 1 << ((int)std::log2((double)c.nchan) / 2);
-    if ((e = cudaMalloc(&x->d_in, in_bytes)) != cudaSuccess) return fail(e);
-    if ((e = cudaMemset(x->d_in, 0, in_bytes)) != cudaSuccess) return fail(e);
-    if ((e = cudaMalloc(&x->d_delays, 4 * sizeof(double) * c.nant)) != cudaSuccess) return fail(e);
+    if (c.window_ffts == 0) {   // whole-subintegration device input (fxc_upload_input / fxc_device_input)
+        if ((e = cudaMalloc(&x->d_in, in_bytes)) != cudaSuccess) return fail(e);
+        if ((e = cudaMemset(x->d_in, 0, in_bytes)) != cudaSuccess) return fail(e);
+    }
+    x->win_ffts = c.window_ffts > 0 ? c.window_ffts : x->T;
+    if ((e = cudaMalloc(&x->d_delays, fxc_ctx::NMODEL * sizeof(double) * c.nant)) != cudaSuccess) return fail(e);
     x->d_offs = x->d_delays + 3 * c.nant;
+    x->d_win_meta = x->d_delays + 4 * c.nant;
     x->last_model.assign(4 * (size_t)c.nant, 0.0);
-    if ((e = cudaHostAlloc(&x->h_stage, fxc_ctx::NRING * 4 * sizeof(double) * c.nant, cudaHostAllocDefault)) !=
-        cudaSuccess)
+    if ((e = cudaHostAlloc(&x->h_stage, fxc_ctx::NRING * fxc_ctx::NMODEL * sizeof(double) * c.nant,
+                           cudaHostAllocDefault)) != cudaSuccess)
         return fail(e);
     for (auto& ev : x->stage_ev)
         if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
@@ -291,8 +302,9 @@ int fxc_create(const fxc_config* cfg, fxc_ctx** out)
     }
     if ((e = cudaMalloc(&x->d_acc, x->acc_bytes)) != cudaSuccess) return fail(e);
     if ((e = cudaMalloc(&x->d_counts, sizeof(int) * x->npair_ant)) != cudaSuccess) return fail(e);
-    if ((e = cudaMalloc(&x->d_err, sizeof(int))) != cudaSuccess) return fail(e);
-    if ((e = cudaMemset(x->d_err, 0, sizeof(int))) != cudaSuccess) return fail(e);
+    // d_err[0]: tensor-core X wait-expiry code; d_err[1]: input-window misses
+    if ((e = cudaMalloc(&x->d_err, 2 * sizeof(int))) != cudaSuccess) return fail(e);
+    if ((e = cudaMemset(x->d_err, 0, 2 * sizeof(int))) != cudaSuccess) return fail(e);
     if ((e = cudaMalloc(&x->d_vis, x->vis_bytes)) != cudaSuccess) return fail(e);
 
     // constant tables: per-subband LO, f32 channel angular frequencies (kernel.c:162-166)
@@ -349,12 +361,12 @@ int fxc_set_stream(fxc_ctx* x, void* s)
 // Reads (and clears) the device-side wait-expiry code; the stream must be idle.
 static int device_status(fxc_ctx* x)
 {
-    int h = 0;
-    FXC_CK(cudaMemcpy(&h, x->d_err, sizeof(int), cudaMemcpyDeviceToHost));
-    if (h != 0) {
-        FXC_CK(cudaMemset(x->d_err, 0, sizeof(int)));
-        g_last_device = h;
-        return FXC_ERR_TIMEOUT;
+    int h[2] = {0, 0};
+    FXC_CK(cudaMemcpy(h, x->d_err, 2 * sizeof(int), cudaMemcpyDeviceToHost));
+    if (h[0] != 0 || h[1] != 0) {
+        FXC_CK(cudaMemset(x->d_err, 0, 2 * sizeof(int)));
+        g_last_device = h[0] != 0 ? h[0] : h[1];
+        return h[0] != 0 ? FXC_ERR_TIMEOUT : FXC_ERR_INVALID;
     }
     return FXC_OK;
 }
@@ -370,6 +382,7 @@ int fxc_synchronize(fxc_ctx* x)
 int fxc_device_input(fxc_ctx* x, uint8_t** d, size_t* pitch)
 {
     if (!x || !d || !pitch) return FXC_ERR_INVALID;
+    if (!x->d_in) return FXC_ERR_UNSUPPORTED;
     *d = x->d_in;
     *pitch = x->pitch;
     return FXC_OK;
@@ -391,7 +404,8 @@ int fxc_host_free(void* p)
 }  // extern "C"
 
 // delays / offsets to the device, then K0 over FFTs first..first+nfft-1
-int ctx_run_delay_table(fxc_ctx* x, const double* delays, const double* offs, int first, int nfft, int* ld_out)
+int ctx_run_delay_table(fxc_ctx* x, const double* delays, const double* offs, int first, int nfft, int* ld_out,
+                        const long long* win_base, const long long* win_len)
 {
     const fxc_config& c = x->cfg;
     if (!delays || !offs || first < 0 || nfft < 1 || (long long)first + nfft > c.numffts) return FXC_ERR_INVALID;
@@ -403,6 +417,7 @@ int ctx_run_delay_table(fxc_ctx* x, const double* delays, const double* offs, in
     // pinned slots so the copy stays asynchronous (a pageable source would block
     // the host until the stream's earlier work had finished).
     const size_t nmodel = 4 * (size_t)c.nant;
+    const size_t slot_doubles = fxc_ctx::NMODEL * (size_t)c.nant;
     bool same = x->model_valid;
     for (size_t i = 0; same && i < 3 * (size_t)c.nant; i++) same = x->last_model[i] == delays[i];
     for (int i = 0; same && i < c.nant; i++) same = x->last_model[3 * c.nant + i] == offs[i];
@@ -410,7 +425,7 @@ int ctx_run_delay_table(fxc_ctx* x, const double* delays, const double* offs, in
         const int slot = x->stage_next;
         x->stage_next = (slot + 1) % fxc_ctx::NRING;
         FXC_CK(cudaEventSynchronize(x->stage_ev[slot]));
-        double* h = x->h_stage + slot * nmodel;
+        double* h = x->h_stage + slot * slot_doubles;
         std::memcpy(h, delays, 3 * sizeof(double) * c.nant);
         std::memcpy(h + 3 * c.nant, offs, sizeof(double) * c.nant);
         FXC_CK(cudaMemcpyAsync(x->d_delays, h, nmodel * sizeof(double), cudaMemcpyHostToDevice, x->stream));
@@ -418,11 +433,25 @@ int ctx_run_delay_table(fxc_ctx* x, const double* delays, const double* offs, in
         std::memcpy(x->last_model.data(), h, nmodel * sizeof(double));
         x->model_valid = true;
     }
+    if (win_base) {
+        // window bases and lengths of this call (samples; exact as doubles below 2^53)
+        const int slot = x->stage_next;
+        x->stage_next = (slot + 1) % fxc_ctx::NRING;
+        FXC_CK(cudaEventSynchronize(x->stage_ev[slot]));
+        double* h = x->h_stage + slot * slot_doubles;
+        for (int a = 0; a < c.nant; a++) {
+            h[a] = (double)win_base[a];
+            h[c.nant + a] = (double)win_len[a];
+        }
+        FXC_CK(cudaMemcpyAsync(x->d_win_meta, h, 2 * sizeof(double) * c.nant, cudaMemcpyHostToDevice, x->stream));
+        FXC_CK(cudaEventRecord(x->stage_ev[slot], x->stream));
+    }
     const int ld = (int)round_up((size_t)nfft, 128);
     const int maxoffset = (c.numffts - 1) * x->F;  // kernel.c:730
     const double sampletime = 1.0 / (2.0 * c.bw);  // kernel.c:14
-    FXC_CK(launch_delay_table(x->d_delays, x->d_offs, nullptr, first, c.nant, nfft, ld, x->F, maxoffset, sampletime,
-                              x->d_dtab, x->d_vbits, x->stream));
+    FXC_CK(launch_delay_table_window(x->d_delays, x->d_offs, nullptr, first, c.nant, nfft, ld, x->F, maxoffset,
+                                     sampletime, win_base ? x->d_win_meta : nullptr, 4 / c.npol, x->d_err + 1,
+                                     x->d_dtab, x->d_vbits, x->stream));
     *ld_out = ld;
     return FXC_OK;
 }
@@ -450,15 +479,16 @@ FArgs ctx_fargs(fxc_ctx* x, const uint8_t* d_data, size_t pitch, int ld)
 
 extern "C" {
 
-int fxc_process_device(fxc_ctx* x, const uint8_t* d_data, size_t pitch, const double* delays,
-                       const double* offs, int first, int nfft)
+}  // extern "C"
+
+// One call's correlation of device rows: whole subintegrations (win_base null) or windows.
+static int ctx_correlate(fxc_ctx* x, const uint8_t* d_data, size_t pitch, const long long* win_base,
+                         const long long* win_len, const double* delays, const double* offs, int first, int nfft)
 {
-    if (!x || !d_data || pitch < x->subint + 16 || pitch % 16 || ((uintptr_t)d_data & 15)) return FXC_ERR_INVALID;
-    FXC_CK(cudaSetDevice(x->device));
     int ld = 0;
     {
         StageScope sc(x, 0, 2);
-        int st = ctx_run_delay_table(x, delays, offs, first, nfft, &ld);
+        int st = ctx_run_delay_table(x, delays, offs, first, nfft, &ld, win_base, win_len);
         if (st != FXC_OK) return st;
         FXC_CK(launch_counts(x->d_vbits, x->cfg.nant, ld / 32, x->d_counts, x->stream));
     }
@@ -501,9 +531,140 @@ int fxc_process_device(fxc_ctx* x, const uint8_t* d_data, size_t pitch, const do
     return FXC_OK;
 }
 
+extern "C" {
+
+int fxc_process_device(fxc_ctx* x, const uint8_t* d_data, size_t pitch, const double* delays,
+                       const double* offs, int first, int nfft)
+{
+    if (!x || !d_data || pitch < x->subint + 16 || pitch % 16 || ((uintptr_t)d_data & 15)) return FXC_ERR_INVALID;
+    FXC_CK(cudaSetDevice(x->device));
+    return ctx_correlate(x, d_data, pitch, nullptr, nullptr, delays, offs, first, nfft);
+}
+
+int fxc_process_device_window(fxc_ctx* x, const uint8_t* d_data, size_t pitch, const long long* base_sample,
+                              size_t row_bytes, const double* delays, const double* offs, int first, int nfft)
+{
+    if (!x || !d_data || !base_sample || row_bytes == 0 || pitch < row_bytes + 32 || pitch % 16 ||
+        ((uintptr_t)d_data & 15))
+        return FXC_ERR_INVALID;
+    const fxc_config& c = x->cfg;
+    const int spb = 4 / c.npol;
+    std::vector<long long> len(c.nant, (long long)row_bytes * spb);
+    for (int a = 0; a < c.nant; a++)
+        if (base_sample[a] < 0 || base_sample[a] % spb) return FXC_ERR_INVALID;
+    FXC_CK(cudaSetDevice(x->device));
+    return ctx_correlate(x, d_data, pitch, base_sample, len.data(), delays, offs, first, nfft);
+}
+
+}  // extern "C"
+
+// Sample range [lo, hi) antenna `a` needs for FFTs k0..k1 (kernel.c:373-386, 733-751 in
+// plain double arithmetic).  The offset k*F - n(k) is quadratic in k (n follows the mean
+// delay q k^2 + (q + l) k + ...), so its extremes lie at the ends of the range or around
+// its vertex (F Ts - q - l) / 2q; widened by two samples for the +-1 offset nudges and
+// rounding, and at the end by the unpacker's read-ahead byte.
+static void window_range(const fxc_config& c, int F, const double* delays, const double* offs, int a, int k0,
+                         int k1, long long& lo, long long& hi)
+{
+    const double q = delays[3 * a], l = delays[3 * a + 1], cc = delays[3 * a + 2];
+    const double Ts = 1.0 / (2.0 * c.bw);
+    auto offset = [&](double k) {
+        const double mean = q * k * k + (q + l) * k + q / 2 + l / 2 + cc - q / 12;   // a/2 + b of kernel.c:383-385
+        const double nf = (mean - offs[a]) / Ts;
+        return (long long)k * F - (long long)std::trunc(nf + 0.5);
+    };
+    long long mn = std::min(offset(k0), offset(k1)), mx = std::max(offset(k0), offset(k1));
+    if (q != 0.0) {
+        const double kv = (F * Ts - q - l) / (2 * q);
+        for (double k : {std::floor(kv), std::ceil(kv)})
+            if (k > k0 && k < k1) {
+                mn = std::min(mn, offset(k));
+                mx = std::max(mx, offset(k));
+            }
+    }
+    const int spb = 4 / c.npol;   // the unpacker may read one byte past the FFT's last sample (kernel.c:402-409)
+    lo = mn - 2;
+    hi = mx + F + 2 + 2 * spb;
+}
+
+static int ensure_windows(fxc_ctx* x)
+{
+    if (x->d_win[0]) return FXC_OK;
+    const fxc_config& c = x->cfg;
+    const int spb = 4 / c.npol;
+    // a window holds win_ffts FFTs plus the spread of their delays (far below an FFT for
+    // sidereal rates) and the nudge margin: (win_ffts + 4) FFT lengths
+    x->win_cap = (long long)(x->win_ffts + 4) * x->F;
+    x->win_pitch = round_up((size_t)(x->win_cap / spb) + 32, 256);
+    const size_t bytes = (size_t)c.nsubband * c.nant * x->win_pitch;
+    for (int s = 0; s < 2; s++) {
+        FXC_CK(cudaMalloc(&x->d_win[s], bytes));
+        FXC_CK(cudaEventCreateWithFlags(&x->win_ready[s], cudaEventDisableTiming));
+        FXC_CK(cudaEventCreateWithFlags(&x->win_free[s], cudaEventDisableTiming));
+    }
+    FXC_CK(cudaStreamCreateWithFlags(&x->copy_stream, cudaStreamNonBlocking));
+    return FXC_OK;
+}
+
+extern "C" {
+
+int fxc_process_host_window(fxc_ctx* x, const uint8_t* const* data, const double* delays, const double* offs,
+                            int first, int nfft)
+{
+    if (!x || !data || !delays || !offs || first < 0 || nfft < 1 || (long long)first + nfft > x->cfg.numffts)
+        return FXC_ERR_INVALID;
+    const fxc_config& c = x->cfg;
+    for (int r = 0; r < c.nsubband * c.nant; r++)
+        if (!data[r]) return FXC_ERR_INVALID;
+    FXC_CK(cudaSetDevice(x->device));
+    int st = ensure_windows(x);
+    if (st != FXC_OK) return st;
+    const int spb = 4 / c.npol;
+    const long long total = (long long)x->subint * spb;   // samples in a host row
+    std::vector<long long> base(c.nant), len(c.nant);
+    int k = first;
+    int piece = x->win_ffts;
+    while (k < first + nfft) {
+        const int n = std::min(piece, first + nfft - k);
+        bool fits = true;
+        for (int a = 0; a < c.nant && fits; a++) {
+            long long lo, hi;
+            window_range(c, x->F, delays, offs, a, k, k + n - 1, lo, hi);
+            lo = std::max(0LL, std::min(lo, total));
+            lo -= lo % spb;
+            hi = std::max(lo, std::min(hi, total));
+            base[a] = lo;
+            len[a] = (hi - lo + spb - 1) / spb * spb;
+            fits = len[a] <= x->win_cap;
+        }
+        if (!fits) {   // delays that drift by more than the window margin: smaller pieces
+            piece = std::max(1, n / 2);
+            continue;
+        }
+        const int s = x->win_next;
+        x->win_next ^= 1;
+        // copy stream: wait until the previous user of this window is done, then fill it
+        FXC_CK(cudaStreamWaitEvent(x->copy_stream, x->win_free[s], 0));
+        for (int sb = 0; sb < c.nsubband; sb++)
+            for (int a = 0; a < c.nant; a++) {
+                const int r = sb * c.nant + a;
+                FXC_CK(cudaMemcpyAsync(x->d_win[s] + (size_t)r * x->win_pitch, data[r] + base[a] / spb,
+                                       (size_t)(len[a] / spb), cudaMemcpyHostToDevice, x->copy_stream));
+            }
+        FXC_CK(cudaEventRecord(x->win_ready[s], x->copy_stream));
+        FXC_CK(cudaStreamWaitEvent(x->stream, x->win_ready[s], 0));
+        st = ctx_correlate(x, x->d_win[s], x->win_pitch, base.data(), len.data(), delays, offs, k, n);
+        if (st != FXC_OK) return st;
+        FXC_CK(cudaEventRecord(x->win_free[s], x->stream));
+        k += n;
+    }
+    return FXC_OK;
+}
+
 int fxc_upload_input(fxc_ctx* x, const uint8_t* const* data)
 {
     if (!x || !data) return FXC_ERR_INVALID;
+    if (!x->d_in) return FXC_ERR_UNSUPPORTED;
     FXC_CK(cudaSetDevice(x->device));
     const fxc_config& c = x->cfg;
     for (int r = 0; r < c.nsubband * c.nant; r++)
@@ -517,9 +678,7 @@ int fxc_upload_input(fxc_ctx* x, const uint8_t* const* data)
 int fxc_process_host(fxc_ctx* x, const uint8_t* const* data, const double* delays, const double* offs, int first,
                      int nfft)
 {
-    const int st = fxc_upload_input(x, data);
-    if (st != FXC_OK) return st;
-    return fxc_process_device(x, x->d_in, x->pitch, delays, offs, first, nfft);
+    return fxc_process_host_window(x, data, delays, offs, first, nfft);
 }
 
 static void counts_out(fxc_ctx* x, const std::vector<int>& pc, int* counts)
@@ -577,6 +736,7 @@ int fxc_autotune(fxc_ctx* x, int reps)
 {
     if (!x || reps < 1) return FXC_ERR_INVALID;
     if (!x->model_valid) return FXC_ERR_INVALID;   // needs the input and delay model of an earlier call
+    if (!x->d_in) return FXC_ERR_UNSUPPORTED;      // times on the whole-subintegration device input
     FXC_CK(cudaSetDevice(x->device));
     const fxc_config& c = x->cfg;
     const int nfft = std::min(x->T, c.numffts);
@@ -708,6 +868,7 @@ int fxc_debug_delay_table(fxc_ctx* x, const double* delays, const double* offs, 
 int fxc_debug_unpack(fxc_ctx* x, const double* delays, const double* offs, int first, int nfft, float* out)
 {
     if (!x || !out) return FXC_ERR_INVALID;
+    if (!x->d_in) return FXC_ERR_UNSUPPORTED;
     FXC_CK(cudaSetDevice(x->device));
     int ld = 0;
     int st = ctx_run_delay_table(x, delays, offs, first, nfft, &ld);
@@ -730,6 +891,7 @@ int fxc_debug_unpack(fxc_ctx* x, const double* delays, const double* offs, int f
 int fxc_debug_spectra(fxc_ctx* x, const double* delays, const double* offs, int first, int nfft, float* out)
 {
     if (!x || !out || nfft > x->T) return FXC_ERR_INVALID;
+    if (!x->d_in) return FXC_ERR_UNSUPPORTED;
     FXC_CK(cudaSetDevice(x->device));
     int ld = 0;
     int st = ctx_run_delay_table(x, delays, offs, first, nfft, &ld);

@@ -9,9 +9,16 @@ namespace fx {
 // mean) and kernel.c:733-756 (integer offset with C truncation, fractional
 // delay, the offset == -1 / maxoffset+1 nudges, validity) in IEEE binary64
 // with every operation rounded separately, as gcc compiles it on x86-64.
+//
+// Input windows: the rows of antenna `ant` start at subintegration sample
+// win[ant] and hold win[nant + ant] samples (win null: the whole subintegration
+// from sample 0); the table stores offsets relative to the window.  A reference-valid FFT whose samples (plus the one-byte
+// read-ahead of kernel.c:402-409) are not all in the window is marked invalid
+// and raises bit kWindowMiss in *err, so nothing outside the rows is read.
 __global__ void k_delay_table(const double* __restrict__ delays, const double* __restrict__ fileoffsets,
                               const int* __restrict__ fftindex, int first, int nfft, int ld, int F, int maxoffset,
-                              double sampletime, DelayEntry* __restrict__ tab, uint32_t* __restrict__ vbits)
+                              double sampletime, const double* __restrict__ win, int nant, int spb,
+                              int* __restrict__ err, DelayEntry* __restrict__ tab, uint32_t* __restrict__ vbits)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int ant = blockIdx.y;
@@ -41,6 +48,14 @@ __global__ void k_delay_table(const double* __restrict__ delays, const double* _
             frac = dsub(frac, sampletime);
         }
         valid = (offset >= 0 && offset <= maxoffset) ? 1 : 0;
+        if (win) {
+            const long long rel = (long long)offset - (long long)win[ant];
+            if (valid && (rel < 0 || rel + F + spb > (long long)win[nant + ant])) {
+                valid = 0;
+                atomicOr(err, kWindowMiss);
+            }
+            offset = (int)rel;
+        }
         DelayEntry e;
         e.a = a;
         e.b = b;
@@ -144,9 +159,19 @@ cudaError_t launch_delay_table(const double* delays, const double* fileoffsets, 
                                int nant, int nfft, int ld, int F, int maxoffset, double sampletime, DelayEntry* tab,
                                uint32_t* vbits, cudaStream_t st)
 {
+    return launch_delay_table_window(delays, fileoffsets, fftindex, first, nant, nfft, ld, F, maxoffset, sampletime,
+                                     nullptr, 0, nullptr, tab, vbits, st);
+}
+
+cudaError_t launch_delay_table_window(const double* delays, const double* fileoffsets, const int* fftindex,
+                                      int first, int nant, int nfft, int ld, int F, int maxoffset, double sampletime,
+                                      const double* win, int spb, int* err, DelayEntry* tab, uint32_t* vbits,
+                                      cudaStream_t st)
+{
+    if (win && !err) return cudaErrorInvalidValue;
     dim3 grid((ld + 127) / 128, nant);
-    k_delay_table<<<grid, 128, 0, st>>>(delays, fileoffsets, fftindex, first, nfft, ld, F, maxoffset, sampletime, tab,
-                                        vbits);
+    k_delay_table<<<grid, 128, 0, st>>>(delays, fileoffsets, fftindex, first, nfft, ld, F, maxoffset, sampletime,
+                                        win, nant, spb, err, tab, vbits);
     return cudaGetLastError();
 }
 

@@ -36,6 +36,9 @@ struct DelayEntry {
 
 enum SpecMode { kSpecF32 = 0, kSpecF16 = 1 };
 
+// device error word bits beyond the tensor-core X stage's wait-expiry codes (1..5)
+constexpr int kWindowMiss = 1 << 4;   // an FFT's input was not inside its input window
+
 // Arguments of the fused F-stage kernel (passed by value).
 struct FArgs {
     const uint8_t* data;        // packed input [nsb][nant][pitch]

@@ -10,6 +10,13 @@ namespace fx {
 cudaError_t launch_delay_table(const double* delays, const double* fileoffsets, const int* fftindex, int first,
                                int nant, int nfft, int ld, int F, int maxoffset, double sampletime, DelayEntry* tab,
                                uint32_t* vbits, cudaStream_t st);
+// as launch_delay_table, for input windows: antenna a's rows start at sample win[a] and hold
+// win[nant + a] samples (device doubles holding integers; spb samples per byte); FFTs not inside
+// their window are left out and set kWindowMiss in *err
+cudaError_t launch_delay_table_window(const double* delays, const double* fileoffsets, const int* fftindex,
+                                      int first, int nant, int nfft, int ld, int F, int maxoffset, double sampletime,
+                                      const double* win, int spb, int* err, DelayEntry* tab, uint32_t* vbits,
+                                      cudaStream_t st);
 cudaError_t launch_counts(const uint32_t* vbits, int nant, int nwords, int* counts, cudaStream_t st);
 cudaError_t launch_finalize(const float2* acc, int acc_layout, int nsig, int npol, int nant, int nchan, int nsb,
                             const int* counts, int normalize, float2* vis, cudaStream_t st);

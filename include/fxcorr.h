@@ -61,6 +61,10 @@ typedef struct fxc_config {
     double bw;         /* bandwidth per subband, Hz; sampling interval 1/(2 bw) (kernel.c:14) */
     double sb_spacing; /* LO step between consecutive subbands, Hz */
     int chunk_ffts;    /* FFTs per F->X chunk (multiple of 64), 0 = chosen by the library */
+    int window_ffts;   /* FFTs per streamed input window (fxc_process_host*); 0 = the chunk length.
+                          > 0 also drops the whole-subintegration device input buffer, so the
+                          subintegration never has to fit in device memory (fxc_upload_input and
+                          fxc_device_input then return FXC_ERR_UNSUPPORTED) */
 } fxc_config;
 
 typedef struct fxc_ctx fxc_ctx;
@@ -90,10 +94,12 @@ int fxc_reset(fxc_ctx* ctx);
 /* Process FFTs first_fft .. first_fft+nfft-1 (0 <= first_fft, first_fft+nfft <= numffts)
  * and accumulate into the context's visibilities.  Calls accumulate, so time
  * shards of one subintegration may be processed by successive calls (the
- * reference's split/merge, main.c:398-433).
+ * reference's split/merge, main.c:398-433).  The input streams to the device in
+ * windows of window_ffts FFTs whose copies overlap the previous window's
+ * correlation (see fxc_process_host_window).
  *   data[sb*nant + ant]  host pointer to the subintegration's packed bytes
  *                        (fxc_subint_bytes each); pinned memory (fxc_host_alloc)
- *                        transfers fastest
+ *                        transfers fastest and lets copies overlap compute
  *   delays[3*ant + k]    (quad, lin, const) seconds, t in FFT units (kernel.c:378-380)
  *   fileoffsets[ant]     seconds (kernel.c:736)
  */
@@ -108,6 +114,24 @@ int fxc_process_device(fxc_ctx* ctx, const uint8_t* d_data, size_t pitch, const 
 
 /* Copy one subintegration's host input rows (data[sb*nant + ant], fxc_subint_bytes
  * each) into the context's device input buffer, asynchronously on its stream. */
+/* Streaming (no counterpart in the reference, whose host reads whole subintegrations,
+ * main.c:389-396).  Row r = sb * nant + ant of d_data holds the packed samples of that
+ * subband and antenna from subintegration sample base_sample[ant] (a whole byte: a
+ * multiple of 4/npol samples) for row_bytes bytes; pitch >= row_bytes + 32, 16-byte
+ * aligned.  Correlates FFTs [first, first + nfft).  An FFT that the reference would
+ * correlate but whose samples are not all inside its antenna's window is left out and
+ * the next synchronising call (fxc_synchronize, fxc_get_visibilities) returns
+ * FXC_ERR_INVALID; nothing outside the rows is read. */
+int fxc_process_device_window(fxc_ctx* ctx, const uint8_t* d_data, size_t pitch, const long long* base_sample,
+                              size_t row_bytes, const double* delays, const double* fileoffsets, int first,
+                              int nfft);
+/* Host rows of the whole subintegration (as fxc_process_host).  Copies only the bytes
+ * FFTs [first, first + nfft) need, window by window (window_ffts FFTs each), into one of
+ * two device windows on a copy stream, so the copy of one window overlaps the
+ * correlation of the previous one (pinned host rows, e.g. fxc_host_alloc, are needed for
+ * the overlap).  fxc_process_host is this call over its FFT range. */
+int fxc_process_host_window(fxc_ctx* ctx, const uint8_t* const* data, const double* delays,
+                            const double* fileoffsets, int first, int nfft);
 int fxc_upload_input(fxc_ctx* ctx, const uint8_t* const* data);
 
 /* The context's own device input buffer (rows of *pitch bytes) for callers
