@@ -621,12 +621,19 @@ int fxc_process_host_window(fxc_ctx* x, const uint8_t* const* data, const double
     if (st != FXC_OK) return st;
     const int spb = 4 / c.npol;
     const long long total = (long long)x->subint * spb;   // samples in a host row
+    const int nrow = c.nsubband * c.nant;
+    // rows evenly spaced in one host array: one strided copy per window over the union
+    // of the antennas' ranges (when it fits), instead of one copy per row
+    const ptrdiff_t rstride = nrow > 1 ? data[1] - data[0] : (ptrdiff_t)x->subint;
+    bool uniform = rstride >= (ptrdiff_t)x->subint;
+    for (int r = 1; r < nrow && uniform; r++) uniform = data[r] == data[0] + (ptrdiff_t)r * rstride;
     std::vector<long long> base(c.nant), len(c.nant);
     int k = first;
     int piece = x->win_ffts;
     while (k < first + nfft) {
         const int n = std::min(piece, first + nfft - k);
         bool fits = true;
+        long long ulo = total, uhi = 0;
         for (int a = 0; a < c.nant && fits; a++) {
             long long lo, hi;
             window_range(c, x->F, delays, offs, a, k, k + n - 1, lo, hi);
@@ -636,21 +643,34 @@ int fxc_process_host_window(fxc_ctx* x, const uint8_t* const* data, const double
             base[a] = lo;
             len[a] = (hi - lo + spb - 1) / spb * spb;
             fits = len[a] <= x->win_cap;
+            ulo = std::min(ulo, lo);
+            uhi = std::max(uhi, base[a] + len[a]);
         }
         if (!fits) {   // delays that drift by more than the window margin: smaller pieces
             piece = std::max(1, n / 2);
             continue;
         }
+        const bool one_copy = uniform && uhi - ulo <= x->win_cap;
+        if (one_copy)
+            for (int a = 0; a < c.nant; a++) {
+                base[a] = ulo;
+                len[a] = uhi - ulo;
+            }
         const int s = x->win_next;
         x->win_next ^= 1;
         // copy stream: wait until the previous user of this window is done, then fill it
         FXC_CK(cudaStreamWaitEvent(x->copy_stream, x->win_free[s], 0));
-        for (int sb = 0; sb < c.nsubband; sb++)
-            for (int a = 0; a < c.nant; a++) {
-                const int r = sb * c.nant + a;
-                FXC_CK(cudaMemcpyAsync(x->d_win[s] + (size_t)r * x->win_pitch, data[r] + base[a] / spb,
-                                       (size_t)(len[a] / spb), cudaMemcpyHostToDevice, x->copy_stream));
-            }
+        if (one_copy) {
+            FXC_CK(cudaMemcpy2DAsync(x->d_win[s], x->win_pitch, data[0] + ulo / spb, (size_t)rstride,
+                                     (size_t)((uhi - ulo) / spb), nrow, cudaMemcpyHostToDevice, x->copy_stream));
+        } else {
+            for (int sb = 0; sb < c.nsubband; sb++)
+                for (int a = 0; a < c.nant; a++) {
+                    const int r = sb * c.nant + a;
+                    FXC_CK(cudaMemcpyAsync(x->d_win[s] + (size_t)r * x->win_pitch, data[r] + base[a] / spb,
+                                           (size_t)(len[a] / spb), cudaMemcpyHostToDevice, x->copy_stream));
+                }
+        }
         FXC_CK(cudaEventRecord(x->win_ready[s], x->copy_stream));
         FXC_CK(cudaStreamWaitEvent(x->stream, x->win_ready[s], 0));
         st = ctx_correlate(x, x->d_win[s], x->win_pitch, base.data(), len.data(), delays, offs, k, n);
