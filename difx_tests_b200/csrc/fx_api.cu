@@ -129,8 +129,6 @@ static int validate(const fxc_config* c)
     // plain X: 8x8 register tiles, one CTA per channel group (<= 64 signals) or per pair of
     // 64-signal super-blocks; tensor-core X: 128x128 block pairs of the Gram
     if (c->nant * c->npol > 512) return FXC_ERR_UNSUPPORTED;
-    // tensor-core form: the F stage stages 16 FFTs x npol x nchan FP16 pairs in shared memory
-    if (c->xmode != FXC_X_PLAIN_FP32 && c->npol * c->nchan > 2048) return FXC_ERR_UNSUPPORTED;
     return FXC_OK;
 }
 

@@ -29,6 +29,15 @@ inline cudaError_t set_smem_once(Kern kern, size_t bytes, unsigned* mask)
     return e;
 }
 
+// Largest dynamic shared memory a block of the current device may opt in to.
+inline size_t smem_optin_limit()
+{
+    int dev = 0, v = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return 0;
+    return (size_t)v;
+}
+
 // ---------------------------------------------------------------- FP64 (no FMA)
 __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }

@@ -589,7 +589,14 @@ cudaError_t launch_fb(const FArgs* d_jobs, const int4* d_tasks, int ntask, cudaS
 template <int F>
 cudaError_t launch_fstage_F(int mode, const FArgs& a, cudaStream_t st)
 {
-    const int tb = a.tb ? a.tb : 16;
+    int tb = a.tb ? a.tb : 16;
+    if (mode == kSpecF16) {
+        // the F16 staging (tb FFTs x npol x nchan) must fit the opt-in shared memory: fewer FFTs
+        // per CTA for long FFTs with two polarisations (down to 4: 8-byte row segments)
+        const size_t lim = smem_optin_limit();
+        while (tb > 4 && fstage_smem<F>(mode, tb, a.npol) > lim) tb /= 2;
+        if (tb == 4) return a.npol == 2 ? launch_f<F, kSpecF16, 4, 2>(a, st) : launch_f<F, kSpecF16, 4, 1>(a, st);
+    }
 #define FX_TB(TBV)                                                                                      \
     if (tb == TBV) {                                                                                    \
         if (mode == kSpecF32) return a.npol == 2 ? launch_f<F, kSpecF32, TBV, 2>(a, st)                \

@@ -381,3 +381,23 @@ def test_tc_matches_plain_multiblock():
     np.testing.assert_array_equal(out[0][1], out[1][1])
     mx, rms = fo.vis_error(out[1][0][0], out[0][0][0])
     assert rms.max() < TC_RMS_TOL and mx.max() < TC_MAX_TOL
+
+
+@pytest.mark.parametrize("nant,npol,nchan,xmode", [(4, 2, 4096, fx.FXC_X_TC_FP16), (5, 2, 2048, fx.FXC_X_TC_FP16),
+                                                   (4, 1, 4096, fx.FXC_X_TC_FP16), (3, 2, 4096, fx.FXC_X_TC_FP8)])
+def test_tc_long_ffts_dual_pol(nant, npol, nchan, xmode):
+    """FFT length x polarisations beyond what 16 FFTs of F16 staging hold: fewer FFTs per CTA."""
+    job = synth.make_job(nant=nant, npol=npol, nchan=nchan, numffts=128, bw=64e6, lo=1.4e9, rho=0.1,
+                         seed=nchan + npol)
+    with corr_for(job, xmode=xmode) as c:
+        c.process(job.data, job.delays, job.fileoffsets)
+        vis, counts = c.visibilities()
+    ref, rc = oracle_vis(job)
+    np.testing.assert_array_equal(counts, rc)
+    if xmode == fx.FXC_X_TC_FP16:
+        mx, rms = fo.vis_error(vis[0], ref)
+        assert rms.max() < TC_RMS_TOL and mx.max() < TC_MAX_TOL
+    else:
+        bound = fp8_error_bound(job, 0, 128)
+        slack = 1e-5 * np.abs(ref).max(axis=-1, keepdims=True)
+        assert (np.abs(vis[0] - ref) <= 1.01 * bound + slack).all()
