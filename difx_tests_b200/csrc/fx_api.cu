@@ -211,7 +211,9 @@ static void free_ctx(fxc_ctx* x)
     delete x;
 }
 
-int fxc_create(const fxc_config* cfg, fxc_ctx** out)
+}  // extern "C"
+
+int ctx_create(const fxc_config* cfg, fxc_ctx** out, bool group_subbands)
 {
     if (!out) return FXC_ERR_INVALID;
     *out = nullptr;
@@ -239,24 +241,44 @@ int fxc_create(const fxc_config* cfg, fxc_ctx** out)
     x->pitch = round_up(x->subint + 16, 256);
     x->rows = (int)round_up((size_t)2 * x->nsig, 128);
 
-    // chunk length: spectra buffer <= ~1 GiB
-    // bytes per FFT slot of the spectra buffer: plain f32x2 [sb][sig][T][chan]; TC f16 [sb][chan][rows][T]
-    // (the FP8 form adds an e4m3 copy of half that size; its chunk is a multiple of 128 FFTs)
+    // Spectra chunk: T FFT slots of nsb_g subbands within a budget of 2 GiB (plain) / 16 GiB
+    // (tensor cores), or FXC_SPECTRA_BUDGET_MB.  Every subband goes into one chunk while that leaves >= 512 slots (or the
+    // whole call); larger problems take the subbands in groups so the chunk stays long: the
+    // tensor-core X stage adds each chunk's Gram to the accumulators once, so short chunks
+    // would make it bound by those additions.
+    // Bytes per FFT slot and subband: plain f32x2 [sb][sig][T][chan]; TC f16 [sb][chan][rows][T]
+    // (the FP8 form adds an e4m3 copy of half that size; its chunk is a multiple of 128 FFTs).
     const bool tc = c.xmode != FXC_X_PLAIN_FP32;
     const bool fp8 = c.xmode == FXC_X_TC_FP8;
     const size_t tq = fp8 ? 128 : 64;
-    const size_t per_slot = tc ? (size_t)c.nsubband * c.nchan * x->rows * sizeof(uint16_t)
-                               : (size_t)c.nsubband * x->nsig * c.nchan * sizeof(float2);
-    size_t T = c.chunk_ffts;
-    if (T == 0) {
-        T = ((size_t)(tc ? 6 : 1) << 30) / per_slot;
-        T = T / tq * tq;
-        if (T < tq) T = tq;
-        if (T > 4096) T = 4096;
+    const size_t per_sb = tc ? (size_t)c.nchan * x->rows * sizeof(uint16_t) : (size_t)x->nsig * c.nchan * sizeof(float2);
+    size_t budget = (size_t)(tc ? 16 : 2) << 30;
+    if (const char* mb = std::getenv("FXC_SPECTRA_BUDGET_MB")) {   // operator override of the budget
+        const long long v = std::atoll(mb);
+        if (v > 0) budget = (size_t)v << 20;
     }
-    T = std::min(T, round_up((size_t)c.numffts, tq));
+    const size_t tmax = round_up((size_t)c.numffts, tq);
+    const size_t nsb = (size_t)c.nsubband;
+    auto fit = [&](size_t bytes_per_slot) { return budget / bytes_per_slot / tq * tq; };
+    size_t T, G = nsb;
+    if (c.chunk_ffts) {
+        T = std::min((size_t)c.chunk_ffts, tmax);
+        if (group_subbands) G = std::max<size_t>(1, std::min(nsb, budget / (per_sb * T)));
+    } else {
+        T = std::min({fit(per_sb * nsb), (size_t)4096, tmax});
+        if (group_subbands && T < std::min((size_t)512, tmax)) {
+            T = std::min((size_t)2048, tmax);
+            G = std::min(nsb, budget / (per_sb * T));
+            if (G == 0) {
+                G = 1;
+                T = std::min(tmax, fit(per_sb));
+            }
+        }
+        if (T < tq) T = tq;
+    }
     x->T = (int)T;
-    x->spec_bytes = per_slot * T;
+    x->nsb_g = (int)G;
+    x->spec_bytes = per_sb * G * T;
 
     auto fail = [&](cudaError_t e) {
         g_last_cuda = (int)e;
@@ -268,7 +290,7 @@ int fxc_create(const fxc_config* cfg, fxc_ctx** out)
     x->stream = x->own_stream;
     const size_t in_bytes = (size_t)c.nsubband * c.nant * x->pitch;
     x->acc_bytes = (size_t)c.nsubband * x->npair * c.nchan * sizeof(float2);
-    x->vis_bytes = fxc_vis_count(cfg) * sizeof(float2);
+    x->vis_bytes = fxc_vis_count(cfg) * sizeof(float2) / c.nsubband;   // one subband (finalised in turn)
     const int stride = 1 << ((int)std::log2((double)c.nchan) / 2);
     if (c.window_ffts == 0) {   // whole-subintegration device input (fxc_upload_input / fxc_device_input)
         if ((e = cudaMalloc(&x->d_in, in_bytes)) != cudaSuccess) return fail(e);
@@ -292,7 +314,7 @@ int fxc_create(const fxc_config* cfg, fxc_ctx** out)
     if ((e = cudaMalloc(&x->d_spec, x->spec_bytes)) != cudaSuccess) return fail(e);
     if ((e = cudaMemset(x->d_spec, 0, x->spec_bytes)) != cudaSuccess) return fail(e);
     if (fp8) {
-        const size_t n8 = x->spec_bytes / 2, nsc = (size_t)c.nsubband * c.nchan * x->nsig;
+        const size_t n8 = x->spec_bytes / 2, nsc = (size_t)x->nsb_g * c.nchan * x->nsig;
         if ((e = cudaMalloc(&x->d_spec8, n8)) != cudaSuccess) return fail(e);
         if ((e = cudaMemset(x->d_spec8, 0, n8)) != cudaSuccess) return fail(e);   // padding rows stay zero
         if ((e = cudaMalloc(&x->d_amax, nsc * sizeof(unsigned))) != cudaSuccess) return fail(e);
@@ -331,6 +353,10 @@ int fxc_create(const fxc_config* cfg, fxc_ctx** out)
     *out = x;
     return FXC_OK;
 }
+
+extern "C" {
+
+int fxc_create(const fxc_config* cfg, fxc_ctx** out) { return ctx_create(cfg, out, true); }
 
 void fxc_destroy(fxc_ctx* x)
 {
@@ -503,7 +529,18 @@ static int ctx_correlate(fxc_ctx* x, const uint8_t* d_data, size_t pitch, const 
     xa.nsb = x->cfg.nsubband;
     xa.rows = x->rows;
     xa.alt = x->plan_alt;
+    const int nsb = x->cfg.nsubband, G = x->nsb_g;
+    const FArgs fall = fa;
+    const XArgs xall = xa;
+    for (int g0 = 0; g0 < nsb; g0 += G)   // subband groups (one group unless the problem is large)
     for (int c0 = 0; c0 < nfft; c0 += x->T) {
+        fa = fall;
+        xa = xall;
+        fa.data = d_data + (size_t)g0 * x->cfg.nant * pitch;
+        fa.sb_lo = x->d_sblo + g0;
+        fa.nsb = std::min(G, nsb - g0);
+        xa.acc = reinterpret_cast<float2*>(x->d_acc) + (size_t)g0 * x->npair * x->cfg.nchan;
+        xa.nsb = fa.nsb;
         fa.t_base = c0;
         fa.nfft = std::min(x->T, nfft - c0);
         {
@@ -648,19 +685,27 @@ int fxc_process_host_window(fxc_ctx* x, const uint8_t* const* data, const double
             piece = std::max(1, n / 2);
             continue;
         }
-        const bool one_copy = uniform && uhi - ulo <= x->win_cap;
-        if (one_copy)
-            for (int a = 0; a < c.nant; a++) {
-                base[a] = ulo;
-                len[a] = uhi - ulo;
-            }
         const int s = x->win_next;
         x->win_next ^= 1;
         // copy stream: wait until the previous user of this window is done, then fill it
         FXC_CK(cudaStreamWaitEvent(x->copy_stream, x->win_free[s], 0));
+        bool one_copy = false;
+        if (uniform && uhi - ulo <= x->win_cap) {
+            // rows that are equally spaced but separately allocated are refused by the strided
+            // copy (its source range spans the allocations): per-row copies from then on
+            one_copy = cudaMemcpy2DAsync(x->d_win[s], x->win_pitch, data[0] + ulo / spb, (size_t)rstride,
+                                         (size_t)((uhi - ulo) / spb), nrow, cudaMemcpyHostToDevice,
+                                         x->copy_stream) == cudaSuccess;
+            if (!one_copy) {
+                (void)cudaGetLastError();
+                uniform = false;
+            }
+        }
         if (one_copy) {
-            FXC_CK(cudaMemcpy2DAsync(x->d_win[s], x->win_pitch, data[0] + ulo / spb, (size_t)rstride,
-                                     (size_t)((uhi - ulo) / spb), nrow, cudaMemcpyHostToDevice, x->copy_stream));
+            for (int a = 0; a < c.nant; a++) {
+                base[a] = ulo;
+                len[a] = uhi - ulo;
+            }
         } else {
             for (int sb = 0; sb < c.nsubband; sb++)
                 for (int a = 0; a < c.nant; a++) {
@@ -709,23 +754,39 @@ static void counts_out(fxc_ctx* x, const std::vector<int>& pc, int* counts)
     for (int a = 0; a < A; a++) counts[b++] = pc[pidx(a, a)];
 }
 
+}  // extern "C"
+
+// Output of subbands [sb0, sb0 + nsb) into d_vis (layout of fxc_get_visibilities).
+static int finalize_subbands(fxc_ctx* x, int sb0, int nsb, float* d_vis, int normalize)
+{
+    const fxc_config& c = x->cfg;
+    StageScope sc(x, 3, 1);
+    FXC_CK(launch_finalize(x->d_acc + (size_t)sb0 * x->npair * c.nchan, c.xmode != FXC_X_PLAIN_FP32 ? 1 : 0, x->nsig,
+                           c.npol, c.nant, c.nchan, nsb, x->d_counts, normalize, reinterpret_cast<float2*>(d_vis),
+                           x->stream));
+    return FXC_OK;
+}
+
+extern "C" {
+
 int fxc_get_visibilities_device(fxc_ctx* x, float* d_vis, int normalize)
 {
     if (!x || !d_vis) return FXC_ERR_INVALID;
     FXC_CK(cudaSetDevice(x->device));
-    const fxc_config& c = x->cfg;
-    StageScope sc(x, 3, 1);
-    FXC_CK(launch_finalize(x->d_acc, c.xmode != FXC_X_PLAIN_FP32 ? 1 : 0, x->nsig, c.npol, c.nant, c.nchan, c.nsubband, x->d_counts, normalize,
-                           reinterpret_cast<float2*>(d_vis), x->stream));
-    return FXC_OK;
+    return finalize_subbands(x, 0, x->cfg.nsubband, d_vis, normalize);
 }
 
 int fxc_get_visibilities(fxc_ctx* x, float* vis, int* counts, int normalize)
 {
     if (!x || !vis) return FXC_ERR_INVALID;
-    int st = fxc_get_visibilities_device(x, reinterpret_cast<float*>(x->d_vis), normalize);
-    if (st != FXC_OK) return st;
-    FXC_CK(cudaMemcpyAsync(vis, x->d_vis, x->vis_bytes, cudaMemcpyDeviceToHost, x->stream));
+    FXC_CK(cudaSetDevice(x->device));
+    // one subband at a time through a one-subband device buffer
+    for (int sb = 0; sb < x->cfg.nsubband; sb++) {
+        const int st = finalize_subbands(x, sb, 1, reinterpret_cast<float*>(x->d_vis), normalize);
+        if (st != FXC_OK) return st;
+        FXC_CK(cudaMemcpyAsync(reinterpret_cast<char*>(vis) + (size_t)sb * x->vis_bytes, x->d_vis, x->vis_bytes,
+                               cudaMemcpyDeviceToHost, x->stream));
+    }
     std::vector<int> pc(x->npair_ant);
     FXC_CK(cudaMemcpyAsync(pc.data(), x->d_counts, sizeof(int) * x->npair_ant, cudaMemcpyDeviceToHost, x->stream));
     FXC_CK(cudaStreamSynchronize(x->stream));
@@ -767,6 +828,7 @@ int fxc_autotune(fxc_ctx* x, int reps)
     fa.t_base = 0;
     fa.nfft = nfft;
     fa.amax = x->d_amax;
+    fa.nsb = x->nsb_g;   // the first subband group: what one chunk's spectra buffer holds
     cudaEvent_t e0, e1;
     FXC_CK(cudaEventCreate(&e0));
     FXC_CK(cudaEventCreate(&e1));
@@ -801,7 +863,7 @@ int fxc_autotune(fxc_ctx* x, int reps)
         xa.nsig = x->nsig;
         xa.T = x->T;
         xa.nchan = c.nchan;
-        xa.nsb = c.nsubband;
+        xa.nsb = x->nsb_g;
         xa.rows = x->rows;
         best = 1e30f;
         for (int alt : {0, 1}) {

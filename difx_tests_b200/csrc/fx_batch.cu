@@ -207,7 +207,7 @@ int fxc_batch_create(const fxc_config* cfgs, int njobs, fxc_batch** out)
     int st = FXC_OK;
     for (int j = 0; j < njobs && st == FXC_OK; j++) {
         fxc_ctx* c = nullptr;
-        st = fxc_create(&cfgs[j], &c);
+        st = ctx_create(&cfgs[j], &c, false);
         if (st == FXC_OK) b->ctx.push_back(c);
     }
     if (st == FXC_OK) {

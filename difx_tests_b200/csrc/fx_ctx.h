@@ -17,6 +17,7 @@ struct fxc_ctx {
     int F = 0, nsig = 0, npair = 0, npair_ant = 0, nbl = 0, nout = 0;
     int ld = 0;            // delay-table leading dimension (FFTs, multiple of 128)
     int T = 0;             // FFT slots per chunk (multiple of 64)
+    int nsb_g = 1;         // subbands per chunk (all of them unless the problem is large)
     int rows = 0;          // F16 spectra rows per channel
     size_t pitch = 0;      // input row pitch
     size_t subint = 0;
@@ -81,6 +82,10 @@ struct fxc_ctx {
 // F16-output F stage, "X <signal blocks of 8>" plain X tile variant.
 std::map<std::string, int> plan_cache_load();
 void plan_cache_append(const std::vector<std::string>& lines);
+
+// fxc_create with control over subband grouping (false: every subband in each chunk, as the
+// multi-job batch's task tables assume)
+int ctx_create(const fxc_config* cfg, fxc_ctx** out, bool group_subbands);
 
 // delay model to the device (only when it changed) + K0 over FFTs first..first+nfft-1; with
 // win_base/win_len (host, per antenna, samples) the input rows are windows (see k_delay_table)

@@ -121,13 +121,13 @@ __global__ void k_finalize(const float2* __restrict__ acc, int acc_layout, int n
         const int sb = (int)(r / nout);
         int a1, a2;
         if (bl < nbl) {
-            int rem = bl;
-            a1 = 0;
-            while (rem >= nant - 1 - a1) {
-                rem -= nant - 1 - a1;
-                a1++;
-            }
-            a2 = a1 + 1 + rem;
+            // row a1 of the strict upper triangle starts at S(a1) = a1 (2 nant - a1 - 1) / 2
+            const double m = 2.0 * nant - 1.0;
+            a1 = (int)((m - sqrt(m * m - 8.0 * bl)) * 0.5);
+            if (a1 < 0) a1 = 0;
+            while (a1 > 0 && a1 * (2 * nant - a1 - 1) / 2 > bl) a1--;
+            while ((a1 + 1) * (2 * nant - a1 - 2) / 2 <= bl) a1++;
+            a2 = a1 + 1 + (bl - a1 * (2 * nant - a1 - 1) / 2);
         } else {
             a1 = a2 = bl - nbl;
         }

@@ -60,7 +60,10 @@ typedef struct fxc_config {
     double lo;         /* LO (sky) frequency of subband 0, Hz; |lo| < 2^31 for reference-identical phases */
     double bw;         /* bandwidth per subband, Hz; sampling interval 1/(2 bw) (kernel.c:14) */
     double sb_spacing; /* LO step between consecutive subbands, Hz */
-    int chunk_ffts;    /* FFTs per F->X chunk (multiple of 64), 0 = chosen by the library */
+    int chunk_ffts;    /* FFTs per F->X chunk (multiple of 64), 0 = chosen by the library: the
+                          spectra of a chunk stay within 2 GiB (plain) / 16 GiB (tensor cores), or
+                          the environment variable FXC_SPECTRA_BUDGET_MB; problems too large for
+                          long chunks of every subband are chunked over groups of subbands */
     int window_ffts;   /* FFTs per streamed input window (fxc_process_host*); 0 = the chunk length.
                           > 0 also drops the whole-subintegration device input buffer, so the
                           subintegration never has to fit in device memory (fxc_upload_input and

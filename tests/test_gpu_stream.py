@@ -98,3 +98,23 @@ def test_device_windows_and_miss_detection():
             c.synchronize()
         assert e.value.status == fx.FXC_ERR_INVALID
         c.synchronize()      # the error is reported once; the context stays usable
+
+
+@pytest.mark.parametrize("xmode", [fx.FXC_X_PLAIN_FP32, fx.FXC_X_TC_FP16, fx.FXC_X_TC_FP8])
+def test_subband_groups(xmode, monkeypatch):
+    """A spectra budget too small for every subband: chunks over groups of subbands."""
+    monkeypatch.setenv("FXC_SPECTRA_BUDGET_MB", "1")
+    job = synth.make_job(nant=8, npol=1, nchan=512, numffts=600, bw=64e6, lo=1.4e9, rho=0.1, seed=21, nsubband=3)
+    with fx.Correlator(cfg_for(job, xmode=xmode)) as c:
+        c.process(job.data, job.delays, job.fileoffsets)
+        vis, counts = c.visibilities()
+    for sb in range(job.nsubband):
+        ref, rc = oracle(job, sb)
+        np.testing.assert_array_equal(counts, rc)
+        mx, rms = fo.vis_error(vis[sb], ref)
+        if xmode == fx.FXC_X_PLAIN_FP32:
+            assert mx.max() < VIS_TOL
+        elif xmode == fx.FXC_X_TC_FP16:
+            assert rms.max() < 1e-3 and mx.max() < 1e-2
+        else:
+            assert rms.max() < 0.05
