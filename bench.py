@@ -595,14 +595,147 @@ def run_batch_arm(args):
     return 0
 
 
+# Large array: 256 antennas x 2 polarisations (512 signals) x 16 subbands x 4096 channels,
+# 1 s at 128 MS/s (15625 FFTs of 8192 per subband), 1.05e12 input samples = 262 GB packed per
+# subintegration: more than HBM holds, so the input streams through device windows
+# (window_ffts FFTs of every row) while the accumulators (69 GB) stay on the device.
+LARGE = dict(nant=256, npol=2, nchan=4096, nsb=16, numffts=15625, bw=64e6, lo=1.4e9, rho=0.02, window_ffts=1024)
+
+
+def large_subset_accuracy(xmode, nsub=16, nf=64):
+    """Error of the 256-antenna correlation against the FP64 oracle on a 16-antenna subset
+    (1 subband, nf FFTs): the subset's baselines are cut out of the full-array output."""
+    import difx_tests_b200 as fx
+    from difx_tests_b200 import synth
+    from oracle import fxoracle as fo
+    L = LARGE
+    job = synth.make_job(nant=L["nant"], npol=L["npol"], nchan=L["nchan"], numffts=nf, bw=L["bw"], lo=L["lo"],
+                         rho=L["rho"], seed=4444)
+    cfg = fx.make_config(job.nant, job.nchan, nf, job.bw, job.lo, npol=job.npol, xmode=xmode)
+    with fx.Correlator(cfg) as c:
+        c.process(job.data, job.delays, job.fileoffsets)
+        vis, counts = c.visibilities()
+    sub = np.arange(nsub) * (L["nant"] // nsub)          # every 16th antenna
+    bl_all = {p: i for i, p in enumerate(fo.baseline_order(L["nant"]))}
+    nbl = len(bl_all)
+    rows = [bl_all[(int(sub[i]), int(sub[j]))] for i in range(nsub - 1) for j in range(i + 1, nsub)]
+    rows += [nbl + int(a) for a in sub]
+    got = vis[0][rows]
+    ref, rc = fo.correlate(job.data[0][sub], job.delays[sub], job.fileoffsets[sub], job.bw, job.lo, job.nchan,
+                           job.npol, numffts=nf)
+    mx, rms = fo.vis_error(got, ref)
+    return {"max_rel": float(mx.max()), "rms_rel": float(rms.max()), "vs": "FP64 oracle",
+            "sample": f"{nsub}-antenna subset of the 256 x 2 pol x 4096 ch correlation, 1 subband x {nf} FFTs",
+            "counts_match": bool(np.array_equal(counts[rows], rc))}
+
+
+def run_large_arm(args):
+    import torch
+
+    import difx_tests_b200 as fx
+
+    L = LARGE
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+    F = 2 * L["nchan"]
+    spb = 4 // L["npol"]
+    W = L["window_ffts"]
+    row_bytes = (W + 4) * F // spb
+    pitch = (row_bytes + 32 + 255) // 256 * 256
+    nsig = L["nant"] * L["npol"]
+    delays, offs = delay_model(L["nant"], L["nchan"], L["bw"], seed=42)
+    # one window of seeded data per row, generated on the device and reused by every window of
+    # the subintegration (throughput does not depend on the sample values)
+    t0 = time.perf_counter()
+    data = gen_device_data(torch, L["nsb"], L["nant"], L["npol"], row_bytes, pitch, L["rho"], seed=7, device=dev)
+    torch.cuda.synchronize()
+    gen_s = time.perf_counter() - t0
+    windows = [(w0, min(W, L["numffts"] - w0)) for w0 in range(0, L["numffts"], W)]
+
+    def run(corr, wins):
+        corr.reset()
+        for w0, n in wins:
+            base = np.full(L["nant"], max(0, (w0 - 2) * F), np.int64)
+            corr.process_device_window(data.data_ptr(), pitch, base, row_bytes, delays, offs, w0, n)
+
+    def timed(xmode, wins, steps, warmup):
+        cfg = fx.make_config(L["nant"], L["nchan"], L["numffts"], L["bw"], L["lo"], npol=L["npol"], nsubband=L["nsb"],
+                             xmode=xmode, window_ffts=W)
+        corr = fx.Correlator(cfg)
+        corr.set_stream(stream.cuda_stream)
+        for _ in range(warmup):
+            run(corr, wins)
+        corr.synchronize()
+        corr.enable_stage_timing(True)
+        corr.stage_times(reset=True)
+        clocks = ClockSampler(0)
+        clocks.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(steps):
+            run(corr, wins)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clk = clocks.stop()
+        corr.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        stage_ms, launches = corr.stage_times(reset=True)
+        corr.close()
+        nfft = sum(n for _, n in wins)
+        samples = L["nant"] * L["npol"] * L["nsb"] * nfft * F
+        xflop = 8.0 * L["nchan"] * nfft * L["nsb"] * nsig * (nsig + 1) / 2
+        return dict(ms=ms, value=samples / (ms / 1e3) / 1e9, samples=samples, stage_ms=stage_ms / steps,
+                    launches=launches, clocks=clk, x_tflops=xflop * steps / (stage_ms[2] / 1e3) / 1e12,
+                    nfft=nfft, xflop=xflop)
+
+    tc = timed(fx.FXC_X_TC_FP16, windows, args.steps, args.warmup)
+    plain = timed(fx.FXC_X_PLAIN_FP32, windows[:1], 1, 1)   # bounded sample: the first window
+    hbm, tc_peak, peak_kind = peaks()
+    f_bytes = tc["samples"] * (0.25 + 2.0)
+    f_gbs = f_bytes / (tc["stage_ms"][1] / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": tc["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": tc["ms"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": DTYPES["tc"], "data": "synthetic (seeded, generated on device; one window reused for every window)",
+        "config": {"workload": "256 ant x 2 pol x 16 subbands x 4096 ch, 1 s @ 128 MS/s (15625 FFTs/subband), "
+                               f"streamed in windows of {W} FFTs", "form": "tc",
+                   "l2": "262 GB of input per step, far above L2; no flush"},
+        "stages_ms_per_step": {"delay+counts": tc["stage_ms"][0], "F": tc["stage_ms"][1], "X": tc["stage_ms"][2]},
+        "x_stage": {"tflops": tc["x_tflops"], "flop_per_step": tc["xflop"], "peak_tflops": tc_peak,
+                    "frac": tc["x_tflops"] / tc_peak,
+                    "note": "algorithmic Hermitian flops; 128x128 block pairs compute 12% more"},
+        "roofline": {"kernel": "k_fstage", "bound": "hbm", "achieved": f_gbs, "peak": hbm, "unit": "GB/s",
+                     "frac": f_gbs / hbm, "traffic": None, "peak_source": peak_kind + " (MEASURED_PEAKS.json)",
+                     "note": "F stage is FP32-issue-bound"},
+        "clocks": tc["clocks"],
+        "gpu_launches": int(tc["launches"].sum()),
+        "plain": {"value": plain["value"], "unit": UNIT, "ms": plain["ms"],
+                  "sample": f"first window: {plain['nfft']} FFTs x 16 subbands",
+                  "stages_ms": {"F": plain["stage_ms"][1], "X": plain["stage_ms"][2]},
+                  "x_tflops": plain["x_tflops"], "clocks": plain["clocks"]},
+        "tc_vs_plain": {"gsamps": tc["value"] / plain["value"]},
+        "data_gen_s": gen_s,
+    }
+    del data
+    torch.cuda.empty_cache()
+    if not args.no_accuracy:
+        line["accuracy"] = {"tc": large_subset_accuracy(fx.FXC_X_TC_FP16)}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS) + ["cfg3"],
-                    help="cfg3: the batched uneven workload (12 jobs through fxc_batch_*)")
+    ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS) + ["cfg3", "cfg4"],
+                    help="cfg3: the batched uneven workload (12 jobs through fxc_batch_*); cfg4: the large "
+                         "array (512 signals x 4096 channels x 16 subbands) streamed through device windows")
     ap.add_argument("--xmode", default="all", choices=["all", "both", "tc", "fp8", "plain"],
                     help="all: the FP16 tensor-core form is the headline value, the FP8 tensor-core and FP32 "
                          "plain forms are timed beside it; both: FP16 tensor-core and plain")
@@ -616,6 +749,8 @@ def main():
         return run_reference_arm(args)
     if args.workload == "cfg3":
         return run_batch_arm(args)
+    if args.workload == "cfg4":
+        return run_large_arm(args)
     return run_gpu_arm(args)
 
 

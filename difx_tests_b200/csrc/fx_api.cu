@@ -543,6 +543,11 @@ static int ctx_correlate(fxc_ctx* x, const uint8_t* d_data, size_t pitch, const 
         xa.nsb = fa.nsb;
         fa.t_base = c0;
         fa.nfft = std::min(x->T, nfft - c0);
+        // slots the chunk uses: the FFTs rounded up to the X stage's stage depth (the F stage
+        // writes zeros after the last FFT; later slots keep an earlier chunk's data, unread)
+        const int q = fp8 ? 128 : 64;
+        fa.tspan = std::min(x->T, (fa.nfft + q - 1) / q * q);
+        xa.ntk = fa.tspan;
         {
             StageScope sc(x, 1, 1);
             if (fp8) FXC_CK(cudaMemsetAsync(x->d_amax, 0, sizeof(unsigned) * xa.nsb * xa.nchan * xa.nsig, x->stream));
@@ -552,8 +557,8 @@ static int ctx_correlate(fxc_ctx* x, const uint8_t* d_data, size_t pitch, const 
             StageScope sc(x, 2, fp8 ? 2 : 1);
             if (fp8) {
                 // the e4m3 cast of the chunk belongs to the X operand: counted with the X stage
-                FXC_CK(launch_cast_fp8(x->d_spec, x->d_amax, x->rows, x->nsig, x->T, xa.nsb * xa.nchan, x->d_spec8,
-                                       x->d_inv, x->stream));
+                FXC_CK(launch_cast_fp8(x->d_spec, x->d_amax, x->rows, x->nsig, x->T, xa.ntk, xa.nsb * xa.nchan,
+                                       x->d_spec8, x->d_inv, x->stream));
                 XArgs x8 = xa;
                 x8.spec = x->d_spec8;
                 x8.inv_scale = x->d_inv;

@@ -562,7 +562,7 @@ cudaError_t launch_f(const FArgs& a, cudaStream_t st)
     static unsigned configured = 0;  // per instantiation and device
     cudaError_t e = set_smem_once(kern, sm, &configured);
     if (e != cudaSuccess) return e;
-    dim3 grid((a.T + TB - 1) / TB, a.nant, a.nsb);
+    dim3 grid(((a.tspan ? a.tspan : a.T) + TB - 1) / TB, a.nant, a.nsb);
     kern<<<grid, P::NTHREADS, sm, st>>>(a);
     return cudaGetLastError();
 }

@@ -56,6 +56,7 @@ struct FArgs {
     int rows;                   // F16 layout: rows per channel (>= 2*nsig)
     int tb;                     // FFTs per CTA (8, 16 or 32; 0 = 16), chosen by the plan / autotuner
     unsigned* amax;             // F16 layout, FP8 form: running absmax per (sb*nchan + chan, sig), or null
+    int tspan;                  // slots [0, tspan) written (>= nfft, multiple of 64; 0 = T)
 };
 
 
@@ -66,6 +67,7 @@ struct XArgs {
     int rows;
     int alt;     // plain-form tile variant: 0 = default, 1 = alternative (chosen by the plan / autotuner)
     const float* inv_scale;   // FP8 form: [nsb*nchan][nsig] factors applied to each Gram product
+    int ntk;                  // slots [0, ntk) of each spectra row consumed (0 = T; multiple of 64 / 128 for FP8)
 };
 
 }  // namespace fx

@@ -31,7 +31,7 @@ int xplain_channel_group(int nsig, int alt);
 cudaError_t launch_xtc(const XArgs& a, int* d_err, int nsm, cudaStream_t st);
 // FP8 form: e4m3 copy of the F16 spectra scaled by 448/absmax per (item = sb*nchan + chan, signal),
 // then the e4m3 Gram with the inverse scales applied per product
-cudaError_t launch_cast_fp8(const void* spec16, const unsigned* amax, int rows, int nsig, int T, int nitems,
+cudaError_t launch_cast_fp8(const void* spec16, const unsigned* amax, int rows, int nsig, int T, int ts, int nitems,
                             uint8_t* spec8, float* inv_scale, cudaStream_t st);
 cudaError_t launch_xtc8(const XArgs& a, int* d_err, int nsm, cudaStream_t st);
 size_t xtc_smem_bytes();

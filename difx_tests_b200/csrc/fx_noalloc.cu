@@ -174,7 +174,7 @@ extern "C" int fxc_correlate_noalloc(const fxc_config* cfg, const uint8_t* d_dat
     fa.chan_step = reinterpret_cast<const float*>(scratch + o_cstep);
     fa.spec = scratch + o_spec;
     fa.T = (int)T;
-    XArgs xa;
+    XArgs xa{};
     xa.spec = scratch + o_spec;
     xa.acc = d_acc;
     xa.nsig = nsig;

@@ -87,7 +87,7 @@ __device__ __forceinline__ void xplain_block(const XArgs& a, int sb, int c0, uns
 #pragma unroll
         for (int j = 0; j < 8; j++) acc[i][j] = make_float2(0.f, 0.f);
 
-    const int nblk = a.T / TK;
+    const int nblk = (a.ntk ? a.ntk : a.T) / TK;
     issue(0, 0);
     for (int blk = 0; blk < nblk; blk++) {
         if (blk + 1 < nblk) {
@@ -267,7 +267,7 @@ k_xplain_big(XArgs a)
 #pragma unroll
         for (int j = 0; j < 8; j++) acc[i][j] = make_float2(0.f, 0.f);
 
-    const int nblk = a.T / TK;
+    const int nblk = (a.ntk ? a.ntk : a.T) / TK;
     issue(0, 0);
     for (int blk = 0; blk < nblk; blk++) {
         if (blk + 1 < nblk) {
@@ -319,7 +319,8 @@ k_xplain_big(XArgs a)
 
 static cudaError_t launch_xbig(const XArgs& a, cudaStream_t st)
 {
-    if (a.nchan % big::CG || a.T % big::TK || a.nsig > 512) return cudaErrorInvalidValue;
+    if (a.nchan % big::CG || a.T % big::TK || a.ntk % big::TK || a.ntk > a.T || a.nsig > 512)
+        return cudaErrorInvalidValue;
     const size_t sm = 2 * (size_t)big::STAGE * sizeof(float2);
     static unsigned configured = 0;
     cudaError_t e = set_smem_once(k_xplain_big, sm, &configured);
@@ -363,7 +364,7 @@ cudaError_t launch_xplain(const XArgs& a, cudaStream_t st)
     if (a.nsig > 64) return launch_xbig(a, st);
     const int nb = (a.nsig + 7) / 8;
     const int alt = a.alt;
-    if (a.T % 16 != 0) return cudaErrorInvalidValue;  // T is a multiple of every TK
+    if (a.T % 16 != 0 || a.ntk % 16 != 0 || a.ntk > a.T) return cudaErrorInvalidValue;  // multiples of every TK
 #define FX_OP(NB_, CG_, TK_) return launch_x<NB_, CG_, TK_>(a, st)
     FX_XPLANS(FX_OP)
 #undef FX_OP

@@ -215,7 +215,7 @@ k_xtc(const __grid_constant__ CUtensorMap tmap, XArgs a, int* err)
     const int nb = MB ? a.rows / BM : 1;
     const int nbp = nb * (nb + 1) / 2;
     const int nitems = a.nsb * a.nchan * nbp;
-    const int nk = a.T / BK;
+    const int nk = (a.ntk ? a.ntk : a.T) / BK;
     const int nsig = a.nsig;
     const int npair = nsig * (nsig + 1) / 2;
 
@@ -447,7 +447,9 @@ template <bool F8>
 static cudaError_t launch_xtc_f(const XArgs& a, int* d_err, int nsm, cudaStream_t st)
 {
     constexpr int BK = F8 ? tc::ROWB : tc::ROWB / 2;
-    if (a.rows % tc::BM != 0 || a.rows < 2 * a.nsig || a.T % BK != 0 || a.nsig > 512) return cudaErrorInvalidValue;
+    if (a.rows % tc::BM != 0 || a.rows < 2 * a.nsig || a.T % BK != 0 || a.ntk % BK != 0 || a.ntk > a.T ||
+        a.nsig > 512)
+        return cudaErrorInvalidValue;
     if ((long long)a.nsb * a.nchan * a.rows > 0x7fffffffLL) return cudaErrorInvalidValue;   // int TMA row coordinate
     if (F8 && !a.inv_scale) return cudaErrorInvalidValue;
     auto enc = get_encode();
@@ -479,9 +481,9 @@ cudaError_t launch_xtc8(const XArgs& a, int* d_err, int nsm, cudaStream_t st)
 // The scale of signal s in item it is k = 448/absmax (1 when the rows are all zero);
 // inv_scale receives 1/k.
 __global__ void k_cast_fp8(const __half* __restrict__ spec16, const unsigned* __restrict__ amax, int rows, int nsig,
-                           int T, long long nvec, uint8_t* __restrict__ spec8, float* __restrict__ inv_scale)
+                           int T, int ts, long long nvec, uint8_t* __restrict__ spec8, float* __restrict__ inv_scale)
 {
-    const int vpr = T / 8;                      // 8-FFT vectors per row
+    const int vpr = ts / 8;                     // 8-FFT vectors per row (slots [0, ts) of T)
     const long long per_item = (long long)2 * nsig * vpr;
     for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nvec;
          v += (long long)gridDim.x * blockDim.x) {
@@ -510,11 +512,11 @@ __global__ void k_cast_fp8(const __half* __restrict__ spec16, const unsigned* __
     }
 }
 
-cudaError_t launch_cast_fp8(const void* spec16, const unsigned* amax, int rows, int nsig, int T, int nitems,
+cudaError_t launch_cast_fp8(const void* spec16, const unsigned* amax, int rows, int nsig, int T, int ts, int nitems,
                             uint8_t* spec8, float* inv_scale, cudaStream_t st)
 {
-    if (T % 8 != 0 || 2 * nsig > rows) return cudaErrorInvalidValue;
-    const long long nvec = (long long)nitems * 2 * nsig * (T / 8);
+    if (T % 8 != 0 || ts % 8 != 0 || ts < 8 || ts > T || 2 * nsig > rows) return cudaErrorInvalidValue;
+    const long long nvec = (long long)nitems * 2 * nsig * (ts / 8);
     int dev = 0, nsm = 0;
     cudaError_t e;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
@@ -522,7 +524,7 @@ cudaError_t launch_cast_fp8(const void* spec16, const unsigned* amax, int rows, 
     const long long want = (nvec + 255) / 256;
     const int grid = (int)(want < (long long)nsm * 8 ? want : (long long)nsm * 8);
     k_cast_fp8<<<grid > 0 ? grid : 1, 256, 0, st>>>(reinterpret_cast<const __half*>(spec16), amax, rows, nsig, T,
-                                                    nvec, spec8, inv_scale);
+                                                    ts, nvec, spec8, inv_scale);
     return cudaGetLastError();
 }
 
