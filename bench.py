@@ -351,10 +351,8 @@ def time_form(torch, dist, fx, w, xmode, data, pitch, delays, offs, steps, warmu
     ms = e0.elapsed_time(e1)
     stage_ms, launches = corr.stage_times(reset=True)
     corr.enable_stage_timing(False)
-    ms_t = torch.tensor([ms], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
+    from difx_tests_b200 import sharding
+    ms_max = sharding.max_over_ranks(ms, device=dev)   # device time: max over ranks
     f_launches = max(1, int(launches[1]))
     x_launches = max(1, int(launches[2]))
     ffts_per_launch = w["numffts"] * steps / f_launches
@@ -464,19 +462,23 @@ def run_gpu_arm(args):
         corr.process(rows, delays, offs)   # warm
         corr.visibilities()
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
+        # CUDA events on the correlator's stream around host-buffer calls: copies (on the library's
+        # copy stream, ordered by events), compute and the read-back all fall inside
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
         for _ in range(e2e_steps):
             corr.reset()
             corr.process(rows, delays, offs)
             corr.visibilities()
-        t = (time.perf_counter() - t0) / e2e_steps
-        t_t = torch.tensor([t], device=dev, dtype=torch.float64)
-        if world > 1:
-            dist.all_reduce(t_t, op=dist.ReduceOp.MAX)
-        line["e2e"] = {"value": world * head["samples"] / float(t_t.item()) / 1e9, "unit": UNIT,
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        t = ev0.elapsed_time(ev1) / 1e3 / e2e_steps
+        from difx_tests_b200 import sharding
+        t_max = sharding.max_over_ranks(t, device=dev)
+        line["e2e"] = {"value": world * head["samples"] / t_max / 1e9, "unit": UNIT,
                        "h2d_bytes_per_step": int(w["nsb"] * w["nant"] * subint),
                        "d2h_bytes_per_step": int(vis_n * 8 + 4 * (w["nant"] * (w["nant"] - 1) // 2 + w["nant"])),
-                       "steps": e2e_steps, "ms_per_step": 1e3 * float(t_t.item()),
+                       "steps": e2e_steps, "ms_per_step": 1e3 * t_max,
                        "path": "fxc_process_host + fxc_get_visibilities, pinned host buffers"}
 
     if rank == 0 and not args.no_accuracy:
