@@ -139,7 +139,8 @@ def _dp(a):
 
 
 def make_config(nant, nchan, numffts, bw, lo, npol=2, nsubband=1, sb_spacing=None, xmode=FXC_X_PLAIN_FP32,
-                chunk_ffts=0, window_ffts=0) -> FxcConfig:
+                chunk_ffts=0, window_ffts=0, cpx=False) -> FxcConfig:
+    """cpx: 8-bit complex input (FFT length nchan) instead of the reference's 2-bit real."""
     cfg = FxcConfig()
     _lib().fxc_config_default(C.byref(cfg))
     cfg.nant, cfg.npol, cfg.nchan, cfg.numffts = nant, npol, nchan, numffts
@@ -149,6 +150,8 @@ def make_config(nant, nchan, numffts, bw, lo, npol=2, nsubband=1, sb_spacing=Non
     cfg.xmode = xmode
     cfg.chunk_ffts = chunk_ffts
     cfg.window_ffts = window_ffts
+    if cpx:
+        cfg.nbit, cfg.iscomplex = 8, 1
     return cfg
 
 

@@ -86,6 +86,8 @@ size_t fxc_subint_bytes(const fxc_config* c)
 {
     if (!c) return 0;
     // allocDataHost.c:21 (cfactor = 2 for real data)
+    if (c->iscomplex)   // 8-bit complex: (re, im) bytes per sample and polarisation, nchan samples per FFT
+        return (size_t)c->nchan * (size_t)(c->numffts + 1) * 2 * c->npol;
     return (size_t)c->nchan * 2 * (size_t)(c->numffts + 1) * c->nbit / 8 * c->npol;
 }
 
@@ -119,7 +121,10 @@ static int validate(const fxc_config* c)
     if (!c) return FXC_ERR_INVALID;
     if (c->nant < 2 || c->npol < 1 || c->npol > 2 || c->numffts < 1 || c->nsubband < 1) return FXC_ERR_INVALID;
     if (c->nchan < 128 || c->nchan > 4096 || (c->nchan & (c->nchan - 1))) return FXC_ERR_INVALID;
-    if (c->nbit != 2 || c->iscomplex != 0) return FXC_ERR_UNSUPPORTED;
+    // 2-bit real (the reference's CPU format) or 8-bit complex (its GPU format, gkernel.cu:277-296)
+    if (!((c->nbit == 2 && c->iscomplex == 0) || (c->nbit == 8 && c->iscomplex == 1))) return FXC_ERR_UNSUPPORTED;
+    if (c->iscomplex && c->nchan < 256) return FXC_ERR_UNSUPPORTED;   // complex FFT length nchan >= 256
+    if (c->iscomplex && (long long)(c->numffts + 1) * c->nchan * 2 * c->npol > 0x7fffffffLL) return FXC_ERR_INVALID;
     if (!(c->bw > 0.0) || !std::isfinite(c->lo) || !std::isfinite(c->sb_spacing)) return FXC_ERR_INVALID;
     if (c->xmode != FXC_X_PLAIN_FP32 && c->xmode != FXC_X_TC_FP16 && c->xmode != FXC_X_TC_FP8)
         return FXC_ERR_INVALID;
@@ -167,9 +172,17 @@ void plan_cache_append(const std::vector<std::string>& lines)
 
 static std::string fplan_key(const fxc_config& c)
 {
-    return std::string(c.xmode == FXC_X_PLAIN_FP32 ? "F " : "H ") + std::to_string(2 * c.nchan) + " " +
-           std::to_string(c.npol);
+    return std::string(c.xmode == FXC_X_PLAIN_FP32 ? "F" : "H") + (c.iscomplex ? "C " : " ") +
+           std::to_string(c.iscomplex ? c.nchan : 2 * c.nchan) + " " + std::to_string(c.npol);
 }
+
+// Input sample geometry: bits per time sample of one row (all polarisations), samples per
+// whole byte (window bases are multiples), and the samples of read-ahead past an FFT's last
+// sample (the 2-bit unpacker's extra byte, kernel.c:402-409).
+static int sample_bits(const fxc_config& c) { return c.iscomplex ? 16 * c.npol : 2 * c.npol; }
+static int sample_align(const fxc_config& c) { return std::max(1, 8 / sample_bits(c)); }
+static int tail_samples(const fxc_config& c) { return c.iscomplex ? 0 : 8 / sample_bits(c); }
+static long long samples_to_bytes(const fxc_config& c, long long s) { return s * sample_bits(c) / 8; }
 
 static std::string xplan_key(int nsig) { return "X " + std::to_string((nsig + 7) / 8); }
 
@@ -230,7 +243,7 @@ int ctx_create(const fxc_config* cfg, fxc_ctx** out, bool group_subbands)
     x->device = dev;
     x->nsm = prop.multiProcessorCount;
     const fxc_config& c = x->cfg;
-    x->F = 2 * c.nchan;
+    x->F = c.iscomplex ? c.nchan : 2 * c.nchan;   // complex samples: every FFT bin is a channel
     x->nsig = c.nant * c.npol;
     x->npair = x->nsig * (x->nsig + 1) / 2;
     x->npair_ant = c.nant * (c.nant + 1) / 2;
@@ -472,9 +485,10 @@ int ctx_run_delay_table(fxc_ctx* x, const double* delays, const double* offs, in
     }
     const int ld = (int)round_up((size_t)nfft, 128);
     const int maxoffset = (c.numffts - 1) * x->F;  // kernel.c:730
-    const double sampletime = 1.0 / (2.0 * c.bw);  // kernel.c:14
+    // kernel.c:14 (real sampling); complex sampling at bw (main_gpu.cu:246-247)
+    const double sampletime = c.iscomplex ? 1.0 / c.bw : 1.0 / (2.0 * c.bw);
     FXC_CK(launch_delay_table_window(x->d_delays, x->d_offs, nullptr, first, c.nant, nfft, ld, x->F, maxoffset,
-                                     sampletime, win_base ? x->d_win_meta : nullptr, 4 / c.npol, x->d_err + 1,
+                                     sampletime, win_base ? x->d_win_meta : nullptr, tail_samples(c), x->d_err + 1,
                                      x->d_dtab, x->d_vbits, x->stream));
     *ld_out = ld;
     return FXC_OK;
@@ -498,6 +512,7 @@ FArgs ctx_fargs(fxc_ctx* x, const uint8_t* d_data, size_t pitch, int ld)
     a.rows = x->rows;
     a.T = x->T;
     a.tb = x->plan_tb;
+    a.cpx = x->cfg.iscomplex;
     return a;
 }
 
@@ -588,10 +603,9 @@ int fxc_process_device_window(fxc_ctx* x, const uint8_t* d_data, size_t pitch, c
         ((uintptr_t)d_data & 15))
         return FXC_ERR_INVALID;
     const fxc_config& c = x->cfg;
-    const int spb = 4 / c.npol;
-    std::vector<long long> len(c.nant, (long long)row_bytes * spb);
+    std::vector<long long> len(c.nant, (long long)row_bytes * 8 / sample_bits(c));
     for (int a = 0; a < c.nant; a++)
-        if (base_sample[a] < 0 || base_sample[a] % spb) return FXC_ERR_INVALID;
+        if (base_sample[a] < 0 || base_sample[a] % sample_align(c)) return FXC_ERR_INVALID;
     FXC_CK(cudaSetDevice(x->device));
     return ctx_correlate(x, d_data, pitch, base_sample, len.data(), delays, offs, first, nfft);
 }
@@ -607,7 +621,7 @@ static void window_range(const fxc_config& c, int F, const double* delays, const
                          int k1, long long& lo, long long& hi)
 {
     const double q = delays[3 * a], l = delays[3 * a + 1], cc = delays[3 * a + 2];
-    const double Ts = 1.0 / (2.0 * c.bw);
+    const double Ts = c.iscomplex ? 1.0 / c.bw : 1.0 / (2.0 * c.bw);
     auto offset = [&](double k) {
         const double mean = q * k * k + (q + l) * k + q / 2 + l / 2 + cc - q / 12;   // a/2 + b of kernel.c:383-385
         const double nf = (mean - offs[a]) / Ts;
@@ -622,20 +636,18 @@ static void window_range(const fxc_config& c, int F, const double* delays, const
                 mx = std::max(mx, offset(k));
             }
     }
-    const int spb = 4 / c.npol;   // the unpacker may read one byte past the FFT's last sample (kernel.c:402-409)
     lo = mn - 2;
-    hi = mx + F + 2 + 2 * spb;
+    hi = mx + F + 2 + tail_samples(c) + sample_align(c);
 }
 
 static int ensure_windows(fxc_ctx* x)
 {
     if (x->d_win[0]) return FXC_OK;
     const fxc_config& c = x->cfg;
-    const int spb = 4 / c.npol;
     // a window holds win_ffts FFTs plus the spread of their delays (far below an FFT for
     // sidereal rates) and the nudge margin: (win_ffts + 4) FFT lengths
     x->win_cap = (long long)(x->win_ffts + 4) * x->F;
-    x->win_pitch = round_up((size_t)(x->win_cap / spb) + 32, 256);
+    x->win_pitch = round_up((size_t)samples_to_bytes(c, x->win_cap) + 32, 256);
     const size_t bytes = (size_t)c.nsubband * c.nant * x->win_pitch;
     for (int s = 0; s < 2; s++) {
         FXC_CK(cudaMalloc(&x->d_win[s], bytes));
@@ -659,8 +671,8 @@ int fxc_process_host_window(fxc_ctx* x, const uint8_t* const* data, const double
     FXC_CK(cudaSetDevice(x->device));
     int st = ensure_windows(x);
     if (st != FXC_OK) return st;
-    const int spb = 4 / c.npol;
-    const long long total = (long long)x->subint * spb;   // samples in a host row
+    const int sal = sample_align(c);
+    const long long total = (long long)x->subint * 8 / sample_bits(c);   // samples in a host row
     const int nrow = c.nsubband * c.nant;
     // rows evenly spaced in one host array: one strided copy per window over the union
     // of the antennas' ranges (when it fits), instead of one copy per row
@@ -678,10 +690,10 @@ int fxc_process_host_window(fxc_ctx* x, const uint8_t* const* data, const double
             long long lo, hi;
             window_range(c, x->F, delays, offs, a, k, k + n - 1, lo, hi);
             lo = std::max(0LL, std::min(lo, total));
-            lo -= lo % spb;
+            lo -= lo % sal;
             hi = std::max(lo, std::min(hi, total));
             base[a] = lo;
-            len[a] = (hi - lo + spb - 1) / spb * spb;
+            len[a] = (hi - lo + sal - 1) / sal * sal;
             fits = len[a] <= x->win_cap;
             ulo = std::min(ulo, lo);
             uhi = std::max(uhi, base[a] + len[a]);
@@ -698,8 +710,9 @@ int fxc_process_host_window(fxc_ctx* x, const uint8_t* const* data, const double
         if (uniform && uhi - ulo <= x->win_cap) {
             // rows that are equally spaced but separately allocated are refused by the strided
             // copy (its source range spans the allocations): per-row copies from then on
-            one_copy = cudaMemcpy2DAsync(x->d_win[s], x->win_pitch, data[0] + ulo / spb, (size_t)rstride,
-                                         (size_t)((uhi - ulo) / spb), nrow, cudaMemcpyHostToDevice,
+            one_copy = cudaMemcpy2DAsync(x->d_win[s], x->win_pitch, data[0] + samples_to_bytes(c, ulo),
+                                         (size_t)rstride, (size_t)samples_to_bytes(c, uhi - ulo), nrow,
+                                         cudaMemcpyHostToDevice,
                                          x->copy_stream) == cudaSuccess;
             if (!one_copy) {
                 (void)cudaGetLastError();
@@ -715,8 +728,10 @@ int fxc_process_host_window(fxc_ctx* x, const uint8_t* const* data, const double
             for (int sb = 0; sb < c.nsubband; sb++)
                 for (int a = 0; a < c.nant; a++) {
                     const int r = sb * c.nant + a;
-                    FXC_CK(cudaMemcpyAsync(x->d_win[s] + (size_t)r * x->win_pitch, data[r] + base[a] / spb,
-                                           (size_t)(len[a] / spb), cudaMemcpyHostToDevice, x->copy_stream));
+                    FXC_CK(cudaMemcpyAsync(x->d_win[s] + (size_t)r * x->win_pitch,
+                                           data[r] + samples_to_bytes(c, base[a]),
+                                           (size_t)samples_to_bytes(c, len[a]), cudaMemcpyHostToDevice,
+                                           x->copy_stream));
                 }
         }
         FXC_CK(cudaEventRecord(x->win_ready[s], x->copy_stream));
@@ -953,7 +968,7 @@ int fxc_debug_delay_table(fxc_ctx* x, const double* delays, const double* offs, 
 int fxc_debug_unpack(fxc_ctx* x, const double* delays, const double* offs, int first, int nfft, float* out)
 {
     if (!x || !out) return FXC_ERR_INVALID;
-    if (!x->d_in) return FXC_ERR_UNSUPPORTED;
+    if (!x->d_in || x->cfg.iscomplex) return FXC_ERR_UNSUPPORTED;
     FXC_CK(cudaSetDevice(x->device));
     int ld = 0;
     int st = ctx_run_delay_table(x, delays, offs, first, nfft, &ld);

@@ -201,7 +201,8 @@ int fxc_batch_create(const fxc_config* cfgs, int njobs, fxc_batch** out)
     if (!cfgs || njobs < 1 || !out) return FXC_ERR_INVALID;
     *out = nullptr;
     for (int j = 0; j < njobs; j++)
-        if (cfgs[j].xmode != FXC_X_PLAIN_FP32 || cfgs[j].nant * cfgs[j].npol > 64 || cfgs[j].window_ffts != 0)
+        if (cfgs[j].xmode != FXC_X_PLAIN_FP32 || cfgs[j].nant * cfgs[j].npol > 64 || cfgs[j].window_ffts != 0 ||
+            cfgs[j].iscomplex)
             return FXC_ERR_UNSUPPORTED;
     fxc_batch* b = new fxc_batch();
     int st = FXC_OK;

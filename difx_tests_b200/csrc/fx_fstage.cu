@@ -31,7 +31,7 @@ size_t fstage_smem_8192(int mode, int tb, int npol);
 
 cudaError_t launch_fstage(int nchan, int mode, const FArgs& a, cudaStream_t st)
 {
-    switch (2 * nchan) {
+    switch (a.cpx ? nchan : 2 * nchan) {   // FFT length: complex samples fill every bin
     case 256: return launch_fstage_256(mode, a, st);
     case 512: return launch_fstage_512(mode, a, st);
     case 1024: return launch_fstage_1024(mode, a, st);

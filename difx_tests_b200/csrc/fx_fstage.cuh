@@ -29,9 +29,12 @@ namespace fx {
 
 constexpr int ilog2c(int x) { return x <= 1 ? 0 : 1 + ilog2c(x / 2); }
 
-template <int F>
+// FFT plan of length F.  CPX: complex input (8-bit complex samples), every bin a
+// channel (C = F); otherwise real input, channels below F/2 (C = F/2).  Only the
+// channel-side constants (C, STRIDE, S, FS, FST, NROT) depend on CPX.
+template <int F, bool CPX = false>
 struct FPlan {
-    static constexpr int C = F / 2;
+    static constexpr int C = CPX ? F : F / 2;
     static constexpr int NT = F / 16;                        // threads per FFT
     static constexpr int STRIDE = 1 << (ilog2c(C) / 2);      // kernel.c:31 generalised
     static constexpr int S = F / STRIDE;                      // substride (kernel.c:36)
@@ -48,6 +51,15 @@ struct FPlan {
     static constexpr int TWQ = F / 4;                         // quarter-wave twiddle table
     static constexpr int MINB = (NTHREADS <= 256) ? 2 : 1;    // CTAs per SM the registers must allow
 };
+
+// Staged input bytes per FFT slot: the FFT's bytes (2-bit real: F*npol/4 plus the
+// read-ahead byte of kernel.c:402-409; 8-bit complex: 2 bytes per sample and
+// polarisation) plus up to 15 bytes of 16-byte alignment slack, rounded to 16.
+template <int F, int NPOL, bool CPX>
+constexpr int fstage_inb()
+{
+    return ((CPX ? F * NPOL * 2 : F * NPOL / 4 + 1) + 15 + 15) / 16 * 16;
+}
 
 template <int F, int PASS>
 struct PassInfo {
@@ -204,11 +216,11 @@ __device__ __forceinline__ void pass_store(float2* buf, const float2* v, int t)
 // Divisions by F are multiplications by the exact power-of-two reciprocal.
 constexpr float kInvPiF = 0.318309886183790671538f;
 
-template <int F>
+template <int F, bool CPX>
 __device__ __forceinline__ float2 rot_entry(int e, const DelayEntry& d, double lo, double lofrac, bool fraclo,
                                             const float* ctab)
 {
-    using P = FPlan<F>;
+    using P = FPlan<F, CPX>;
     constexpr double kInvF = 1.0 / F;
     float x;
     if (e < P::S) {
@@ -279,14 +291,14 @@ using Tw2Of = PassTw<F, (FPlan<F>::NPASS > 2 ? 2 : 1)>;
 // One F-stage block: TB consecutive FFTs x NPOL of antenna `ant`, subband `sb`,
 // starting at chunk slot tb0.  Shared by the single-job grid (k_fstage) and the
 // persistent multi-job kernel (k_fstage_batch).
-template <int F, int MODE, int TB, int NPOL>
+template <int F, int MODE, int TB, int NPOL, bool CPX>
 __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant, int tb0, unsigned char* smem,
                                              const PassTw<F, 1>& tw1, const Tw2Of<F>& tw2)
 {
-    using P = FPlan<F>;
+    using P = FPlan<F, CPX>;
     constexpr int NT = P::NT;
     constexpr int C = P::C;
-    constexpr int INB = F / 2 + 16;                                    // staged bytes per slot
+    constexpr int INB = fstage_inb<F, NPOL, CPX>();                    // staged bytes per slot
     float2* bufs = reinterpret_cast<float2*>(smem);                   // [NSLOT][BUF]
     float2* tq = bufs + P::NSLOT * P::BUF;                              // [TWQ]
     float2* rtabs = tq + (P::TWREG ? 0 : P::TWQ);                      // [NSLOT][NROT]
@@ -314,12 +326,19 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
     constexpr int NITEM = TB * NPOL;
     const DelayEntry* dtab = args.dtab + (size_t)ant * args.ld + args.t_base;
 
-    // Input window of an item (kernel.c:402-409): 16-byte aligned start, one
-    // 128-bit vector per thread at most (F*NPOL/4 + 16 <= 16*NT).
+    // Input window of an item: 16-byte aligned start.  2-bit real (kernel.c:402-409):
+    // one 128-bit vector per thread at most (F*NPOL/4 + 16 <= 16*NT), prefetched into a
+    // register one item ahead; 8-bit complex: 2*NPOL vectors per thread, loaded per item.
     auto window = [&](const DelayEntry& d, int& base, int& nvec) {
-        const int first = (NPOL == 2) ? (d.offset >> 1) : (d.offset >> 2);
-        base = first & ~15;
-        nvec = (F * NPOL / 4 + 1 + (first - base) + 15) >> 4;
+        if constexpr (CPX) {
+            const int first = d.offset * 2 * NPOL;
+            base = first & ~15;
+            nvec = (F * NPOL * 2 + (first - base) + 15) >> 4;
+        } else {
+            const int first = (NPOL == 2) ? (d.offset >> 1) : (d.offset >> 2);
+            base = first & ~15;
+            nvec = (F * NPOL / 4 + 1 + (first - base) + 15) >> 4;
+        }
     };
 
     // Items (polarisation-major: item = pol * TB + FFT) are dealt to the slots in
@@ -340,7 +359,7 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
     }
     if (vn) {
         window(dn, basen, nvecn);
-        if (t < nvecn) pf = __ldg(reinterpret_cast<const uint4*>(row + basen) + t);
+        if (!CPX && t < nvecn) pf = __ldg(reinterpret_cast<const uint4*>(row + basen) + t);
     }
 
     for (; item < item_end; item++) {
@@ -350,7 +369,13 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
         const DelayEntry d = dn;
         const bool valid = vn;
         const int base_byte = basen;
-        if (valid && t < nvecn) reinterpret_cast<uint4*>(inb)[t] = pf;
+        if constexpr (CPX) {
+            if (valid)
+                for (int i = t; i < nvecn; i += NT)
+                    reinterpret_cast<uint4*>(inb)[i] = __ldg(reinterpret_cast<const uint4*>(row + base_byte) + i);
+        } else {
+            if (valid && t < nvecn) reinterpret_cast<uint4*>(inb)[t] = pf;
+        }
         // ---- prefetch the next item of this slot
         {
             const int ni = item + 1;
@@ -361,12 +386,12 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
             }
             if (vn) {
                 window(dn, basen, nvecn);
-                if (t < nvecn) pf = __ldg(reinterpret_cast<const uint4*>(row + basen) + t);
+                if (!CPX && t < nvecn) pf = __ldg(reinterpret_cast<const uint4*>(row + basen) + t);
             }
         }
         // ---- rotator tables for this FFT (per slot)
         for (int e = t; e < P::NROT; e += NT)
-            rtab[e] = valid ? rot_entry<F>(e, d, lo, lofrac, fraclo, ctab) : make_float2(0.f, 0.f);
+            rtab[e] = valid ? rot_entry<F, CPX>(e, d, lo, lofrac, fraclo, ctab) : make_float2(0.f, 0.f);
         slot_sync<NT>(slot);
 
         // ---- pass 0: unpack + fringe rotation + radix-16 (samples n = t + r*NT)
@@ -377,8 +402,11 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
             const int s0 = valid ? d.offset + t : t;
             const int b0 = valid ? base_byte : 0;
             const uint8_t* bp;
-            int sh;
-            if constexpr (NPOL == 2) {
+            int sh = 0;
+            if constexpr (CPX) {
+                // 8-bit complex: (re, im) int8 pairs, polarisations interleaved per sample
+                bp = inb + (s0 * 2 * NPOL + 2 * pol - b0);
+            } else if constexpr (NPOL == 2) {
                 bp = inb + ((s0 >> 1) - b0);
                 sh = 4 * (s0 & 1) + 2 * pol;
             } else {
@@ -395,8 +423,6 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
             }
 #pragma unroll
             for (int r = 0; r < 16; r++) {
-                const uint32_t byte = bp[r * (NT * NPOL / 4)];
-                const float lv = level2bit((byte >> sh) & 3u);
                 float2 rot;
                 if constexpr (NT % P::S == 0) {
                     rot = cmul(sub_c, stp[r * (NT / P::S)]);
@@ -404,7 +430,14 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
                     const int n = t + r * NT;
                     rot = cmul(fr_sub[n % P::S], fr_step[n / P::S]);
                 }
-                v[r] = make_float2(lv * rot.x, lv * rot.y);
+                if constexpr (CPX) {
+                    const char2 c8 = *reinterpret_cast<const char2*>(bp + r * (NT * 2 * NPOL));
+                    v[r] = cmul(make_float2((float)c8.x, (float)c8.y), rot);
+                } else {
+                    const uint32_t byte = bp[r * (NT * NPOL / 4)];
+                    const float lv = level2bit((byte >> sh) & 3u);
+                    v[r] = make_float2(lv * rot.x, lv * rot.y);
+                }
             }
         }
         dft<16>(v);
@@ -432,8 +465,13 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
         if constexpr (LP == 1) pass_load<F, 1>(buf, tq, &tw1, v, t);
         else if constexpr (LP == 2) pass_load<F, 2>(buf, tq, &tw2, v, t);
         else pass_load<F, 3>(buf, tq, nullptr, v, t);
+        // real input: outputs r < R/2 only (channels below F/2); complex input: every output
+        constexpr int NOUT = CPX ? LI::R : LI::R / 2;
 #pragma unroll
-        for (int b = 0; b < LI::NB; b++) dft_lo<LI::R>(v + b * LI::R);   // outputs r < R/2 only
+        for (int b = 0; b < LI::NB; b++) {
+            if constexpr (CPX) dft<LI::R>(v + b * LI::R);
+            else dft_lo<LI::R>(v + b * LI::R);
+        }
 
         // ---- fractional-sample correction + store of channels k = j + r*F/R < C
         constexpr int KSTEP = F / LI::R;
@@ -447,7 +485,7 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
             const float2 fsub = fc_sub[j % P::FS];
             const float2* fst = fc_step + j / P::FS;
 #pragma unroll
-            for (int r = 0; r < LI::R / 2; r++) {
+            for (int r = 0; r < NOUT; r++) {
                 const float2 fr = cmul(fsub, fst[r * (KSTEP / P::FS)]);
                 const float2 y = cmul(fr, v[b * LI::R + r]);
                 if constexpr (MODE == kSpecF32) {
@@ -510,7 +548,7 @@ __device__ __forceinline__ void fstage_prologue(unsigned char* smem, PassTw<F, 1
 }
 
 // Single job: grid (T / TB, nant, nsb).
-template <int F, int MODE, int TB, int NPOL>
+template <int F, int MODE, int TB, int NPOL, bool CPX>
 __global__ void __launch_bounds__(FPlan<F>::NTHREADS, FPlan<F>::MINB)
 k_fstage(FArgs args)
 {
@@ -518,12 +556,12 @@ k_fstage(FArgs args)
     PassTw<F, 1> tw1;
     Tw2Of<F> tw2;
     fstage_prologue<F>(smem, tw1, tw2);
-    fstage_block<F, MODE, TB, NPOL>(args, blockIdx.z, blockIdx.y, blockIdx.x * TB, smem, tw1, tw2);
+    fstage_block<F, MODE, TB, NPOL, CPX>(args, blockIdx.z, blockIdx.y, blockIdx.x * TB, smem, tw1, tw2);
 }
 
 // Many jobs in one persistent launch: CTAs stride over a task table
 // {job, subband, antenna, first slot}; every job of the launch has this F, NPOL
-// and spectra layout, each its own FArgs.
+// and spectra layout, each its own FArgs (2-bit real input).
 template <int F, int MODE, int TB, int NPOL>
 __global__ void __launch_bounds__(FPlan<F>::NTHREADS, FPlan<F>::MINB)
 k_fstage_batch(const FArgs* __restrict__ jobs, const int4* __restrict__ tasks, int ntask)
@@ -535,30 +573,30 @@ k_fstage_batch(const FArgs* __restrict__ jobs, const int4* __restrict__ tasks, i
     for (int i = blockIdx.x; i < ntask; i += gridDim.x) {
         const int4 tk = tasks[i];
         const FArgs a = jobs[tk.x];
-        fstage_block<F, MODE, TB, NPOL>(a, tk.y, tk.z, tk.w, smem, tw1, tw2);
+        fstage_block<F, MODE, TB, NPOL, false>(a, tk.y, tk.z, tk.w, smem, tw1, tw2);
         __syncthreads();   // the next task rewrites the channel table and staging buffers
     }
 }
 
-template <int F>
+template <int F, bool CPX = false>
 size_t fstage_smem(int mode, int tb, int npol)
 {
-    using P = FPlan<F>;
+    using P = FPlan<F, CPX>;
     size_t s = (size_t)P::NSLOT * P::BUF * sizeof(float2);
     if (!P::TWREG) s += (size_t)P::TWQ * sizeof(float2);
     s += (size_t)P::NSLOT * P::NROT * sizeof(float2);
     s += (size_t)(P::FS + P::FST) * sizeof(float);
-    s += (size_t)P::NSLOT * (F / 2 + 16);
+    s += (size_t)P::NSLOT * (npol == 2 ? fstage_inb<F, 2, CPX>() : fstage_inb<F, 1, CPX>());
     if (mode == kSpecF16) s += (size_t)npol * tb * P::C * sizeof(__half2);
     return s;
 }
 
-template <int F, int MODE, int TB, int NPOL>
+template <int F, int MODE, int TB, int NPOL, bool CPX>
 cudaError_t launch_f(const FArgs& a, cudaStream_t st)
 {
-    using P = FPlan<F>;
-    const size_t sm = fstage_smem<F>(MODE, TB, NPOL);
-    auto kern = k_fstage<F, MODE, TB, NPOL>;
+    using P = FPlan<F, CPX>;
+    const size_t sm = fstage_smem<F, CPX>(MODE, TB, NPOL);
+    auto kern = k_fstage<F, MODE, TB, NPOL, CPX>;
     static unsigned configured = 0;  // per instantiation and device
     cudaError_t e = set_smem_once(kern, sm, &configured);
     if (e != cudaSuccess) return e;
@@ -585,23 +623,48 @@ cudaError_t launch_fb(const FArgs* d_jobs, const int4* d_tasks, int ntask, cudaS
     return cudaGetLastError();
 }
 
+// FFT block size: the plan's (0: 16), reduced while the F16 staging (tb FFTs x npol x nchan)
+// does not fit the opt-in shared memory (down to 4: 8-byte row segments).
+template <int F, bool CPX>
+int fstage_tb(int mode, const FArgs& a)
+{
+    int tb = a.tb ? a.tb : 16;
+    if (CPX && tb > 16) tb = 16;   // complex input: 4, 8 and 16 FFTs per CTA are built
+    if (mode == kSpecF16) {
+        const size_t lim = smem_optin_limit();
+        while (tb > 4 && fstage_smem<F, CPX>(mode, tb, a.npol) > lim) tb /= 2;
+    }
+    return tb;
+}
+
 // Entry points of one FFT length, instantiated in its own translation unit.
 template <int F>
 cudaError_t launch_fstage_F(int mode, const FArgs& a, cudaStream_t st)
 {
-    int tb = a.tb ? a.tb : 16;
-    if (mode == kSpecF16) {
-        // the F16 staging (tb FFTs x npol x nchan) must fit the opt-in shared memory: fewer FFTs
-        // per CTA for long FFTs with two polarisations (down to 4: 8-byte row segments)
-        const size_t lim = smem_optin_limit();
-        while (tb > 4 && fstage_smem<F>(mode, tb, a.npol) > lim) tb /= 2;
-        if (tb == 4) return a.npol == 2 ? launch_f<F, kSpecF16, 4, 2>(a, st) : launch_f<F, kSpecF16, 4, 1>(a, st);
+    if constexpr (F <= 4096) if (a.cpx) {   // complex FFT length = nchan <= 4096
+        const int tb = fstage_tb<F, true>(mode, a);
+#define FX_TBC(TBV)                                                                                          \
+    if (tb == TBV) {                                                                                         \
+        if (mode == kSpecF32) return a.npol == 2 ? launch_f<F, kSpecF32, TBV, 2, true>(a, st)               \
+                                                 : launch_f<F, kSpecF32, TBV, 1, true>(a, st);              \
+        return a.npol == 2 ? launch_f<F, kSpecF16, TBV, 2, true>(a, st) : launch_f<F, kSpecF16, TBV, 1, true>(a, st); \
     }
+        if (tb == 4 && mode == kSpecF16)
+            return a.npol == 2 ? launch_f<F, kSpecF16, 4, 2, true>(a, st) : launch_f<F, kSpecF16, 4, 1, true>(a, st);
+        FX_TBC(8)
+        FX_TBC(16)
+#undef FX_TBC
+        return cudaErrorInvalidValue;
+    }
+    const int tb = fstage_tb<F, false>(mode, a);
+    if (tb == 4 && mode == kSpecF16)
+        return a.npol == 2 ? launch_f<F, kSpecF16, 4, 2, false>(a, st) : launch_f<F, kSpecF16, 4, 1, false>(a, st);
 #define FX_TB(TBV)                                                                                      \
     if (tb == TBV) {                                                                                    \
-        if (mode == kSpecF32) return a.npol == 2 ? launch_f<F, kSpecF32, TBV, 2>(a, st)                \
-                                                 : launch_f<F, kSpecF32, TBV, 1>(a, st);               \
-        return a.npol == 2 ? launch_f<F, kSpecF16, TBV, 2>(a, st) : launch_f<F, kSpecF16, TBV, 1>(a, st); \
+        if (mode == kSpecF32) return a.npol == 2 ? launch_f<F, kSpecF32, TBV, 2, false>(a, st)         \
+                                                 : launch_f<F, kSpecF32, TBV, 1, false>(a, st);        \
+        return a.npol == 2 ? launch_f<F, kSpecF16, TBV, 2, false>(a, st)                                \
+                           : launch_f<F, kSpecF16, TBV, 1, false>(a, st);                               \
     }
     FX_TB(8)
     FX_TB(16)

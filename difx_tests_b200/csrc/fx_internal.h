@@ -2,7 +2,9 @@
 // the sm_100a kernels of the FX correlator hot path.
 //
 // Device memory layout (one process call, per subintegration):
-//   packed input   u8   [nsb][nant][pitch]        pitch >= subintbytes + 16, 16-B multiple
+//   packed input   u8   [nsb][nant][pitch]        pitch >= subintbytes + 16, 16-B multiple; 2-bit real
+//                                                  (reference bit order) or 8-bit complex: int8 (re, im)
+//                                                  per polarisation, polarisations interleaved per sample
 //   delay table    DelayEntry [nant][ld]           one entry per (antenna, FFT of the call)
 //   valid bits     u32  [nant][ld/32]              bit t = antenna valid for FFT t
 //   spectra (F32)  f32x2 [nsb][nsig][T][nchan]     plain X stage input, channel-contiguous
@@ -57,6 +59,7 @@ struct FArgs {
     int tb;                     // FFTs per CTA (8, 16 or 32; 0 = 16), chosen by the plan / autotuner
     unsigned* amax;             // F16 layout, FP8 form: running absmax per (sb*nchan + chan, sig), or null
     int tspan;                  // slots [0, tspan) written (>= nfft, multiple of 64; 0 = T)
+    int cpx;                    // input format: 0 = 2-bit real, 1 = 8-bit complex (FFT length nchan)
 };
 
 

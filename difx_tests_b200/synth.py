@@ -147,13 +147,20 @@ def make_job(nant=4, npol=1, nchan=256, numffts=64, bw=32e6, lo=1.4e9, rho=0.1, 
                sb_lo=sb_lo)
 
 
-def random_job(nant=4, npol=1, nchan=256, numffts=64, bw=32e6, lo=1.4e9, seed=0, nsubband=1):
-    """Uncorrelated uniform random bytes with the same delay model (fast, any size)."""
+def subint_bytes_c8(nchan: int, numffts: int, npol: int) -> int:
+    """8-bit complex input: nchan complex samples per FFT, (numffts + 1) FFTs, an int8
+    (re, im) pair per sample and polarisation."""
+    return nchan * (numffts + 1) * 2 * npol
+
+
+def random_job(nant=4, npol=1, nchan=256, numffts=64, bw=32e6, lo=1.4e9, seed=0, nsubband=1, cpx=False):
+    """Uncorrelated uniform random bytes with the same delay model (fast, any size).
+    cpx: 8-bit complex samples (FFT length nchan, sample time 1/bw) instead of 2-bit real."""
     rng = np.random.default_rng(seed)
-    F = 2 * nchan
-    Ts = 1.0 / (2.0 * bw)
+    F = nchan if cpx else 2 * nchan
+    Ts = 1.0 / bw if cpx else 1.0 / (2.0 * bw)
     delays, fileoffsets = draw_delays(rng, nant, F * Ts)
-    sbb = subint_bytes(nchan, numffts, npol)
+    sbb = subint_bytes_c8(nchan, numffts, npol) if cpx else subint_bytes(nchan, numffts, npol)
     data = rng.integers(0, 256, size=(nsubband, nant, sbb), dtype=np.uint8)
     return Job(nant=nant, npol=npol, nchan=nchan, numffts=numffts, bw=bw, lo=lo,
                nsubband=nsubband, delays=delays, fileoffsets=fileoffsets, data=data,

@@ -18,7 +18,17 @@ twiG56/difx_tests) in numpy:
 Generalisations beyond the reference's CPU path (documented, used by the GPU
 path's parity tests): single polarisation input (4 consecutive samples per
 byte, LSB first), non-square channel counts, autocorrelations, several
-independent subbands.
+independent subbands, and 8-bit complex input (``cpx=True``).
+
+8-bit complex input is the reference's GPU-path format, which its CPU path
+rejects (kernel.c:392-394): each time sample is an int8 (re, im) pair per
+polarisation, polarisations interleaved per sample (gkernel.cu:277-296), sampled
+at the bandwidth (sampletime 1/bw, main_gpu.cu:246-247) with FFT length nchan
+(cfactor 1, main_gpu.cu:236-242), every FFT bin a channel.  The CPU path's own
+formulas carry over with that FFT length: substride = (2/cfact)*stride
+(kernel.c:16, 36) = F/stride, the rotator and fractional-sample tables
+unchanged.  No reference CPU output exists for this format, so its parity rests
+on these shared, pinned formulas; the unpack restates gkernel.cu's byte layout.
 """
 from __future__ import annotations
 
@@ -39,7 +49,7 @@ def lut2bit() -> np.ndarray:
     return LEVELS[(b >> (2 * i)) & 3]
 
 
-def geometry(nchan: int):
+def geometry(nchan: int, cpx: bool = False):
     """Derived sizes, kernel.c:13-36 generalised to any power-of-two channel count.
 
     Returns (fftchannels F, stride, substride S).  The reference requires nchan
@@ -49,7 +59,7 @@ def geometry(nchan: int):
     """
     if nchan <= 0 or nchan & (nchan - 1):
         raise ValueError("nchan must be a power of two")
-    F = 2 * nchan
+    F = nchan if cpx else 2 * nchan
     stride = 1 << (int(math.log2(nchan)) // 2)
     S = F // stride
     return F, stride, S
@@ -77,7 +87,7 @@ def station_delay(delays: np.ndarray, fftindex: np.ndarray):
     return a, b, mean
 
 
-def delay_table(delays, fileoffsets, bw, nchan, fftindex, maxoffset_ffts):
+def delay_table(delays, fileoffsets, bw, nchan, fftindex, maxoffset_ffts, cpx=False):
     """kernel.c:733-756: integer sample offset, fractional delay and validity.
 
     maxoffset_ffts is numffts*split of the reference (total FFTs of the
@@ -85,8 +95,8 @@ def delay_table(delays, fileoffsets, bw, nchan, fftindex, maxoffset_ffts):
     Returns dict of [nant][nfft] arrays: offset (int64), frac (float64 seconds),
     valid (bool), a, b (float64).
     """
-    F = 2 * nchan
-    sampletime = 1.0 / (2.0 * bw)  # kernel.c:14
+    F = nchan if cpx else 2 * nchan
+    sampletime = 1.0 / bw if cpx else 1.0 / (2.0 * bw)  # main_gpu.cu:246-247 / kernel.c:14
     a, b, mean = station_delay(np.asarray(delays, np.float64), fftindex)
     off = np.asarray(fileoffsets, np.float64)[:, None]
     nf = (mean - off) / sampletime
@@ -128,12 +138,25 @@ def unpack(data: np.ndarray, offsets: np.ndarray, F: int, npol: int) -> np.ndarr
     return out
 
 
+def unpack_c8(data: np.ndarray, offsets: np.ndarray, F: int, npol: int) -> np.ndarray:
+    """8-bit complex samples (gkernel.cu:277-296 byte layout): sample s of polarisation
+    p is the int8 pair at bytes 2*(s*npol + p), 2*(s*npol + p) + 1; returns complex128
+    [npol][nfft][F] for samples offset .. offset+F-1."""
+    s = offsets[:, None].astype(np.int64) + np.arange(F, dtype=np.int64)[None, :]
+    b = np.asarray(data).view(np.int8)
+    out = np.empty((npol,) + s.shape, dtype=np.complex128)
+    for p in range(npol):
+        i = 2 * (s * npol + p)
+        out[p] = b[i].astype(np.float64) + 1j * b[i + 1].astype(np.float64)
+    return out
+
+
 def _frac_int(x):
     """x - (int)x with C truncation (kernel.c:434-435, 465, 469)."""
     return x - np.trunc(x)
 
 
-def fringe_rotator(a, b, lo, nchan, ref_args=True):
+def fringe_rotator(a, b, lo, nchan, ref_args=True, cpx=False):
     """kernel.c:428-488: complex rotator for one FFT per (a, b) pair.
 
     a, b: float64 arrays (any shape).  Returns complex128 [..., F].
@@ -144,7 +167,7 @@ def fringe_rotator(a, b, lo, nchan, ref_args=True):
     (kernel.c:455-460).  The step spacing i*stride/F (kernel.c:145) is the
     reference's formula and is kept as is.
     """
-    F, stride, S = geometry(nchan)
+    F, stride, S = geometry(nchan, cpx)
     out_shape = np.broadcast(np.asarray(a), np.asarray(b)).shape + (F,)
     a = np.asarray(a, np.float64)[..., None]
     b = np.asarray(b, np.float64)[..., None]
@@ -203,7 +226,7 @@ def frac_rotator(frac, bw, nchan, ref_args=True):
 
 
 def channelise(data, delays, fileoffsets, bw, lo, nchan, npol, fftindex, maxoffset_ffts,
-               ref_args=True):
+               ref_args=True, cpx=False):
     """Per antenna: unpack -> fringe rotate -> FFT -> fractional-sample correct.
 
     Follows kernel.c:725-789 for every FFT in fftindex.  data: [nant][nbytes]
@@ -212,8 +235,8 @@ def channelise(data, delays, fileoffsets, bw, lo, nchan, npol, fftindex, maxoffs
     """
     data = np.asarray(data)
     nant = data.shape[0]
-    F = 2 * nchan
-    tab = delay_table(delays, fileoffsets, bw, nchan, fftindex, maxoffset_ffts)
+    F = nchan if cpx else 2 * nchan
+    tab = delay_table(delays, fileoffsets, bw, nchan, fftindex, maxoffset_ffts, cpx)
     nfft = len(fftindex)
     spec = np.zeros((nant, npol, nfft, nchan), dtype=np.complex128)
     for ant in range(nant):
@@ -221,8 +244,11 @@ def channelise(data, delays, fileoffsets, bw, lo, nchan, npol, fftindex, maxoffs
         if not v.any():
             continue
         idx = np.nonzero(v)[0]
-        x = unpack(data[ant], tab["offset"][ant, idx], F, npol).astype(np.float64)  # [P][n][F]
-        rot = fringe_rotator(tab["a"][ant, idx], tab["b"][ant, idx], lo, nchan, ref_args)
+        if cpx:
+            x = unpack_c8(data[ant], tab["offset"][ant, idx], F, npol)                 # [P][n][F]
+        else:
+            x = unpack(data[ant], tab["offset"][ant, idx], F, npol).astype(np.float64)  # [P][n][F]
+        rot = fringe_rotator(tab["a"][ant, idx], tab["b"][ant, idx], lo, nchan, ref_args, cpx)
         X = np.fft.fft(x * rot[None], axis=-1)[..., :nchan]
         X = X * frac_rotator(tab["frac"][ant, idx], bw, nchan, ref_args)[None]
         spec[ant][:, idx, :] = X
@@ -235,7 +261,7 @@ def baseline_order(nant):
 
 
 def correlate(data, delays, fileoffsets, bw, lo, nchan, npol, fftindex=None, numffts=None,
-              maxoffset_ffts=None, ref_args=True, chunk=256):
+              maxoffset_ffts=None, ref_args=True, chunk=256, cpx=False):
     """Full per-subintegration FX correlation in float64 (kernel.c:709-854).
 
     Returns (vis, counts):
@@ -258,7 +284,7 @@ def correlate(data, delays, fileoffsets, bw, lo, nchan, npol, fftindex=None, num
     for c0 in range(0, len(fftindex), chunk):
         idx = fftindex[c0:c0 + chunk]
         spec, tab = channelise(data, delays, fileoffsets, bw, lo, nchan, npol, idx,
-                               maxoffset_ffts, ref_args)
+                               maxoffset_ffts, ref_args, cpx=cpx)
         valid_all[:, c0:c0 + len(idx)] = tab["valid"]
         X = spec.reshape(nsig, len(idx), nchan).transpose(2, 0, 1)  # [C][sig][t]
         V += X @ np.conj(X).transpose(0, 2, 1)

@@ -136,3 +136,16 @@ def test_plan_arguments_rejected():
     assert L.fxc_set_plan(None, 16, 0) == fx.FXC_ERR_INVALID
     assert L.fxc_get_plan(None, None, None) == fx.FXC_ERR_INVALID
     assert L.fxc_autotune(None, 1) == fx.FXC_ERR_INVALID
+
+
+def test_complex_input_config_rules():
+    L = fx.lib()
+    ctx = C.c_void_p()
+    cfg = fx.make_config(4, 128, 64, 32e6, 1.4e9, cpx=True)
+    assert L.fxc_create(C.byref(cfg), C.byref(ctx)) == fx.FXC_ERR_UNSUPPORTED     # complex FFT length >= 256
+    cfg = fx.make_config(4, 256, 64, 32e6, 1.4e9)
+    cfg.nbit = 8                                                                   # 8-bit real: not a format
+    assert L.fxc_create(C.byref(cfg), C.byref(ctx)) == fx.FXC_ERR_UNSUPPORTED
+    cfg = fx.make_config(4, 1024, 99, 32e6, 1.4e9, npol=2, cpx=True)
+    assert L.fxc_subint_bytes(C.byref(cfg)) == 1024 * 100 * 4
+    assert not ctx.value

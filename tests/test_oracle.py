@@ -132,3 +132,30 @@ def test_generator_phases_align():
     assert np.all(np.abs(np.angle(cross)) < 0.15)
     ratio = np.abs(cross) / auto
     assert np.all((ratio > 0.12) & (ratio < 0.22)), ratio
+
+
+def test_unpack_c8_byte_layout():
+    """8-bit complex: int8 (re, im) per sample and polarisation, polarisations interleaved."""
+    npol, F = 2, 4
+    raw = np.arange(2 * npol * 8, dtype=np.int16) - 10          # samples 0..7
+    data = raw.astype(np.int8).view(np.uint8)
+    x = fo.unpack_c8(data, np.array([1, 3]), F, npol)          # [pol][fft][n]
+    for k, off in enumerate((1, 3)):
+        for p in range(npol):
+            for n in range(F):
+                i = 2 * ((off + n) * npol + p)
+                assert x[p, k, n] == complex(raw[i], raw[i + 1])
+    assert synth.subint_bytes_c8(1024, 99, 2) == 1024 * 100 * 4
+
+
+def test_complex_geometry_and_delays():
+    F, stride, S = fo.geometry(1024, cpx=True)
+    assert (F, stride, S) == (1024, 32, 32)
+    job = synth.random_job(nant=3, npol=1, nchan=512, numffts=40, bw=64e6, seed=5, cpx=True)
+    tab = fo.delay_table(job.delays, job.fileoffsets, job.bw, job.nchan, np.arange(40), 40, cpx=True)
+    # offsets in complex samples (sample time 1/bw), FFT length nchan
+    a, b, mean = fo.station_delay(job.delays, np.arange(40))
+    n = np.trunc((mean - job.fileoffsets[:, None]) * job.bw + 0.5).astype(np.int64)
+    expect = np.arange(40)[None, :] * 512 - n
+    v = tab["valid"]
+    np.testing.assert_array_equal(tab["offset"][v], expect[v])
