@@ -235,10 +235,19 @@ class Correlator:
         _check(_lib().fxc_device_input(self._ctx, C.byref(p), C.byref(pitch)), "fxc_device_input")
         return p.value, pitch.value
 
-    def visibilities(self, normalize=False):
-        """-> (vis complex64 [nsb][nbl + nant][npol^2][nchan], counts int32 [nbl + nant])."""
+    def visibilities(self, normalize=False, out=None):
+        """-> (vis complex64 [nsb][nbl + nant][npol^2][nchan], counts int32 [nbl + nant]).
+
+        out: optional caller-owned buffer of the same number of complex64 values (any
+        shape); pinned memory (fxc_host_alloc, torch pin_memory) reads back at full
+        bandwidth, a fresh pageable array goes through the driver's staging copies."""
         n = self.nsb * (self.nbl + self.nant) * self.npol ** 2 * self.nchan
-        out = np.empty(2 * n, dtype=np.float32)
+        if out is None:
+            out = np.empty(2 * n, dtype=np.float32)
+        else:
+            out = out.reshape(-1).view(np.float32)
+            if out.size != 2 * n or not out.flags.c_contiguous:
+                raise ValueError("out must be a contiguous buffer of the visibility size")
         counts = np.empty(self.nbl + self.nant, dtype=np.int32)
         _check(_lib().fxc_get_visibilities(self._ctx, out.ctypes.data_as(_FP), counts.ctypes.data_as(_IP),
                                            1 if normalize else 0), "fxc_get_visibilities")

@@ -193,7 +193,8 @@ static void free_ctx(fxc_ctx* x)
     if (!x) return;
     cudaFree(x->d_in);
     cudaFree(x->d_delays);
-    for (int s = 0; s < 2; s++) {
+    cudaFree(x->d_win_meta);
+    for (int s = 0; s < fxc_ctx::NWIN; s++) {
         cudaFree(x->d_win[s]);
         if (x->win_ready[s]) cudaEventDestroy(x->win_ready[s]);
         if (x->win_free[s]) cudaEventDestroy(x->win_free[s]);
@@ -309,10 +310,13 @@ int ctx_create(const fxc_config* cfg, fxc_ctx** out, bool group_subbands)
         if ((e = cudaMalloc(&x->d_in, in_bytes)) != cudaSuccess) return fail(e);
         if ((e = cudaMemset(x->d_in, 0, in_bytes)) != cudaSuccess) return fail(e);
     }
-    x->win_ffts = c.window_ffts > 0 ? c.window_ffts : x->T;
+    // streamed windows: short, so the first copy and the last window's correlation (the parts
+    // that cannot overlap) stay small
+    x->win_ffts = c.window_ffts > 0 ? c.window_ffts : std::min(x->T, 1024);
     if ((e = cudaMalloc(&x->d_delays, fxc_ctx::NMODEL * sizeof(double) * c.nant)) != cudaSuccess) return fail(e);
     x->d_offs = x->d_delays + 3 * c.nant;
-    x->d_win_meta = x->d_delays + 4 * c.nant;
+    if ((e = cudaMalloc(&x->d_win_meta, (fxc_ctx::NWIN + 1) * 2 * sizeof(double) * c.nant)) != cudaSuccess)
+        return fail(e);
     x->last_model.assign(4 * (size_t)c.nant, 0.0);
     if ((e = cudaHostAlloc(&x->h_stage, fxc_ctx::NRING * fxc_ctx::NMODEL * sizeof(double) * c.nant,
                            cudaHostAllocDefault)) != cudaSuccess)
@@ -441,8 +445,27 @@ int fxc_host_free(void* p)
 }  // extern "C"
 
 // delays / offsets to the device, then K0 over FFTs first..first+nfft-1
+// Window bases and lengths (samples; exact as doubles below 2^53) to the device window
+// descriptor d_meta, through a pinned ring slot, on stream st.
+static int upload_window_meta(fxc_ctx* x, const long long* base, const long long* len, double* d_meta,
+                              cudaStream_t st)
+{
+    const int n = x->cfg.nant;
+    const int slot = x->stage_next;
+    x->stage_next = (slot + 1) % fxc_ctx::NRING;
+    FXC_CK(cudaEventSynchronize(x->stage_ev[slot]));
+    double* h = x->h_stage + slot * fxc_ctx::NMODEL * (size_t)n;
+    for (int a = 0; a < n; a++) {
+        h[a] = (double)base[a];
+        h[n + a] = (double)len[a];
+    }
+    FXC_CK(cudaMemcpyAsync(d_meta, h, 2 * sizeof(double) * n, cudaMemcpyHostToDevice, st));
+    FXC_CK(cudaEventRecord(x->stage_ev[slot], st));
+    return FXC_OK;
+}
+
 int ctx_run_delay_table(fxc_ctx* x, const double* delays, const double* offs, int first, int nfft, int* ld_out,
-                        const long long* win_base, const long long* win_len)
+                        const double* d_meta)
 {
     const fxc_config& c = x->cfg;
     if (!delays || !offs || first < 0 || nfft < 1 || (long long)first + nfft > c.numffts) return FXC_ERR_INVALID;
@@ -470,25 +493,12 @@ int ctx_run_delay_table(fxc_ctx* x, const double* delays, const double* offs, in
         std::memcpy(x->last_model.data(), h, nmodel * sizeof(double));
         x->model_valid = true;
     }
-    if (win_base) {
-        // window bases and lengths of this call (samples; exact as doubles below 2^53)
-        const int slot = x->stage_next;
-        x->stage_next = (slot + 1) % fxc_ctx::NRING;
-        FXC_CK(cudaEventSynchronize(x->stage_ev[slot]));
-        double* h = x->h_stage + slot * slot_doubles;
-        for (int a = 0; a < c.nant; a++) {
-            h[a] = (double)win_base[a];
-            h[c.nant + a] = (double)win_len[a];
-        }
-        FXC_CK(cudaMemcpyAsync(x->d_win_meta, h, 2 * sizeof(double) * c.nant, cudaMemcpyHostToDevice, x->stream));
-        FXC_CK(cudaEventRecord(x->stage_ev[slot], x->stream));
-    }
     const int ld = (int)round_up((size_t)nfft, 128);
     const int maxoffset = (c.numffts - 1) * x->F;  // kernel.c:730
     // kernel.c:14 (real sampling); complex sampling at bw (main_gpu.cu:246-247)
     const double sampletime = c.iscomplex ? 1.0 / c.bw : 1.0 / (2.0 * c.bw);
     FXC_CK(launch_delay_table_window(x->d_delays, x->d_offs, nullptr, first, c.nant, nfft, ld, x->F, maxoffset,
-                                     sampletime, win_base ? x->d_win_meta : nullptr, tail_samples(c), x->d_err + 1,
+                                     sampletime, d_meta, tail_samples(c), x->d_err + 1,
                                      x->d_dtab, x->d_vbits, x->stream));
     *ld_out = ld;
     return FXC_OK;
@@ -521,13 +531,13 @@ extern "C" {
 }  // extern "C"
 
 // One call's correlation of device rows: whole subintegrations (win_base null) or windows.
-static int ctx_correlate(fxc_ctx* x, const uint8_t* d_data, size_t pitch, const long long* win_base,
-                         const long long* win_len, const double* delays, const double* offs, int first, int nfft)
+static int ctx_correlate(fxc_ctx* x, const uint8_t* d_data, size_t pitch, const double* d_meta,
+                         const double* delays, const double* offs, int first, int nfft)
 {
     int ld = 0;
     {
         StageScope sc(x, 0, 2);
-        int st = ctx_run_delay_table(x, delays, offs, first, nfft, &ld, win_base, win_len);
+        int st = ctx_run_delay_table(x, delays, offs, first, nfft, &ld, d_meta);
         if (st != FXC_OK) return st;
         FXC_CK(launch_counts(x->d_vbits, x->cfg.nant, ld / 32, x->d_counts, x->stream));
     }
@@ -593,7 +603,7 @@ int fxc_process_device(fxc_ctx* x, const uint8_t* d_data, size_t pitch, const do
 {
     if (!x || !d_data || pitch < x->subint + 16 || pitch % 16 || ((uintptr_t)d_data & 15)) return FXC_ERR_INVALID;
     FXC_CK(cudaSetDevice(x->device));
-    return ctx_correlate(x, d_data, pitch, nullptr, nullptr, delays, offs, first, nfft);
+    return ctx_correlate(x, d_data, pitch, nullptr, delays, offs, first, nfft);
 }
 
 int fxc_process_device_window(fxc_ctx* x, const uint8_t* d_data, size_t pitch, const long long* base_sample,
@@ -607,7 +617,11 @@ int fxc_process_device_window(fxc_ctx* x, const uint8_t* d_data, size_t pitch, c
     for (int a = 0; a < c.nant; a++)
         if (base_sample[a] < 0 || base_sample[a] % sample_align(c)) return FXC_ERR_INVALID;
     FXC_CK(cudaSetDevice(x->device));
-    return ctx_correlate(x, d_data, pitch, base_sample, len.data(), delays, offs, first, nfft);
+    // the caller's rows: the descriptor slot after the host windows', uploaded on the compute stream
+    double* d_meta = x->d_win_meta + (size_t)fxc_ctx::NWIN * 2 * c.nant;
+    const int st = upload_window_meta(x, base_sample, len.data(), d_meta, x->stream);
+    if (st != FXC_OK) return st;
+    return ctx_correlate(x, d_data, pitch, d_meta, delays, offs, first, nfft);
 }
 
 }  // extern "C"
@@ -649,7 +663,7 @@ static int ensure_windows(fxc_ctx* x)
     x->win_cap = (long long)(x->win_ffts + 4) * x->F;
     x->win_pitch = round_up((size_t)samples_to_bytes(c, x->win_cap) + 32, 256);
     const size_t bytes = (size_t)c.nsubband * c.nant * x->win_pitch;
-    for (int s = 0; s < 2; s++) {
+    for (int s = 0; s < fxc_ctx::NWIN; s++) {
         FXC_CK(cudaMalloc(&x->d_win[s], bytes));
         FXC_CK(cudaEventCreateWithFlags(&x->win_ready[s], cudaEventDisableTiming));
         FXC_CK(cudaEventCreateWithFlags(&x->win_free[s], cudaEventDisableTiming));
@@ -703,9 +717,12 @@ int fxc_process_host_window(fxc_ctx* x, const uint8_t* const* data, const double
             continue;
         }
         const int s = x->win_next;
-        x->win_next ^= 1;
-        // copy stream: wait until the previous user of this window is done, then fill it
+        x->win_next = (s + 1) % fxc_ctx::NWIN;
+        // copy stream: wait until the previous user of this window is done, then fill it and its
+        // descriptor.  The descriptor goes on the copy stream too: an upload on the compute
+        // stream would queue on the copy engine behind the window copies running ahead of it.
         FXC_CK(cudaStreamWaitEvent(x->copy_stream, x->win_free[s], 0));
+        double* d_meta = x->d_win_meta + (size_t)s * 2 * c.nant;
         bool one_copy = false;
         if (uniform && uhi - ulo <= x->win_cap) {
             // rows that are equally spaced but separately allocated are refused by the strided
@@ -734,9 +751,11 @@ int fxc_process_host_window(fxc_ctx* x, const uint8_t* const* data, const double
                                            x->copy_stream));
                 }
         }
+        st = upload_window_meta(x, base.data(), len.data(), d_meta, x->copy_stream);
+        if (st != FXC_OK) return st;
         FXC_CK(cudaEventRecord(x->win_ready[s], x->copy_stream));
         FXC_CK(cudaStreamWaitEvent(x->stream, x->win_ready[s], 0));
-        st = ctx_correlate(x, x->d_win[s], x->win_pitch, base.data(), len.data(), delays, offs, k, n);
+        st = ctx_correlate(x, x->d_win[s], x->win_pitch, d_meta, delays, offs, k, n);
         if (st != FXC_OK) return st;
         FXC_CK(cudaEventRecord(x->win_free[s], x->stream));
         k += n;

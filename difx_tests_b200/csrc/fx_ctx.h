@@ -41,19 +41,20 @@ struct fxc_ctx {
     int* d_counts = nullptr;
     int* d_err = nullptr;   // device-side wait expiry code of the tensor-core X stage
     int nsm = 148;
-    // delay-model upload: [3*nant delays | nant file offsets | nant window bases | nant window
-    // lengths], pinned ring; d_win_meta = d_delays + 4*nant
+    // delay-model upload: [3*nant delays | nant file offsets] (d_delays), or window descriptors
+    // [nant bases | nant lengths], through a pinned ring of slots
     static constexpr int NRING = 4;
     static constexpr int NMODEL = 6;   // doubles per antenna in a ring slot
-    double* d_win_meta = nullptr;
+    double* d_win_meta = nullptr;      // NWIN + 1 window descriptors (host windows, caller's rows)
     // streamed host input: two device windows of win_cap samples per row, filled on copy_stream
     int win_ffts = 0;
     long long win_cap = 0;
     size_t win_pitch = 0;
-    uint8_t* d_win[2] = {nullptr, nullptr};
+    static constexpr int NWIN = 3;     // copies may run two windows ahead of the correlation
+    uint8_t* d_win[NWIN] = {};
     cudaStream_t copy_stream = nullptr;
-    cudaEvent_t win_ready[2] = {nullptr, nullptr};
-    cudaEvent_t win_free[2] = {nullptr, nullptr};
+    cudaEvent_t win_ready[NWIN] = {};
+    cudaEvent_t win_free[NWIN] = {};
     int win_next = 0;
     double* h_stage = nullptr;
     cudaEvent_t stage_ev[NRING] = {};
@@ -87,9 +88,10 @@ void plan_cache_append(const std::vector<std::string>& lines);
 // multi-job batch's task tables assume)
 int ctx_create(const fxc_config* cfg, fxc_ctx** out, bool group_subbands);
 
-// delay model to the device (only when it changed) + K0 over FFTs first..first+nfft-1; with
-// win_base/win_len (host, per antenna, samples) the input rows are windows (see k_delay_table)
+// delay model to the device (only when it changed) + K0 over FFTs first..first+nfft-1; with a
+// device window descriptor d_meta ([nant bases | nant lengths], samples) the input rows are
+// windows (see k_delay_table)
 int ctx_run_delay_table(fxc_ctx* x, const double* delays, const double* offs, int first, int nfft, int* ld_out,
-                        const long long* win_base = nullptr, const long long* win_len = nullptr);
+                        const double* d_meta = nullptr);
 // F-stage arguments of this context for device input rows d_data of `pitch` bytes
 fx::FArgs ctx_fargs(fxc_ctx* x, const uint8_t* d_data, size_t pitch, int ld);

@@ -64,7 +64,8 @@ typedef struct fxc_config {
                           spectra of a chunk stay within 2 GiB (plain) / 16 GiB (tensor cores), or
                           the environment variable FXC_SPECTRA_BUDGET_MB; problems too large for
                           long chunks of every subband are chunked over groups of subbands */
-    int window_ffts;   /* FFTs per streamed input window (fxc_process_host*); 0 = the chunk length.
+    int window_ffts;   /* FFTs per streamed input window (fxc_process_host*); 0 = the chunk length,
+                          at most 1024 (three windows in flight: copies run ahead of the correlation).
                           > 0 also drops the whole-subintegration device input buffer, so the
                           subintegration never has to fit in device memory (fxc_upload_input and
                           fxc_device_input then return FXC_ERR_UNSUPPORTED) */
@@ -130,7 +131,7 @@ int fxc_process_device_window(fxc_ctx* ctx, const uint8_t* d_data, size_t pitch,
                               int nfft);
 /* Host rows of the whole subintegration (as fxc_process_host).  Copies only the bytes
  * FFTs [first, first + nfft) need, window by window (window_ffts FFTs each), into one of
- * two device windows on a copy stream, so the copy of one window overlaps the
+ * three device windows on a copy stream, so the copy of one window overlaps the
  * correlation of the previous one (pinned host rows, e.g. fxc_host_alloc, are needed for
  * the overlap).  fxc_process_host is this call over its FFT range. */
 int fxc_process_host_window(fxc_ctx* ctx, const uint8_t* const* data, const double* delays,

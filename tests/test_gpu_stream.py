@@ -1,4 +1,4 @@
-"""Streamed input: host subintegrations copied window by window (two device
+"""Streamed input: host subintegrations copied window by window (three device
 windows, copies on their own stream), explicit device windows, and the
 coverage check that keeps an FFT from reading outside its window.
 
