@@ -246,9 +246,9 @@ __device__ __forceinline__ float2 rot_entry(int e, const DelayEntry& d, double l
 }
 
 // One (polarisation, channel) row pair of the F16 layout: NR consecutive FFTs from
-// the stage (element q at src[q * C], Re/Im half2) to the Re row at dst and
+// the stage (element q at src[q * CS], Re/Im half2) to the Re row at dst and
 // the Im row at dst + T; for the FP8 form also the running absmax.
-template <int NR, int NPOL, int C>
+template <int NR, int NPOL, int C, int CS>
 __device__ __forceinline__ void flush_row(const FArgs& args, const __half2* src, int sb, int ant, int pol, int k,
                                           __half* dst)
 {
@@ -257,8 +257,8 @@ __device__ __forceinline__ void flush_row(const FArgs& args, const __half2* src,
     __half2 mx = __float2half2_rn(0.f);
 #pragma unroll
     for (int q = 0; q < NR / 2; q++) {
-        const __half2 h0 = src[(2 * q) * C];
-        const __half2 h1 = src[(2 * q + 1) * C];
+        const __half2 h0 = src[(2 * q) * CS];
+        const __half2 h1 = src[(2 * q + 1) * CS];
         const __half2 r2 = __lows2half2(h0, h1);
         const __half2 i2 = __highs2half2(h0, h1);
         rw[q] = *reinterpret_cast<const uint32_t*>(&r2);
@@ -304,7 +304,9 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
     float2* rtabs = tq + (P::TWREG ? 0 : P::TWQ);                      // [NSLOT][NROT]
     float* ctab = reinterpret_cast<float*>(rtabs + P::NSLOT * P::NROT);     // [FS + FST] channel freqs
     uint8_t* inbs = reinterpret_cast<uint8_t*>(ctab + P::FS + P::FST);      // [NSLOT][INB]
-    __half2* stage = reinterpret_cast<__half2*>(inbs + P::NSLOT * INB);       // [NPOL][TB][C]
+    // [NPOL][TB][CS]: rows padded by 2 half2, so paired flush lanes 8 FFTs apart read other banks
+    constexpr int CS = C + 2;
+    __half2* stage = reinterpret_cast<__half2*>(inbs + P::NSLOT * INB);
 
     const int tid = threadIdx.x;
     const int slot = tid / NT;
@@ -493,7 +495,7 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
                                   (((size_t)sb * nsig + sig) * args.T + tc) * C + j;
                     if (tc < args.T) out[r * KSTEP] = y;
                 } else {
-                    stage[(pol * TB + tl) * C + j + r * KSTEP] = __floats2half2_rn(y.x, y.y);
+                    stage[(pol * TB + tl) * CS + j + r * KSTEP] = __floats2half2_rn(y.x, y.y);
                 }
             }
         }
@@ -502,7 +504,28 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
 
     if constexpr (MODE == kSpecF16) {
         __half* spec = reinterpret_cast<__half*>(args.spec);
-        if constexpr (SEG >= 4) {
+        auto row_dst = [&](int pol, int k) {
+            return spec + (((size_t)sb * C + k) * args.rows + 2 * (ant * NPOL + pol)) * (size_t)args.T + tb0;
+        };
+        if constexpr (TB >= 16) {
+            // whole 32-byte row segments, written by lane pairs: lanes l and l + 16 of a warp
+            // take the first and second 8 FFTs of the same (polarisation, channel), so each
+            // store instruction covers 16 full sectors (the CTA's 16 FFTs of a row are only
+            // all staged after a CTA-wide barrier; one slot needs none)
+            if constexpr (P::NSLOT > 1) __syncthreads();
+            for (int e = tid; e < 2 * NPOL * C; e += P::NTHREADS) {
+                const int lane = e & 31;
+                const int h = lane >> 4;
+                const int idx = (e >> 5) * 16 + (lane & 15);
+                const int pol = idx / C;
+                const int k = idx - pol * C;
+                for (int hb = 0; hb < TB / 16; hb++) {   // 16-FFT segments of the row
+                    const int tl0 = hb * 16 + h * 8;
+                    flush_row<8, NPOL, C, CS>(args, stage + (pol * TB + tl0) * CS + k, sb, ant, pol, k,
+                                              row_dst(pol, k) + tl0);
+                }
+            }
+        } else if constexpr (SEG >= 4) {
             // flush of this slot's rows: FFTs [tl0, tl0 + NR) of NPS polarisations (the slot's
             // last slot_sync made its stage entries visible to all its threads)
             constexpr int NR = SEG < TB ? SEG : TB;
@@ -512,9 +535,8 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
             for (int e = t; e < NPS * C; e += NT) {
                 const int pol = pol0 + e / C;
                 const int k = e % C;
-                flush_row<NR, NPOL, C>(args, stage + (pol * TB + tl0) * C + k, sb, ant, pol, k,
-                                    spec + (((size_t)sb * C + k) * args.rows + 2 * (ant * NPOL + pol)) *
-                                               (size_t)args.T + tb0 + tl0);
+                flush_row<NR, NPOL, C, CS>(args, stage + (pol * TB + tl0) * CS + k, sb, ant, pol, k,
+                                           row_dst(pol, k) + tl0);
             }
         } else {
             __syncthreads();
@@ -522,9 +544,7 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
             for (int e = tid; e < NPOL * C; e += P::NTHREADS) {
                 const int pol = e / C;
                 const int k = e - pol * C;
-                flush_row<TB, NPOL, C>(args, stage + (pol * TB) * C + k, sb, ant, pol, k,
-                                    spec + (((size_t)sb * C + k) * args.rows + 2 * (ant * NPOL + pol)) *
-                                               (size_t)args.T + tb0);
+                flush_row<TB, NPOL, C, CS>(args, stage + (pol * TB) * CS + k, sb, ant, pol, k, row_dst(pol, k));
             }
         }
     }
@@ -587,7 +607,7 @@ size_t fstage_smem(int mode, int tb, int npol)
     s += (size_t)P::NSLOT * P::NROT * sizeof(float2);
     s += (size_t)(P::FS + P::FST) * sizeof(float);
     s += (size_t)P::NSLOT * (npol == 2 ? fstage_inb<F, 2, CPX>() : fstage_inb<F, 1, CPX>());
-    if (mode == kSpecF16) s += (size_t)npol * tb * P::C * sizeof(__half2);
+    if (mode == kSpecF16) s += (size_t)npol * tb * (P::C + 2) * sizeof(__half2);
     return s;
 }
 
