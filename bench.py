@@ -305,7 +305,7 @@ def run_reference_arm(args):
 # dram__bytes_read.sum + dram__bytes_write.sum from one ncu capture of
 # k_fstage<2048,1,16,1> on the 64-antenna x 1024-channel profiling case, divided
 # by the samples of that launch (profiles/kernels_cfg2s_ncu_full.txt).
-FSTAGE_TC_DRAM_BYTES_PER_SAMPLE = 2.19
+FSTAGE_TC_DRAM_BYTES_PER_SAMPLE = 2.17
 
 
 XMODES = {"plain": 0, "tc": 1, "fp8": 2}    # FXC_X_PLAIN_FP32, FXC_X_TC_FP16, FXC_X_TC_FP8
