@@ -38,6 +38,15 @@ inline size_t smem_optin_limit()
     return (size_t)v;
 }
 
+// Shared memory of one SM of the current device (all resident CTAs together).
+inline size_t smem_per_sm_limit()
+{
+    int dev = 0, v = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess) return 0;
+    return (size_t)v;
+}
+
 // ---------------------------------------------------------------- FP64 (no FMA)
 __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }

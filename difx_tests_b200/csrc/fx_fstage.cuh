@@ -307,6 +307,9 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
     // [NPOL][TB][CS]: rows padded by 2 half2, so paired flush lanes 8 FFTs apart read other banks
     constexpr int CS = C + 2;
     __half2* stage = reinterpret_cast<__half2*>(inbs + P::NSLOT * INB);
+    // one FFT slot per CTA and two polarisations: the stage holds one polarisation's FFTs and is
+    // flushed when they are done (items are polarisation-major), so twice the FFT block fits
+    constexpr bool PERPOL = (MODE == kSpecF16) && (P::NSLOT == 1) && (NPOL == 2);
 
     const int tid = threadIdx.x;
     const int slot = tid / NT;
@@ -340,6 +343,38 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
             const int first = (NPOL == 2) ? (d.offset >> 1) : (d.offset >> 2);
             base = first & ~15;
             nvec = (F * NPOL / 4 + 1 + (first - base) + 15) >> 4;
+        }
+    };
+
+    // F16 destination of (polarisation, channel) rows of this block
+    auto row_dst = [&](int pol, int k) {
+        return reinterpret_cast<__half*>(args.spec) +
+               (((size_t)sb * C + k) * args.rows + 2 * (ant * NPOL + pol)) * (size_t)args.T + tb0;
+    };
+    // Flush of every channel's Re/Im rows of polarisations [p0, p0 + np) from stage rows
+    // (pol - sp0) * TB + tl, by all threads of the CTA; 32-byte row segments by lane pairs (lanes
+    // l and l + 16 take the first and second 8 FFTs of one channel: 16 whole sectors per store).
+    auto flush_pols = [&](int p0, int np, int sp0) {
+        if constexpr (TB >= 16) {
+            for (int e = tid; e < 2 * np * C; e += P::NTHREADS) {
+                const int lane = e & 31;
+                const int h = lane >> 4;
+                const int idx = (e >> 5) * 16 + (lane & 15);
+                const int pol = p0 + idx / C;
+                const int k = idx % C;
+                for (int hb = 0; hb < TB / 16; hb++) {
+                    const int tl0 = hb * 16 + h * 8;
+                    flush_row<8, NPOL, C, CS>(args, stage + ((pol - sp0) * TB + tl0) * CS + k, sb, ant, pol, k,
+                                              row_dst(pol, k) + tl0);
+                }
+            }
+        } else {
+            for (int e = tid; e < np * C; e += P::NTHREADS) {
+                const int pol = p0 + e / C;
+                const int k = e % C;
+                flush_row<TB, NPOL, C, CS>(args, stage + ((pol - sp0) * TB) * CS + k, sb, ant, pol, k,
+                                           row_dst(pol, k));
+            }
         }
     };
 
@@ -495,36 +530,25 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
                                   (((size_t)sb * nsig + sig) * args.T + tc) * C + j;
                     if (tc < args.T) out[r * KSTEP] = y;
                 } else {
-                    stage[(pol * TB + tl) * CS + j + r * KSTEP] = __floats2half2_rn(y.x, y.y);
+                    stage[((PERPOL ? 0 : pol) * TB + tl) * CS + j + r * KSTEP] = __floats2half2_rn(y.x, y.y);
                 }
             }
         }
         slot_sync<NT>(slot);   // buf / rtab / inb are reused by the next item
+        if constexpr (PERPOL) {
+            if (tl == TB - 1) {       // this polarisation's FFTs are staged (the CTA is one slot)
+                flush_pols(pol, 1, pol);
+                slot_sync<NT>(slot);  // the next polarisation reuses the stage
+            }
+        }
     }
 
-    if constexpr (MODE == kSpecF16) {
-        __half* spec = reinterpret_cast<__half*>(args.spec);
-        auto row_dst = [&](int pol, int k) {
-            return spec + (((size_t)sb * C + k) * args.rows + 2 * (ant * NPOL + pol)) * (size_t)args.T + tb0;
-        };
+    if constexpr (MODE == kSpecF16 && !PERPOL) {
         if constexpr (TB >= 16) {
-            // whole 32-byte row segments, written by lane pairs: lanes l and l + 16 of a warp
-            // take the first and second 8 FFTs of the same (polarisation, channel), so each
-            // store instruction covers 16 full sectors (the CTA's 16 FFTs of a row are only
-            // all staged after a CTA-wide barrier; one slot needs none)
+            // whole row segments by lane pairs; the CTA's 16 FFTs of a row are all staged only
+            // after a CTA-wide barrier (one slot needs none)
             if constexpr (P::NSLOT > 1) __syncthreads();
-            for (int e = tid; e < 2 * NPOL * C; e += P::NTHREADS) {
-                const int lane = e & 31;
-                const int h = lane >> 4;
-                const int idx = (e >> 5) * 16 + (lane & 15);
-                const int pol = idx / C;
-                const int k = idx - pol * C;
-                for (int hb = 0; hb < TB / 16; hb++) {   // 16-FFT segments of the row
-                    const int tl0 = hb * 16 + h * 8;
-                    flush_row<8, NPOL, C, CS>(args, stage + (pol * TB + tl0) * CS + k, sb, ant, pol, k,
-                                              row_dst(pol, k) + tl0);
-                }
-            }
+            flush_pols(0, NPOL, 0);
         } else if constexpr (SEG >= 4) {
             // flush of this slot's rows: FFTs [tl0, tl0 + NR) of NPS polarisations (the slot's
             // last slot_sync made its stage entries visible to all its threads)
@@ -540,12 +564,7 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
             }
         } else {
             __syncthreads();
-            // flush: one (pol, channel) per thread -> Re row and Im row, TB halves each
-            for (int e = tid; e < NPOL * C; e += P::NTHREADS) {
-                const int pol = e / C;
-                const int k = e - pol * C;
-                flush_row<TB, NPOL, C, CS>(args, stage + (pol * TB) * CS + k, sb, ant, pol, k, row_dst(pol, k));
-            }
+            flush_pols(0, NPOL, 0);   // one (pol, channel) per thread, TB FFTs each
         }
     }
 }
@@ -607,7 +626,8 @@ size_t fstage_smem(int mode, int tb, int npol)
     s += (size_t)P::NSLOT * P::NROT * sizeof(float2);
     s += (size_t)(P::FS + P::FST) * sizeof(float);
     s += (size_t)P::NSLOT * (npol == 2 ? fstage_inb<F, 2, CPX>() : fstage_inb<F, 1, CPX>());
-    if (mode == kSpecF16) s += (size_t)npol * tb * (P::C + 2) * sizeof(__half2);
+    // F16 stage: [npol][tb][C + 2] half2, one polarisation at a time when the CTA is one slot
+    if (mode == kSpecF16) s += (size_t)(P::NSLOT == 1 ? 1 : npol) * tb * (P::C + 2) * sizeof(__half2);
     return s;
 }
 
@@ -653,6 +673,14 @@ int fstage_tb(int mode, const FArgs& a)
     if (mode == kSpecF16) {
         const size_t lim = smem_optin_limit();
         while (tb > 4 && fstage_smem<F, CPX>(mode, tb, a.npol) > lim) tb /= 2;
+        // where the registers allow two CTAs per SM, keep the staging small enough for two
+        // (their latency hiding outweighs longer row segments)
+        if (FPlan<F>::MINB >= 2) {
+            const size_t half = smem_per_sm_limit() / 2 - 1024;   // 1 KB reserved per CTA
+            int t2 = tb;
+            while (t2 > 4 && fstage_smem<F, CPX>(mode, t2, a.npol) > half) t2 /= 2;
+            if (fstage_smem<F, CPX>(mode, t2, a.npol) <= half) tb = t2;
+        }
     }
     return tb;
 }
