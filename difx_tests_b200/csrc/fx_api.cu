@@ -523,6 +523,7 @@ FArgs ctx_fargs(fxc_ctx* x, const uint8_t* d_data, size_t pitch, int ld)
     a.T = x->T;
     a.tb = x->plan_tb;
     a.cpx = x->cfg.iscomplex;
+    a.err = x->d_err;
     return a;
 }
 

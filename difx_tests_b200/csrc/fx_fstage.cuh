@@ -133,6 +133,60 @@ __device__ __forceinline__ void slot_sync(int slot)
     }
 }
 
+// ---- input staging by the bulk-copy (TMA) engine: one cp.async.bulk per FFT into the
+// slot's staging buffer, completing an mbarrier phase; every wait is bounded by time.
+__device__ __forceinline__ uint32_t smem_u32a(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ unsigned long long gtimer()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void stg_bar_init(uint64_t* bar)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32a(bar)) : "memory");
+}
+
+// Copy `bytes` (16-byte multiple, both addresses 16-byte aligned) from global src to shared dst.
+// The issuing thread orders the slot's earlier reads of dst (made visible to it by a barrier)
+// before the async-proxy write.
+__device__ __forceinline__ void stg_issue(uint64_t* bar, void* dst, const void* src, uint32_t bytes)
+{
+    size_t gsrc;
+    asm volatile("cvta.to.global.u64 %0, %1;" : "=l"(gsrc) : "l"(src));
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32a(bar)), "r"(bytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_u32a(dst)), "l"(gsrc), "r"(bytes), "r"(smem_u32a(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ bool stg_try(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32a(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// true when the phase completed, false after 1 s
+__device__ __forceinline__ bool stg_wait(uint64_t* bar, uint32_t parity)
+{
+    if (stg_try(bar, parity)) return true;
+    const unsigned long long t0 = gtimer();
+    while (!stg_try(bar, parity))
+        if (gtimer() - t0 > 1000000000ull) return false;
+    return true;
+}
+
 // Twiddles a thread needs for pass PASS (r = 0..R-1 of each of its NB butterflies).
 template <int F, int PASS>
 struct PassTw {
@@ -291,9 +345,18 @@ using Tw2Of = PassTw<F, (FPlan<F>::NPASS > 2 ? 2 : 1)>;
 // One F-stage block: TB consecutive FFTs x NPOL of antenna `ant`, subband `sb`,
 // starting at chunk slot tb0.  Shared by the single-job grid (k_fstage) and the
 // persistent multi-job kernel (k_fstage_batch).
+// The slots' staging mbarriers: 16 bytes per slot after the channel table.
+template <int F, bool CPX>
+__device__ __forceinline__ uint64_t* fstage_bars(unsigned char* smem)
+{
+    using P = FPlan<F, CPX>;
+    float2* rtabs = reinterpret_cast<float2*>(smem) + P::NSLOT * P::BUF + (P::TWREG ? 0 : P::TWQ);
+    return reinterpret_cast<uint64_t*>(reinterpret_cast<float*>(rtabs + P::NSLOT * P::NROT) + P::FS + P::FST);
+}
+
 template <int F, int MODE, int TB, int NPOL, bool CPX>
 __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant, int tb0, unsigned char* smem,
-                                             const PassTw<F, 1>& tw1, const Tw2Of<F>& tw2)
+                                             const PassTw<F, 1>& tw1, const Tw2Of<F>& tw2, uint32_t& phase)
 {
     using P = FPlan<F, CPX>;
     constexpr int NT = P::NT;
@@ -303,7 +366,8 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
     float2* tq = bufs + P::NSLOT * P::BUF;                              // [TWQ]
     float2* rtabs = tq + (P::TWREG ? 0 : P::TWQ);                      // [NSLOT][NROT]
     float* ctab = reinterpret_cast<float*>(rtabs + P::NSLOT * P::NROT);     // [FS + FST] channel freqs
-    uint8_t* inbs = reinterpret_cast<uint8_t*>(ctab + P::FS + P::FST);      // [NSLOT][INB]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(ctab + P::FS + P::FST);    // [NSLOT] (16 B each)
+    uint8_t* inbs = reinterpret_cast<uint8_t*>(bars + 2 * P::NSLOT);        // [NSLOT][INB]
     // [NPOL][TB][CS]: rows padded by 2 half2, so paired flush lanes 8 FFTs apart read other banks
     constexpr int CS = C + 2;
     __half2* stage = reinterpret_cast<__half2*>(inbs + P::NSLOT * INB);
@@ -317,6 +381,7 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
     float2* buf = bufs + slot * P::BUF;
     float2* rtab = rtabs + slot * P::NROT;
     uint8_t* inb = inbs + slot * INB;
+    uint64_t* bar = bars + 2 * slot;
 
     const double lo = args.sb_lo[sb];
     const double lofrac = dsub(lo, trunc(lo));
@@ -331,9 +396,10 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
     constexpr int NITEM = TB * NPOL;
     const DelayEntry* dtab = args.dtab + (size_t)ant * args.ld + args.t_base;
 
-    // Input window of an item: 16-byte aligned start.  2-bit real (kernel.c:402-409):
-    // one 128-bit vector per thread at most (F*NPOL/4 + 16 <= 16*NT), prefetched into a
-    // register one item ahead; 8-bit complex: 2*NPOL vectors per thread, loaded per item.
+    // Input window of an item: 16-byte aligned start, nvec 16-byte vectors (2-bit real:
+    // F*NPOL/4 bytes + the read-ahead byte of kernel.c:402-409; 8-bit complex: 2*NPOL bytes
+    // per sample), copied into the slot's staging buffer by one bulk copy, issued as soon
+    // as the previous item's bytes are decoded so the copy overlaps that item's FFT.
     auto window = [&](const DelayEntry& d, int& base, int& nvec) {
         if constexpr (CPX) {
             const int first = d.offset * 2 * NPOL;
@@ -384,19 +450,19 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
     constexpr int SEG = (NITEM >= P::NSLOT) ? NITEM / P::NSLOT : 1;
     const int item_end = min(slot * SEG + SEG, NITEM);
 
-    // prefetch of the first item's delay entry and input vector
+    // the first item's delay entry and input copy
     int item = slot * SEG;
     DelayEntry dn;
     bool vn = false;
     int basen = 0, nvecn = 0;
-    uint4 pf = make_uint4(0, 0, 0, 0);
+    bool expired = false;   // a staging wait gave up (recorded in *args.err)
     if (item < item_end && tb0 + item % TB < args.nfft) {
         dn = dtab[tb0 + item % TB];
         vn = dn.valid != 0;
     }
     if (vn) {
         window(dn, basen, nvecn);
-        if (!CPX && t < nvecn) pf = __ldg(reinterpret_cast<const uint4*>(row + basen) + t);
+        if (t == 0) stg_issue(bar, inb, row + basen, 16u * nvecn);
     }
 
     for (; item < item_end; item++) {
@@ -406,14 +472,14 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
         const DelayEntry d = dn;
         const bool valid = vn;
         const int base_byte = basen;
-        if constexpr (CPX) {
-            if (valid)
-                for (int i = t; i < nvecn; i += NT)
-                    reinterpret_cast<uint4*>(inb)[i] = __ldg(reinterpret_cast<const uint4*>(row + base_byte) + i);
-        } else {
-            if (valid && t < nvecn) reinterpret_cast<uint4*>(inb)[t] = pf;
+        if (valid) {
+            if (!stg_wait(bar, phase)) {
+                if (t == 0 && args.err) atomicCAS(args.err, 0, 6);
+                expired = true;
+            }
+            phase ^= 1;
         }
-        // ---- prefetch the next item of this slot
+        // ---- the next item of this slot: delay entry now, its copy after this item's decode
         {
             const int ni = item + 1;
             vn = false;
@@ -421,10 +487,7 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
                 dn = dtab[tb0 + ni % TB];
                 vn = dn.valid != 0;
             }
-            if (vn) {
-                window(dn, basen, nvecn);
-                if (!CPX && t < nvecn) pf = __ldg(reinterpret_cast<const uint4*>(row + basen) + t);
-            }
+            if (vn) window(dn, basen, nvecn);
         }
         // ---- rotator tables for this FFT (per slot)
         for (int e = t; e < P::NROT; e += NT)
@@ -480,6 +543,8 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
         dft<16>(v);
         pass_store<F, 0>(buf, v, t);
         slot_sync<NT>(slot);
+        // this item's bytes are decoded: the next item's copy overlaps the rest of its FFT
+        if (vn && t == 0) stg_issue(bar, inb, row + basen, 16u * nvecn);
 
         // ---- middle passes
         if constexpr (P::NPASS > 2) {
@@ -542,6 +607,9 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
             }
         }
     }
+    // after an expired wait the copy may still land: wait for it once more (bounded) so it
+    // cannot write into the staging buffer of a later task or an exited CTA
+    if (expired) stg_wait(bar, phase ^ 1);
 
     if constexpr (MODE == kSpecF16 && !PERPOL) {
         if constexpr (TB >= 16) {
@@ -586,6 +654,18 @@ __device__ __forceinline__ void fstage_prologue(unsigned char* smem, PassTw<F, 1
     }
 }
 
+// One staging mbarrier per FFT slot, initialised by the slot's first thread before the
+// block's first barrier (fstage_block's channel-table __syncthreads) orders it before use.
+template <int F, bool CPX>
+__device__ __forceinline__ void fstage_bars_init(unsigned char* smem)
+{
+    using P = FPlan<F, CPX>;
+    if (threadIdx.x % P::NT == 0) {
+        stg_bar_init(fstage_bars<F, CPX>(smem) + 2 * (threadIdx.x / P::NT));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+}
+
 // Single job: grid (T / TB, nant, nsb).
 template <int F, int MODE, int TB, int NPOL, bool CPX>
 __global__ void __launch_bounds__(FPlan<F>::NTHREADS, FPlan<F>::MINB)
@@ -595,7 +675,9 @@ k_fstage(FArgs args)
     PassTw<F, 1> tw1;
     Tw2Of<F> tw2;
     fstage_prologue<F>(smem, tw1, tw2);
-    fstage_block<F, MODE, TB, NPOL, CPX>(args, blockIdx.z, blockIdx.y, blockIdx.x * TB, smem, tw1, tw2);
+    fstage_bars_init<F, CPX>(smem);
+    uint32_t phase = 0;
+    fstage_block<F, MODE, TB, NPOL, CPX>(args, blockIdx.z, blockIdx.y, blockIdx.x * TB, smem, tw1, tw2, phase);
 }
 
 // Many jobs in one persistent launch: CTAs stride over a task table
@@ -609,10 +691,12 @@ k_fstage_batch(const FArgs* __restrict__ jobs, const int4* __restrict__ tasks, i
     PassTw<F, 1> tw1;
     Tw2Of<F> tw2;
     fstage_prologue<F>(smem, tw1, tw2);
+    fstage_bars_init<F, false>(smem);
+    uint32_t phase = 0;
     for (int i = blockIdx.x; i < ntask; i += gridDim.x) {
         const int4 tk = tasks[i];
         const FArgs a = jobs[tk.x];
-        fstage_block<F, MODE, TB, NPOL, false>(a, tk.y, tk.z, tk.w, smem, tw1, tw2);
+        fstage_block<F, MODE, TB, NPOL, false>(a, tk.y, tk.z, tk.w, smem, tw1, tw2, phase);
         __syncthreads();   // the next task rewrites the channel table and staging buffers
     }
 }
@@ -625,6 +709,7 @@ size_t fstage_smem(int mode, int tb, int npol)
     if (!P::TWREG) s += (size_t)P::TWQ * sizeof(float2);
     s += (size_t)P::NSLOT * P::NROT * sizeof(float2);
     s += (size_t)(P::FS + P::FST) * sizeof(float);
+    s += (size_t)P::NSLOT * 16;   // staging mbarriers
     s += (size_t)P::NSLOT * (npol == 2 ? fstage_inb<F, 2, CPX>() : fstage_inb<F, 1, CPX>());
     // F16 stage: [npol][tb][C + 2] half2, one polarisation at a time when the CTA is one slot
     if (mode == kSpecF16) s += (size_t)(P::NSLOT == 1 ? 1 : npol) * tb * (P::C + 2) * sizeof(__half2);

@@ -60,6 +60,7 @@ struct FArgs {
     unsigned* amax;             // F16 layout, FP8 form: running absmax per (sb*nchan + chan, sig), or null
     int tspan;                  // slots [0, tspan) written (>= nfft, multiple of 64; 0 = T)
     int cpx;                    // input format: 0 = 2-bit real, 1 = 8-bit complex (FFT length nchan)
+    int* err;                   // device error word (code 6: an input staging wait expired), or null
 };
 
 

@@ -243,8 +243,9 @@ const char* fxc_strerror(int status);
 /* Last CUDA error code seen by this thread's calls (cudaError_t as int). */
 int fxc_last_cuda_error(void);
 /* Which device-side wait expired when a call returned FXC_ERR_TIMEOUT on this
- * thread: 1 stage load, 2 stage release, 3 accumulator release, 4 accumulator
- * ready, 5 drain at exit; 0 if none. */
+ * thread: tensor-core X stage 1 stage load, 2 stage release, 3 accumulator release,
+ * 4 accumulator ready, 5 drain at exit; F stage 6 input staging copy; 0 if none.
+ * (16 after FXC_ERR_INVALID: an FFT's input was outside its window.) */
 int fxc_last_device_error(void);
 
 /* ---- inspection entry points (parity tests; not needed for correlation) ---- */
