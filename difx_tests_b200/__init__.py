@@ -106,6 +106,7 @@ SIGNATURES = {
     "fxc_debug_delay_table": (_I, [_P, _DP, _DP, _I, _I, _IP, _IP, _DP, _DP, _DP]),
     "fxc_debug_unpack": (_I, [_P, _DP, _DP, _I, _I, _FP]),
     "fxc_debug_spectra": (_I, [_P, _DP, _DP, _I, _I, _FP]),
+    "fxc_debug_expire_wait": (_I, [_P]),
 }
 
 

@@ -108,5 +108,23 @@ cudaError_t launch_unpack_debug(int nchan, const FArgs& a, float* out, cudaStrea
     return cudaGetLastError();
 }
 
+// Failure-path check: the F stage's bounded staging wait on an mbarrier that nothing
+// completes (no copy is ever issued, so nothing is left in flight) runs out after 1 s and
+// records code 6 in the error word, as an expired input copy would.
+__global__ void k_expire_wait(int* err)
+{
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        stg_bar_init(&bar);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        if (!stg_wait(&bar, 0)) atomicCAS(err, 0, 6);
+    }
+}
+
+cudaError_t launch_expire_wait(int* err, cudaStream_t st)
+{
+    k_expire_wait<<<1, 32, 0, st>>>(err);
+    return cudaGetLastError();
+}
 
 }  // namespace fx

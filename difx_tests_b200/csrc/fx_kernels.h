@@ -36,5 +36,7 @@ cudaError_t launch_cast_fp8(const void* spec16, const unsigned* amax, int rows, 
 cudaError_t launch_xtc8(const XArgs& a, int* d_err, int nsm, cudaStream_t st);
 size_t xtc_smem_bytes();
 cudaError_t launch_unpack_debug(int nchan, const FArgs& a, float* out, cudaStream_t st);
+// a bounded device wait that runs out (error word code 6), for tests of the failure path
+cudaError_t launch_expire_wait(int* err, cudaStream_t st);
 
 }  // namespace fx

@@ -268,6 +268,12 @@ int fxc_debug_unpack(fxc_ctx* ctx, const double* delays, const double* fileoffse
 int fxc_debug_spectra(fxc_ctx* ctx, const double* delays, const double* fileoffsets, int first_fft, int nfft,
                       float* out);
 
+/* Launches a kernel whose bounded device wait (the F stage's input-staging wait, on a
+ * barrier that nothing completes) runs out after about 1 s; the next synchronising call
+ * returns FXC_ERR_TIMEOUT and fxc_last_device_error() gives 6.  Exercises the failure
+ * path of the device waits without faulting the GPU; the context stays usable. */
+int fxc_debug_expire_wait(fxc_ctx* ctx);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

@@ -401,3 +401,22 @@ def test_tc_long_ffts_dual_pol(nant, npol, nchan, xmode):
         bound = fp8_error_bound(job, 0, 128)
         slack = 1e-5 * np.abs(ref).max(axis=-1, keepdims=True)
         assert (np.abs(vis[0] - ref) <= 1.01 * bound + slack).all()
+
+
+def test_expired_device_wait_is_reported_and_context_survives():
+    """A bounded device wait that runs out (on a barrier nothing completes) comes back as
+    FXC_ERR_TIMEOUT with its code; the next correlation on the same context is correct."""
+    import ctypes as C
+    job = synth.make_job(nant=4, npol=1, nchan=256, numffts=64, bw=64e6, lo=1.4e9, rho=0.1, seed=91)
+    with corr_for(job) as c:
+        assert fx.lib().fxc_debug_expire_wait(C.c_void_p(c.handle.value)) == fx.FXC_OK
+        with pytest.raises(fx.FxcError) as e:
+            c.synchronize()
+        assert e.value.status == fx.FXC_ERR_TIMEOUT
+        assert fx.lib().fxc_last_device_error() == 6
+        c.reset()
+        c.process(job.data, job.delays, job.fileoffsets)
+        vis, counts = c.visibilities()
+    ref, rc = oracle_vis(job)
+    np.testing.assert_array_equal(counts, rc)
+    assert_vis_close(vis[0], ref)
