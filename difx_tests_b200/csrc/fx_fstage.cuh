@@ -351,7 +351,7 @@ __device__ __forceinline__ uint64_t* fstage_bars(unsigned char* smem)
 {
     using P = FPlan<F, CPX>;
     float2* rtabs = reinterpret_cast<float2*>(smem) + P::NSLOT * P::BUF + (P::TWREG ? 0 : P::TWQ);
-    return reinterpret_cast<uint64_t*>(reinterpret_cast<float*>(rtabs + P::NSLOT * P::NROT) + P::FS + P::FST);
+    return reinterpret_cast<uint64_t*>(reinterpret_cast<float*>(rtabs + 2 * P::NSLOT * P::NROT) + P::FS + P::FST);
 }
 
 template <int F, int MODE, int TB, int NPOL, bool CPX>
@@ -364,8 +364,8 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
     constexpr int INB = fstage_inb<F, NPOL, CPX>();                    // staged bytes per slot
     float2* bufs = reinterpret_cast<float2*>(smem);                   // [NSLOT][BUF]
     float2* tq = bufs + P::NSLOT * P::BUF;                              // [TWQ]
-    float2* rtabs = tq + (P::TWREG ? 0 : P::TWQ);                      // [NSLOT][NROT]
-    float* ctab = reinterpret_cast<float*>(rtabs + P::NSLOT * P::NROT);     // [FS + FST] channel freqs
+    float2* rtabs = tq + (P::TWREG ? 0 : P::TWQ);                      // [NSLOT][2][NROT]
+    float* ctab = reinterpret_cast<float*>(rtabs + 2 * P::NSLOT * P::NROT);   // [FS + FST] channel freqs
     uint64_t* bars = reinterpret_cast<uint64_t*>(ctab + P::FS + P::FST);    // [NSLOT] (16 B each)
     uint8_t* inbs = reinterpret_cast<uint8_t*>(bars + 2 * P::NSLOT);        // [NSLOT][INB]
     // [NPOL][TB][CS]: rows padded by 2 half2, so paired flush lanes 8 FFTs apart read other banks
@@ -379,7 +379,9 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
     const int slot = tid / NT;
     const int t = tid - slot * NT;
     float2* buf = bufs + slot * P::BUF;
-    float2* rtab = rtabs + slot * P::NROT;
+    // rotator tables alternate between two buffers per slot, so the next FFT's table can be
+    // written while this FFT's epilogue still reads its own: no barrier between FFTs
+    float2* rtab2 = rtabs + slot * 2 * P::NROT;
     uint8_t* inb = inbs + slot * INB;
     uint64_t* bar = bars + 2 * slot;
 
@@ -469,6 +471,7 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
         const int pol = item / TB;
         const int tl = item - pol * TB;
         const int tc = tb0 + tl;                    // FFT slot within the chunk
+        float2* rtab = rtab2 + ((item - slot * SEG) & 1) * P::NROT;
         const DelayEntry d = dn;
         const bool valid = vn;
         const int base_byte = basen;
@@ -599,9 +602,11 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
                 }
             }
         }
-        slot_sync<NT>(slot);   // buf / rtab / inb are reused by the next item
+        // no barrier here: the next FFT writes the other rotator table before its first barrier,
+        // and buf only after it (the staging buffer's copy was issued after this FFT's decode)
         if constexpr (PERPOL) {
             if (tl == TB - 1) {       // this polarisation's FFTs are staged (the CTA is one slot)
+                slot_sync<NT>(slot);
                 flush_pols(pol, 1, pol);
                 slot_sync<NT>(slot);  // the next polarisation reuses the stage
             }
@@ -614,12 +619,13 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
     if constexpr (MODE == kSpecF16 && !PERPOL) {
         if constexpr (TB >= 16) {
             // whole row segments by lane pairs; the CTA's 16 FFTs of a row are all staged only
-            // after a CTA-wide barrier (one slot needs none)
-            if constexpr (P::NSLOT > 1) __syncthreads();
+            // after a CTA-wide barrier
+            __syncthreads();
             flush_pols(0, NPOL, 0);
         } else if constexpr (SEG >= 4) {
-            // flush of this slot's rows: FFTs [tl0, tl0 + NR) of NPS polarisations (the slot's
-            // last slot_sync made its stage entries visible to all its threads)
+            // flush of this slot's rows: FFTs [tl0, tl0 + NR) of NPS polarisations, once the
+            // slot's stage entries are visible to all its threads
+            slot_sync<NT>(slot);
             constexpr int NR = SEG < TB ? SEG : TB;
             constexpr int NPS = SEG / NR;
             const int pol0 = (slot * SEG) / TB;
@@ -707,7 +713,7 @@ size_t fstage_smem(int mode, int tb, int npol)
     using P = FPlan<F, CPX>;
     size_t s = (size_t)P::NSLOT * P::BUF * sizeof(float2);
     if (!P::TWREG) s += (size_t)P::TWQ * sizeof(float2);
-    s += (size_t)P::NSLOT * P::NROT * sizeof(float2);
+    s += (size_t)2 * P::NSLOT * P::NROT * sizeof(float2);
     s += (size_t)(P::FS + P::FST) * sizeof(float);
     s += (size_t)P::NSLOT * 16;   // staging mbarriers
     s += (size_t)P::NSLOT * (npol == 2 ? fstage_inb<F, 2, CPX>() : fstage_inb<F, 1, CPX>());
