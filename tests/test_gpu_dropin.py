@@ -72,3 +72,71 @@ def test_fxcorr_main_matches_reference_cli(tmp_path):
     ref = run_in(tmp, REF_CLI, "ref")
     got = run_in(tmp, FX_CLI, "fx", args=("test.conf",))
     compare(got, ref, nbl=10)
+
+
+def read_visbin(path, nrec):
+    """The -b dump: per subintegration int32 {nsubband, nbl+nant, npol*npol, nchan}, int32 counts,
+    complex64 visibilities."""
+    raw = open(path, "rb").read()
+    out, pos = [], 0
+    for _ in range(nrec):
+        nsb, nrow, np2, nchan = np.frombuffer(raw, np.int32, 4, pos)
+        pos += 16
+        counts = np.frombuffer(raw, np.int32, nrow, pos)
+        pos += 4 * nrow
+        n = nsb * nrow * np2 * nchan
+        vis = np.frombuffer(raw, np.complex64, n, pos).reshape(nsb, nrow, np2, nchan)
+        pos += 8 * n
+        out.append((counts, vis))
+    assert pos == len(raw)
+    return out
+
+
+@pytest.mark.parametrize("xmode", ["plain", "tc"])
+def test_fxcorr_main_streams_subintegrations_of_several_subbands(tmp_path, xmode):
+    """NSUBINT successive subintegrations of NSUBBAND per-antenna streams: subintegration s is
+    FFTs s*NUMFFTS.. of each stream with the delay polynomial shifted to its first FFT, and must
+    equal a one-subintegration correlation of that byte range with the shifted polynomial."""
+    import dataclasses
+
+    import difx_tests_b200 as fx
+
+    nsub, nsb, numffts, nchan, nant = 3, 2, 40, 256, 4
+    big = synth.random_job(nant=nant, npol=2, nchan=nchan, numffts=nsub * numffts, nsubband=nsb, seed=21)
+    job = dataclasses.replace(big, numffts=numffts)
+    names = []
+    for a in range(nant):
+        for sb in range(nsb):
+            big.data[sb, a].tofile(tmp_path / f"ant{a}_sb{sb}.bin")
+        names.append(f"ant{a}_sb%d.bin")
+    synth.write_conf(tmp_path / "s.conf", job, names)
+    with open(tmp_path / "s.conf", "a") as f:
+        f.write(f"NSUBBAND {nsb}\nNSUBINT {nsub}\n")
+    r = subprocess.run([FX_CLI, "s.conf", "-x", xmode, "-b", "vis.bin"], cwd=tmp_path, capture_output=True,
+                       text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    recs = read_visbin(tmp_path / "vis.bin", nsub)
+    for s in range(nsub):
+        for sb in range(nsb):
+            assert os.path.exists(tmp_path / f"vis.out.{s}.sb{sb}")
+
+    F = 2 * nchan
+    stride = numffts * F * 2 * 2 // 8                 # NUMFFTS FFTs of 2-bit, 2-pol samples
+    sbb = synth.subint_bytes(nchan, numffts, 2)
+    xm = fx.FXC_X_PLAIN_FP32 if xmode == "plain" else fx.FXC_X_TC_FP16
+    cfg = fx.make_config(nant, nchan, numffts, job.bw, job.lo, npol=2, nsubband=nsb, xmode=xm)
+    for s in range(nsub):
+        k0 = float(s * numffts)
+        d = np.array(job.delays, np.float64).copy()
+        if s:
+            for a in range(nant):
+                q, l, c0 = job.delays[a]
+                d[a] = (q, l + 2.0 * q * k0, c0 + l * k0 + q * k0 * k0)
+        with fx.Correlator(cfg) as c:
+            c.process(np.ascontiguousarray(big.data[:, :, s * stride:s * stride + sbb]), d, job.fileoffsets)
+            vis, counts = c.visibilities(normalize=True)
+        got_counts, got = recs[s]
+        np.testing.assert_array_equal(got_counts, counts)
+        want = np.asarray(vis).reshape(got.shape)
+        scale = np.abs(want).max()
+        np.testing.assert_allclose(got, want, rtol=0, atol=1e-6 * scale)

@@ -51,3 +51,23 @@ def test_short_file_is_an_error(tmp_path):
 def test_usage(tmp_path):
     r = run(tmp_path, "-q")
     assert r.returncode == 1 and "usage" in r.stderr
+
+
+def test_subband_file_pattern_needs_one_int_conversion(tmp_path):
+    job = synth.random_job(nant=2, npol=2, nchan=256, numffts=8, seed=3)
+    synth.write_conf(tmp_path / "t.conf", job, ["x0.bin", "x%s.bin"])
+    with open(tmp_path / "t.conf", "a") as f:
+        f.write("NSUBBAND 2\n")
+    r = run(tmp_path, "t.conf")
+    assert r.returncode == 1 and "needs one %d" in r.stderr
+
+
+def test_missing_subband_stream_is_an_error(tmp_path):
+    job = synth.random_job(nant=2, npol=2, nchan=256, numffts=8, seed=4)
+    synth.write_conf(tmp_path / "t.conf", job, ["x0_%d.bin", "x1_%d.bin"])
+    with open(tmp_path / "t.conf", "a") as f:
+        f.write("NSUBBAND 2\nNSUBINT 2\n")
+    for a in range(2):
+        job.data[0, a].tofile(tmp_path / f"x{a}_0.bin")
+    r = run(tmp_path, "t.conf", "-s", "3")
+    assert r.returncode == 1 and "x0_1.bin" in r.stderr
