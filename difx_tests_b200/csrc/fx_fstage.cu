@@ -1,5 +1,8 @@
 // fx_fstage.cu -- dispatch of the fused F stage by FFT length (kernels in
 // fx_fstage.cuh, one translation unit per length) and the debug unpack export.
+#include <cstdlib>
+#include <cstring>
+
 #include "fx_fstage.cuh"
 
 namespace fx {
@@ -29,8 +32,17 @@ cudaError_t launch_fstage_batch_8192(int mode, int npol, int tb, const FArgs* d_
                                   cudaStream_t st);
 size_t fstage_smem_8192(int mode, int tb, int npol);
 
+// The F16 layout's F stage runs on the tensor cores where that kernel covers the geometry;
+// FXC_TC_FSTAGE=fft selects the FP32 FFT kernel instead (the two agree within FP16 rounding).
+static bool ftc_wanted()
+{
+    const char* v = std::getenv("FXC_TC_FSTAGE");
+    return !(v && std::strcmp(v, "fft") == 0);
+}
+
 cudaError_t launch_fstage(int nchan, int mode, const FArgs& a, cudaStream_t st)
 {
+    if (ftc_supported(nchan, mode, a) && ftc_wanted()) return launch_ftc(a, st);
     switch (a.cpx ? nchan : 2 * nchan) {   // FFT length: complex samples fill every bin
     case 256: return launch_fstage_256(mode, a, st);
     case 512: return launch_fstage_512(mode, a, st);

@@ -21,6 +21,9 @@ cudaError_t launch_counts(const uint32_t* vbits, int nant, int nwords, int* coun
 cudaError_t launch_finalize(const float2* acc, int acc_layout, int nsig, int npol, int nant, int nchan, int nsb,
                             const int* counts, int normalize, float2* vis, cudaStream_t st);
 cudaError_t launch_fstage(int nchan, int mode, const FArgs& a, cudaStream_t st);
+// tensor-core F stage (F16 layout, 2048-point FFTs of one polarisation of 2-bit real input)
+bool ftc_supported(int nchan, int mode, const FArgs& a);
+cudaError_t launch_ftc(const FArgs& a, cudaStream_t st);
 size_t fstage_smem_bytes(int nchan, int mode, int npol, int tb);
 cudaError_t launch_fstage_batch(int nchan, int npol, int mode, int tb, const FArgs* d_jobs, const int4* d_tasks,
                                 int ntask, cudaStream_t st);

@@ -34,6 +34,7 @@
 
 #include "fx_common.cuh"
 #include "fx_kernels.h"
+#include "fx_tc.cuh"
 
 namespace fx {
 
@@ -46,7 +47,7 @@ constexpr int NSTAGE_MB = 6;               // multi-block Gram: 6 x 32 KB
 constexpr int STAGE_BYTES = BM * ROWB;     // 16 KB
 constexpr int NTHREADS = 192;              // 6 warps
 constexpr int TMEM_COLS = 256;             // two 128-column FP32 accumulators
-constexpr unsigned long long WAIT_NS = 1000000000ull;   // 1 s per wait
+constexpr uint32_t kIdesc = idesc_f16(128, 128);
 
 // NST stages of SLOTS 16-KB tiles (one tile: the single-block Gram; two: tiles I and J of a
 // block pair of a multi-block Gram)
@@ -61,124 +62,6 @@ struct Smem {
     uint32_t tmem_base;
     int abort;
 };
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ unsigned long long globaltimer()
-{
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
-    return t;
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t* b)
-{
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity)
-{
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(b)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// Bounded wait: true when the phase completed, false after WAIT_NS or on abort.
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag)
-{
-    if (mbar_try(b, parity)) return true;
-    const unsigned long long t0 = globaltimer();
-    while (true) {
-        if (mbar_try(b, parity)) return true;
-        if (*abort_flag) return false;
-        if (globaltimer() - t0 > WAIT_NS) return false;
-    }
-}
-
-__device__ __forceinline__ void tma_load_2d(const CUtensorMap* map, uint64_t* bar, void* dst, int x, int y)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
-        ::"r"(smem_u32(dst)), "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y)
-        : "memory");
-}
-
-// UMMA shared-memory descriptor: K-major, SWIZZLE_128B, 8-row groups 1024 B apart.
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr)
-{
-    uint64_t d = 0;
-    d |= (uint64_t)((saddr >> 4) & 0x3FFF);   // start address
-    d |= (uint64_t)1 << 16;                   // leading byte offset (unused for swizzled K-major)
-    d |= (uint64_t)(1024 >> 4) << 32;         // stride byte offset
-    d |= (uint64_t)1 << 46;                   // descriptor version (sm100)
-    d |= (uint64_t)2 << 61;                   // SWIZZLE_128B
-    return d;
-}
-
-// Instruction descriptor, kind::f16: D F32, A/B F16, both K-major, M=128, N=128.
-constexpr uint32_t kIdesc = (1u << 4) | (0u << 7) | (0u << 10) | ((uint32_t)(128 >> 3) << 17) |
-                            ((uint32_t)(128 >> 4) << 24);
-
-// kind::f8f6f4 with A and B both E4M3 (format code 0) uses the same descriptor bits.
-template <bool F8>
-__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t accumulate)
-{
-    if constexpr (F8) {
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "setp.ne.b32 p, %4, 0;\n\t"
-            "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}"
-            ::"r"(tmem_d), "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate)
-            : "memory");
-    } else {
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "setp.ne.b32 p, %4, 0;\n\t"
-            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-            ::"r"(tmem_d), "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate)
-            : "memory");
-    }
-}
-
-__device__ __forceinline__ void umma_commit(uint64_t* bar)
-{
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-                 : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t* r)
-{
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-        : "r"(taddr));
-}
-
-__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
 }  // namespace tc
 
@@ -233,10 +116,7 @@ k_xtc(const __grid_constant__ CUtensorMap tmap, XArgs a, int* err)
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sm.tmem_base)),
-                     "r"(TMEM_COLS)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        tmem_alloc(&sm.tmem_base, TMEM_COLS);
     }
     __syncthreads();
     tc_fence_after();
@@ -318,7 +198,7 @@ k_xtc(const __grid_constant__ CUtensorMap tmap, XArgs a, int* err)
                     const uint32_t sb = (MB && I != J) ? smem_u32(sm.stage[stage][MB ? 1 : 0]) : sa;
 #pragma unroll
                     for (int k = 0; k < 4; k++) {   // 32 bytes of K per MMA: K16 for f16, K32 for e4m3
-                        umma<F8>(d, umma_desc(sa + k * 32), umma_desc(sb + k * 32), (kb > 0 || k > 0) ? 1u : 0u);
+                        umma<F8>(d, umma_desc(sa + k * 32), umma_desc(sb + k * 32), kIdesc, (kb > 0 || k > 0) ? 1u : 0u);
                     }
                     umma_commit(&sm.empty[stage]);
                     if (++stage == NST) {
@@ -404,7 +284,7 @@ k_xtc(const __grid_constant__ CUtensorMap tmap, XArgs a, int* err)
     __syncthreads();
     if (warp == 0) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+        tc::tmem_dealloc(tmem, TMEM_COLS);
     }
 }
 
