@@ -270,13 +270,13 @@ __device__ __forceinline__ void pass_store(float2* buf, const float2* v, int t)
 // Divisions by F are multiplications by the exact power-of-two reciprocal.
 constexpr float kInvPiF = 0.318309886183790671538f;
 
+// Rotator argument x (half-turns) of table entry e; the entry is (cos, sin)(pi x).
 template <int F, bool CPX>
-__device__ __forceinline__ float2 rot_entry(int e, const DelayEntry& d, double lo, double lofrac, bool fraclo,
-                                            const float* ctab)
+__device__ __forceinline__ float rot_arg(int e, const DelayEntry& d, double lo, double lofrac, bool fraclo,
+                                         const float* ctab)
 {
     using P = FPlan<F, CPX>;
     constexpr double kInvF = 1.0 / F;
-    float x;
     if (e < P::S) {
         // kernel.c:434-466: subphase[j] = lo * (j/F * a + b'), b' = b - (int)b
         const double intdelay = trunc(d.b);
@@ -284,18 +284,24 @@ __device__ __forceinline__ float2 rot_entry(int e, const DelayEntry& d, double l
         const double xoff = dmul((double)e, kInvF);
         double ph = dmul(dadd(dmul(xoff, d.a), bp), lo);
         if (fraclo) ph = dadd(ph, dmul(lofrac, intdelay));
-        x = __double2float_rn(-2.0 * dsub(ph, trunc(ph)));
+        return __double2float_rn(-2.0 * dsub(ph, trunc(ph)));
     } else if (e < P::S + P::STRIDE) {
         // kernel.c:145, 452, 469: stepphase[i] = lo * (i*stride/F * a)
         const double xoff = dmul((double)((e - P::S) * P::STRIDE), kInvF);
         const double ph = dmul(dmul(xoff, d.a), lo);
-        x = __double2float_rn(-2.0 * dsub(ph, trunc(ph)));
+        return __double2float_rn(-2.0 * dsub(ph, trunc(ph)));
     } else {
         const float arg = __fmul_rn(ctab[e - P::S - P::STRIDE], __double2float_rn(d.frac));
-        x = __fmul_rn(arg, kInvPiF);
+        return __fmul_rn(arg, kInvPiF);
     }
+}
+
+template <int F, bool CPX>
+__device__ __forceinline__ float2 rot_entry(int e, const DelayEntry& d, double lo, double lofrac, bool fraclo,
+                                            const float* ctab)
+{
     float sn, cs;
-    sincospif(x, &sn, &cs);
+    sincospif(rot_arg<F, CPX>(e, d, lo, lofrac, fraclo, ctab), &sn, &cs);
     return make_float2(cs, sn);
 }
 

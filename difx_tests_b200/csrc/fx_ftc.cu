@@ -40,8 +40,9 @@ constexpr int TB = 16;                    // FFTs per work item
 constexpr int NPAIR = TB / 2;             // A1 stages per item
 constexpr int NA1 = 3;                    // A1 ring
 constexpr int ND1 = 4;                    // D1 ring (64 TMEM columns each)
-constexpr int NTHREADS = 416;             // 13 warps
+constexpr int NTHREADS = 448;             // 14 warps
 constexpr int INB = 544;                  // staged bytes per FFT: the window plus read-ahead
+constexpr int NIB = 4;                    // pair slots the helper fills ahead of the producer
 constexpr int NROT = F2 + F1;             // fringe sub[64] | step[32] per FFT
 constexpr uint32_t TMEM_COLS = 512;
 constexpr uint32_t D2_COL = ND1 * 64;     // D2: 4 tiles x 64 columns
@@ -54,19 +55,26 @@ struct Smem {
     alignas(1024) uint8_t a1[NA1][128 * 128];    // [stage][row b * 64 + n2]
     alignas(1024) uint8_t b1[64 * 128];          // [(k1, re|im)][(n1, re|im)]
     alignas(1024) uint8_t b2[2][64 * 128];       // [K half][(k2, re|im)][(n2 % 32, re|im)]
-    alignas(16) uint8_t inb[2][2][INB];         // [pair parity][FFT of the pair]
-    float2 rtab[2][2][NROT];                     // [pair parity][FFT of the pair]
-    float2 fsub[TB][F1];                         // [b][k1]
-    float2 fstep[K2H][TB];                       // [k2][b]
+    alignas(16) uint8_t inb[NIB][2][INB];       // [pair % NIB][FFT of the pair] input bytes
+    float2 rtab[NIB][2][NROT];                   // [pair % NIB][FFT of the pair] fringe sub | step
+    int2 pwin[NIB][2];                           // [pair % NIB][FFT] (bit of sample 0 in inb, valid)
+    DelayEntry oent[2][TB];                      // output: delay entries [item parity][FFT]
+    double olo[2];                               // LO of the item's subband
+    float2 fsub[TB][F1 + 1];                     // output: [b][k1] (padded row)
+    float2 fstep[K2H][TB];                       // output: [k2][b]
     float2 lut[16];                              // two 2-bit codes -> two levels
     float ctab[P::FS + P::FST];                  // chan_sub | chan_step
     uint64_t a1_full[NA1], a1_empty[NA1], d1_full[ND1], d1_empty[ND1];
     uint64_t a2_full, a2_empty, d2_full, d2_empty, drain;
-    uint64_t stg[2];
+    uint64_t cp_full[NIB], tab_full[NIB], tab_empty[NIB];
     uint32_t tmem_base;
     int abort;
 };
 static_assert(sizeof(Smem) + 1024 <= 232448, "fits the opt-in shared memory of one CTA");
+
+// A1 row of sample n2 = 4 o + i2 of FFT b of a pair: the eight n2 quads a quarter-warp stores
+// land in eight different rows mod 8, so its 16-byte stores hit eight different bank groups
+__device__ __forceinline__ int a1_row(int b, int o, int i2) { return b * 64 + 8 * i2 + (o & 7) + 32 * (o >> 3); }
 
 // 16-byte chunk c of row r of a K-major SWIZZLE_128B tile
 __device__ __forceinline__ uint32_t sw128(int r, int c) { return (uint32_t)(r * 128 + ((c ^ (r & 7)) << 4)); }
@@ -126,28 +134,45 @@ __device__ __forceinline__ void window(const DelayEntry& d, int& base, int& nvec
     nvec = (F / 4 + 1 + (first - base) + 15) >> 4;
 }
 
-// Input bytes of the two FFTs of flat pair g, by one thread: one expect_tx for both, then the copies.
-__device__ __forceinline__ void issue_pair(const FArgs& a, Smem& sm, int g, int ntb)
+// Rotator entry e (the F stage's table order) from the same FP64 phase argument, evaluated by
+// the special-function unit: absolute error ~1e-6, far below the FP16 rounding of these spectra
+__device__ __forceinline__ float2 rot_fast(int e, const DelayEntry& d, double lo, double lofrac, bool fraclo,
+                                           const float* ctab)
 {
-    const Item it = item_of(blockIdx.x + (g / NPAIR) * gridDim.x, a.nant, ntb);
-    const int p = g % NPAIR;
-    const uint8_t* row = a.data + ((size_t)it.sb * a.nant + it.ant) * a.pitch;
-    int base[2], nvec[2];
-    bool v[2];
-    uint32_t total = 0;
-    for (int b = 0; b < 2; b++) {
-        DelayEntry d;
-        v[b] = entry(a, it.ant, it.tb0 + 2 * p + b, d);
-        if (v[b]) {
-            window(d, base[b], nvec[b]);
-            total += 16u * nvec[b];
-        }
-    }
-    uint64_t* bar = &sm.stg[g & 1];
-    tc::fence_async_smem();   // earlier reads of the buffer (ordered by the producers' barrier)
-    tc::mbar_expect_tx(bar, total);
-    for (int b = 0; b < 2; b++)
-        if (v[b]) bulk_copy(bar, sm.inb[g & 1][b], row + base[b], 16u * nvec[b]);
+    float sn, cs;
+    __sincosf(3.14159265358979f * rot_arg<F, false>(e, d, lo, lofrac, fraclo, ctab), &sn, &cs);
+    return make_float2(cs, sn);
+}
+
+// (cos, sin)(pi x) by the special-function unit
+__device__ __forceinline__ float2 cis_half_turns(float x)
+{
+    float sn, cs;
+    __sincosf(3.14159265358979f * x, &sn, &cs);
+    return make_float2(cs, sn);
+}
+
+// Delay entry of FFT t of item i of this CTA (valid = 0 for slots without data)
+__device__ __forceinline__ DelayEntry item_entry(const FArgs& a, int i, int ntb, int t)
+{
+    const Item it = item_of(blockIdx.x + i * gridDim.x, a.nant, ntb);
+    DelayEntry d;
+    if (!entry(a, it.ant, it.tb0 + t, d)) d.valid = 0;
+    return d;
+}
+
+// Input bytes of the two FFTs of a pair (entries d0, d1 of subband/antenna row `row`) into pair
+// slot x, by one thread: one arrive.expect_tx for both, then the copies.
+__device__ __forceinline__ void issue_pair(Smem& sm, int x, const uint8_t* row, const DelayEntry& d0,
+                                           const DelayEntry& d1)
+{
+    int base[2] = {0, 0}, nvec[2] = {0, 0};
+    if (d0.valid) window(d0, base[0], nvec[0]);
+    if (d1.valid) window(d1, base[1], nvec[1]);
+    // the producers' earlier reads of this slot are ordered before the copy by tab_empty
+    tc::mbar_expect_tx(&sm.cp_full[x], 16u * (nvec[0] + nvec[1]));
+    if (d0.valid) bulk_copy(&sm.cp_full[x], sm.inb[x][0], row + base[0], 16u * nvec[0]);
+    if (d1.valid) bulk_copy(&sm.cp_full[x], sm.inb[x][1], row + base[1], 16u * nvec[1]);
 }
 
 template <bool AMAX>
@@ -180,8 +205,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc(FArgs a)
         mbar_init(&sm.d2_full, 1);
         mbar_init(&sm.d2_empty, 128);
         mbar_init(&sm.drain, 1);
-        mbar_init(&sm.stg[0], 1);
-        mbar_init(&sm.stg[1], 1);
+        for (int s = 0; s < NIB; s++) {
+            mbar_init(&sm.cp_full[s], 1);
+            mbar_init(&sm.tab_full[s], 1);
+            mbar_init(&sm.tab_empty[s], 128);
+        }
         sm.abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -216,57 +244,33 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc(FArgs a)
 
     if (warp < 4) {
         // ================================================================ producer
+        // pair g's input bytes, rotator tables and window offsets are in slot g % NIB once
+        // cp_full and tab_full complete (the helper warp fills them ahead)
         const int tp = threadIdx.x;
         const int bsel = tp >> 6, t64 = tp & 63, o = t64 & 15, h = t64 >> 4;
         const int npair = nitem * NPAIR;
-        int issued = -1;   // last flat pair whose copy was issued
-        if (tp == 0 && npair > 0) {
-            issue_pair(a, sm, 0, ntb);
-            issued = 0;
-        }
-        bool bad = false;
         for (int g = 0; g < npair; g++) {
-            const Item it = item_of(blockIdx.x + (g / NPAIR) * gridDim.x, a.nant, ntb);
-            const int p = g % NPAIR;
-            const int par = g & 1;
-            const double lo = a.sb_lo[it.sb];
-            const double lofrac = dsub(lo, trunc(lo));
-            const bool fraclo = lofrac > 1e-11;   // kernel.c:39
-            // fringe rotator tables of the pair's two FFTs
-            for (int e = tp; e < 2 * NROT; e += 128) {
-                const int b = e / NROT, idx = e - b * NROT;
-                DelayEntry d;
-                const bool v = entry(a, it.ant, it.tb0 + 2 * p + b, d);
-                sm.rtab[par][b][idx] = v ? rot_entry<F, false>(idx, d, lo, lofrac, fraclo, sm.ctab) : make_float2(0.f, 0.f);
-            }
-            if (bar_or(1, 128, bad || *abort_flag)) break;
-            if (tp == 0 && g + 1 < npair) {
-                issue_pair(a, sm, g + 1, ntb);
-                issued = g + 1;
-            }
-            const int s = g % NA1;
-            if (!mbar_wait(&sm.stg[par], (g >> 1) & 1, abort_flag) ||
+            const int x = g % NIB, s = g % NA1;
+            const uint32_t ph = (g / NIB) & 1;
+            if (!mbar_wait(&sm.cp_full[x], ph, abort_flag) || !mbar_wait(&sm.tab_full[x], ph, abort_flag) ||
                 !mbar_wait(&sm.a1_empty[s], ((g / NA1) & 1) ^ 1, abort_flag)) {
                 if (!*abort_flag) atomicCAS(a.err, 0, ERR_WAIT);
                 *abort_flag = 1;
-                bad = true;
-                continue;   // leave at the next barrier, together with the other producers
+                break;
             }
             // 4 consecutive samples n2 = 4o..4o+3 for 8 values n1 = 8h..8h+7 of FFT bsel
             uint32_t res[4][8];
-            DelayEntry d;
-            if (entry(a, it.ant, it.tb0 + 2 * p + bsel, d)) {
-                int base, nvec;
-                window(d, base, nvec);
-                const int P0 = 2 * (d.offset + 4 * o - 4 * base);   // bit of sample 4o in the window
+            const int2 wv = sm.pwin[x][bsel];
+            if (wv.y) {
+                const int P0 = wv.x + 8 * o;                 // bit of sample 4o in the window
                 const int w0 = P0 >> 5, sh = P0 & 31;
-                const uint32_t* wp = reinterpret_cast<const uint32_t*>(sm.inb[par][bsel]);
-                const float2* rt = sm.rtab[par][bsel];
+                const uint32_t* wp = reinterpret_cast<const uint32_t*>(sm.inb[x][bsel]);
+                const float2* rt = sm.rtab[x][bsel];
                 float2 sub[4], stp[8];
 #pragma unroll
-                for (int i = 0; i < 4; i++) sub[i] = rt[4 * o + i];
+                for (int k = 0; k < 4; k++) sub[k] = rt[4 * o + k];
 #pragma unroll
-                for (int i = 0; i < 8; i++) stp[i] = rt[F2 + 8 * h + i];
+                for (int k = 0; k < 8; k++) stp[k] = rt[F2 + 8 * h + k];
 #pragma unroll
                 for (int i1 = 0; i1 < 8; i1++) {
                     const int idx = w0 + 4 * (8 * h + i1);   // 128 bits per n1
@@ -286,10 +290,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc(FArgs a)
 #pragma unroll
                     for (int i1 = 0; i1 < 8; i1++) res[i2][i1] = 0u;
             }
+            mbar_arrive(&sm.tab_empty[x]);   // this thread's last read of slot x
             uint8_t* st = sm.a1[s];
 #pragma unroll
             for (int i2 = 0; i2 < 4; i2++) {
-                const int r = bsel * 64 + 4 * o + i2;
+                const int r = a1_row(bsel, o, i2);
 #pragma unroll
                 for (int jj = 0; jj < 2; jj++)
                     *reinterpret_cast<uint4*>(st + sw128(r, 2 * h + jj)) =
@@ -298,22 +303,19 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc(FArgs a)
             fence_async_smem();
             mbar_arrive(&sm.a1_full[s]);
         }
-        // copies must land before the CTA exits: the last one issued, and the one before it when
-        // its wait gave up (waits on phases already complete return at once)
-        if (tp == 0)
-            for (int x = issued - 1; x <= issued; x++)
-                if (x >= 0 && !mbar_drain(&sm.stg[x & 1], (x >> 1) & 1)) atomicCAS(a.err, 0, ERR_WAIT);
     } else if (warp < 8) {
         // ================================================================ twiddle
         const int q = warp & 3;
-        const int r = 32 * q + lane;                // D1 row: b % 2 = r / 64, n2 = r % 64
-        const int bl = r >> 6, n2 = r & 63;
+        const int r = 32 * q + lane;                // D1 row = a1_row(b % 2, o, i2), n2 = 4 o + i2
+        const int bl = r >> 6, rr = r & 63;
+        const int n2 = 4 * ((rr & 7) + 8 * (rr >> 5)) + ((rr >> 3) & 3);
         const int khalf = n2 >> 5, cl = (n2 & 31) >> 2, wd = n2 & 3;
         float2 tw[F1];
 #pragma unroll
         for (int k1 = 0; k1 < F1; k1++) tw[k1] = twiddle_exact(n2 * k1, F);
         bool ok = true;
         for (int i = 0; i < nitem && ok; i++) {
+            // warp-uniform (the TMEM loads are .sync.aligned)
             if (!__all_sync(0xffffffffu, mbar_wait(&sm.a2_empty, (i & 1) ^ 1, abort_flag))) {
                 ok = false;
                 break;
@@ -321,7 +323,6 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc(FArgs a)
             for (int p = 0; p < NPAIR; p++) {
                 const int g = i * NPAIR + p;
                 const int dslot = g % ND1;
-                // warp-uniform: the TMEM loads below are .sync.aligned
                 if (!__all_sync(0xffffffffu, mbar_wait(&sm.d1_full[dslot], (g / ND1) & 1, abort_flag))) {
                     ok = false;
                     break;
@@ -365,34 +366,50 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc(FArgs a)
         __half* spec = reinterpret_cast<__half*>(a.spec);
         const size_t chan_stride = (size_t)a.rows * a.T;
         const int nsig = a.nant;
+        // item i's entries are in oent[i & 1] before the item's first barrier (written after the
+        // previous item's second barrier, loaded into registers one item earlier)
+        DelayEntry dnext;
+        double lonext = 0.0;
+        if (to < TB && nitem > 0) sm.oent[0][to] = item_entry(a, 0, ntb, to);
+        if (to == 0 && nitem > 0) sm.olo[0] = a.sb_lo[item_of(blockIdx.x, a.nant, ntb).sb];
+        if (to < TB && nitem > 1) dnext = item_entry(a, 1, ntb, to);
+        if (to == 0 && nitem > 1) lonext = a.sb_lo[item_of(blockIdx.x + gridDim.x, a.nant, ntb).sb];
         bool ok = true;
         for (int i = 0; i < nitem; i++) {
             const Item it = item_of(blockIdx.x + i * gridDim.x, a.nant, ntb);
-            if (bar_or(2, 128, !ok || *abort_flag)) break;   // the previous item's table reads are done
-            const double lo = a.sb_lo[it.sb];
+            // item i's entries visible; every thread is done with item i - 1's tables
+            if (bar_or(2, 128, !ok || *abort_flag)) break;
+            const double lo = sm.olo[i & 1];
             const double lofrac = dsub(lo, trunc(lo));
             const bool fraclo = lofrac > 1e-11;
-            for (int e = to; e < TB * (F1 + K2H); e += 128) {
-                const bool isub = e < TB * F1;
-                const int e2 = isub ? e : e - TB * F1;
-                const int bb = isub ? e2 / F1 : e2 % TB;
-                const int kx = isub ? e2 % F1 : e2 / TB;
-                DelayEntry d;
-                const bool v = entry(a, it.ant, it.tb0 + bb, d);
-                const int ridx = F2 + F1 + (isub ? kx : P::FS + kx);
-                const float2 w = v ? rot_entry<F, false>(ridx, d, lo, lofrac, fraclo, sm.ctab) : make_float2(0.f, 0.f);
-                if (isub) sm.fsub[bb][kx] = w;
-                else sm.fstep[kx][bb] = w;
+#pragma unroll
+            for (int e = to; e < TB * K2H; e += 128) {
+                const int bb = e % TB, k2 = e / TB;
+                const DelayEntry& d = sm.oent[i & 1][bb];
+                sm.fstep[k2][bb] = d.valid ? rot_fast(F2 + F1 + P::FS + k2, d, lo, lofrac, fraclo, sm.ctab)
+                                           : make_float2(0.f, 0.f);
+            }
+#pragma unroll
+            for (int e = to; e < TB * F1; e += 128) {
+                const int bb = e / F1, k1 = e % F1;
+                const DelayEntry& d = sm.oent[i & 1][bb];
+                sm.fsub[bb][k1] = d.valid ? rot_fast(F2 + F1 + k1, d, lo, lofrac, fraclo, sm.ctab) : make_float2(0.f, 0.f);
             }
             if (bar_or(2, 128, !ok || *abort_flag)) break;
-            // warp-uniform (the TMEM loads are .sync.aligned); a thread that gave up leaves at the
-            // next barrier together with the rest of the group
+            if (i + 1 < nitem) {
+                if (to < TB) sm.oent[(i + 1) & 1][to] = dnext;
+                if (to == 0) sm.olo[(i + 1) & 1] = lonext;
+                if (to < TB && i + 2 < nitem) dnext = item_entry(a, i + 2, ntb, to);
+                if (to == 0 && i + 2 < nitem) lonext = a.sb_lo[item_of(blockIdx.x + (i + 2) * gridDim.x, a.nant, ntb).sb];
+            }
             if (!__all_sync(0xffffffffu, mbar_wait(&sm.d2_full, i & 1, abort_flag))) {
                 ok = false;
                 continue;
             }
             tc_fence_after();
             __half* dst0 = spec + ((size_t)it.sb * C) * chan_stride + (size_t)(2 * it.ant) * a.T + it.tb0 + b;
+            const size_t kstep = (size_t)F1 * chan_stride;   // channel k -> k + 32
+            const size_t tim = (size_t)a.T;                  // Re row -> Im row
 #pragma unroll 1
             for (int j = 0; j < 4; j++) {
                 const int k1 = 8 * j + kl;
@@ -400,6 +417,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc(FArgs a)
 #pragma unroll
                 for (int hf = 0; hf < 2; hf++) {
                     uint32_t v[32];
+                    __half* pk = dst0 + (size_t)k1 * chan_stride + (size_t)(16 * hf) * kstep;
                     tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + D2_COL + 64 * j + 32 * hf, v);
                     tmem_wait_ld();
                     if (j == 3 && hf == 1) {
@@ -410,13 +428,12 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc(FArgs a)
                     for (int kk = 0; kk < 16; kk++) {
                         const int k2 = 16 * hf + kk;
                         const float2 x = make_float2(__uint_as_float(v[2 * kk]), __uint_as_float(v[2 * kk + 1]));
-                        const float2 fr = cmul(fs, sm.fstep[k2][b]);
-                        const float2 y = cmul(fr, x);
+                        const float2 y = cmul(cmul(fs, sm.fstep[k2][b]), x);
                         const __half2 hv = __floats2half2_rn(y.x, y.y);
                         const int k = k1 + F1 * k2;
-                        __half* dst = dst0 + (size_t)k * chan_stride;
-                        dst[0] = __low2half(hv);
-                        dst[a.T] = __high2half(hv);
+                        pk[0] = __low2half(hv);
+                        pk[tim] = __high2half(hv);
+                        pk += kstep;
                         if constexpr (AMAX) {
                             // max(|Re|, |Im|) over the item's 16 FFTs: lanes 0-15 and 16-31 hold
                             // channels k1 and k1 + 1
@@ -437,6 +454,73 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc(FArgs a)
             if (!*abort_flag) atomicCAS(a.err, 0, ERR_WAIT);
             *abort_flag = 1;
         }
+    } else if (warp == 13) {
+        // ================================================================ helper
+        // For each pair, NIB pairs ahead of the producer: the input copies, the fringe rotator
+        // tables and the window offsets.  The phases are linear in the sample index
+        // (kernel.c:434-470): sub[j] has phase lo (j a / F + b') (+ lofrac (int)b when the LO has
+        // a fractional part) and step[i] has lo i stride a / F, each evaluated as one FP64
+        // multiply-add from per-FFT slope and offset (rounding ~1e-16 of the phase in turns).
+        const int npair = nitem * NPAIR;
+        DelayEntry dn0, dn1;                 // entries of the next pair
+        double lon = 0.0;
+        const uint8_t* rown = nullptr;
+        auto fetch = [&](int g, DelayEntry& d0, DelayEntry& d1, double& lo, const uint8_t*& row) {
+            const int i = g / NPAIR, p = g % NPAIR;
+            d0 = item_entry(a, i, ntb, 2 * p);
+            d1 = item_entry(a, i, ntb, 2 * p + 1);
+            const Item it = item_of(blockIdx.x + i * gridDim.x, a.nant, ntb);
+            lo = a.sb_lo[it.sb];
+            row = a.data + ((size_t)it.sb * a.nant + it.ant) * a.pitch;
+        };
+        if (npair > 0) fetch(0, dn0, dn1, lon, rown);
+        int issued = -1;
+        for (int g = 0; g < npair; g++) {
+            const int x = g % NIB;
+            const DelayEntry d0 = dn0, d1 = dn1;
+            const double lo = lon;
+            const uint8_t* row = rown;
+            if (g + 1 < npair) fetch(g + 1, dn0, dn1, lon, rown);   // in flight during this pair
+            if (!__all_sync(0xffffffffu, mbar_wait(&sm.tab_empty[x], ((g / NIB) & 1) ^ 1, abort_flag))) {
+                if (!*abort_flag) atomicCAS(a.err, 0, ERR_WAIT);
+                *abort_flag = 1;
+                break;
+            }
+            if (lane == 0) {
+                issue_pair(sm, x, row, d0, d1);
+                issued = g;
+            }
+            const double lofrac = lo - trunc(lo);
+            const bool fraclo = lofrac > 1e-11;   // kernel.c:39
+#pragma unroll
+            for (int b = 0; b < 2; b++) {
+                const DelayEntry& d = b ? d1 : d0;
+                const double intdelay = trunc(d.b);
+                double v = lo * (d.b - intdelay);
+                if (fraclo) v = fma(lofrac, intdelay, v);
+                const double slope = lo * d.a * (1.0 / F);
+#pragma unroll
+                for (int k = 0; k < 2; k++) {
+                    const int j = lane + 32 * k;
+                    const double ph = fma((double)j, slope, v);
+                    sm.rtab[x][b][j] = d.valid ? cis_half_turns((float)(-2.0 * (ph - trunc(ph)))) : make_float2(0.f, 0.f);
+                }
+                const double phs = (double)(lane * F1) * slope;
+                sm.rtab[x][b][F2 + lane] = d.valid ? cis_half_turns((float)(-2.0 * (phs - trunc(phs))))
+                                                   : make_float2(0.f, 0.f);
+                if (lane == b) {
+                    int base = 0, nvec = 0;
+                    if (d.valid) window(d, base, nvec);
+                    sm.pwin[x][b] = make_int2(2 * (d.offset - 4 * base), d.valid);
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&sm.tab_full[x]);
+        }
+        // copies must land before the CTA exits (phases already complete return at once)
+        if (lane == 0)
+            for (int g = issued - (NIB - 1); g <= issued; g++)
+                if (g >= 0 && !mbar_drain(&sm.cp_full[g % NIB], (g / NIB) & 1)) atomicCAS(a.err, 0, ERR_WAIT);
     } else if (lane == 0) {
         // ================================================================ MMA issuer
         bool ok = true;
