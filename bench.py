@@ -301,10 +301,10 @@ def run_reference_arm(args):
 
 
 # ------------------------------------------------------------------ GPU arm
-# DRAM bytes per input sample of the F stage's FP16 (tensor-core) variant,
-# dram__bytes_read.sum + dram__bytes_write.sum from one ncu capture of
-# k_fstage<2048,1,16,1> on the 64-antenna x 1024-channel profiling case, divided
-# by the samples of that launch (profiles/kernels_cfg2s_ncu_full.txt).
+# DRAM bytes per input sample of the tensor-core F stage (k_ftc, 2048-point FFTs, FP16
+# spectra), dram__bytes_read.sum + dram__bytes_write.sum from one ncu capture on the
+# 64-antenna x 1024-channel profiling case, divided by the samples of that launch
+# (profiles/k_ftc_cfg2s_ncu.txt).
 FSTAGE_TC_DRAM_BYTES_PER_SAMPLE = 2.17
 
 
@@ -413,12 +413,18 @@ def run_gpu_arm(args):
     sm = head["stage_ms"]
     traffic = (FSTAGE_TC_DRAM_BYTES_PER_SAMPLE * head["samples_per_launch"]
                if xmode == fx.FXC_X_TC_FP16 and args.workload.startswith("cfg2") else None)
-    roof = {"kernel": "k_fstage (fused unpack/shift/fringe/FFT/frac-delay)", "bound": "hbm", "achieved": f_gbs,
+    ftc = xmode != fx.FXC_X_PLAIN_FP32 and w["nchan"] == 1024 and w["npol"] == 1
+    roof = {"kernel": ("k_ftc (tcgen05 F stage: unpack/fringe, 32x64 DFT as two tensor-core GEMMs, twiddles, "
+                       "frac-delay, F16 store)" if ftc else
+                       "k_fstage (fused unpack/shift/fringe/FFT/frac-delay)"),
+            "bound": "hbm", "achieved": f_gbs,
             "peak": hbm, "unit": "GB/s", "frac": f_gbs / hbm, "traffic": traffic,
             "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
             "algorithmic_bytes_per_launch": f_bytes, "launch_ms": head["f_ms_launch"],
             "share": sm[1] / max(1e-9, sm.sum()),
-            "note": "F stage is FP32-issue-bound; HBM fraction shown for its algorithmic bytes"}
+            "note": ("latency-bound warp-specialised pipeline (the output warpgroup saturates first); "
+                     "HBM fraction shown for its algorithmic bytes" if ftc else
+                     "F stage is FP32-issue-bound; HBM fraction shown for its algorithmic bytes")}
 
     line = {
         "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,

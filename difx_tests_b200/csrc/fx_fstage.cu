@@ -32,17 +32,21 @@ cudaError_t launch_fstage_batch_8192(int mode, int npol, int tb, const FArgs* d_
                                   cudaStream_t st);
 size_t fstage_smem_8192(int mode, int tb, int npol);
 
-// The F16 layout's F stage runs on the tensor cores where that kernel covers the geometry;
-// FXC_TC_FSTAGE=fft selects the FP32 FFT kernel instead (the two agree within FP16 rounding).
-static bool ftc_wanted()
+// The F16 layout's F stage runs on the tensor cores where that kernel covers the geometry, for
+// the FP16 form (the FP8 form's per-channel absmax lands on that kernel's busiest warps and the
+// FP32 FFT kernel is faster there).  FXC_TC_FSTAGE=fft selects the FFT kernel for both forms,
+// FXC_TC_FSTAGE=tc the tensor-core kernel for both (the two agree within FP16 rounding).
+static bool ftc_wanted(const FArgs& a)
 {
     const char* v = std::getenv("FXC_TC_FSTAGE");
-    return !(v && std::strcmp(v, "fft") == 0);
+    if (v && std::strcmp(v, "fft") == 0) return false;
+    if (v && std::strcmp(v, "tc") == 0) return true;
+    return a.amax == nullptr;
 }
 
 cudaError_t launch_fstage(int nchan, int mode, const FArgs& a, cudaStream_t st)
 {
-    if (ftc_supported(nchan, mode, a) && ftc_wanted()) return launch_ftc(a, st);
+    if (ftc_supported(nchan, mode, a) && ftc_wanted(a)) return launch_ftc(a, st);
     switch (a.cpx ? nchan : 2 * nchan) {   // FFT length: complex samples fill every bin
     case 256: return launch_fstage_256(mode, a, st);
     case 512: return launch_fstage_512(mode, a, st);

@@ -1,6 +1,7 @@
 """GPU parity of the tensor-core F stage (2048-point FFTs, one polarisation, F16 spectra):
 visibilities against the FP64 oracle at the tensor-core bar, and against the FP32-FFT
-F stage that FXC_TC_FSTAGE=fft selects.  Work items are 16 FFTs of one (subband,
+F stage that FXC_TC_FSTAGE=fft selects (FXC_TC_FSTAGE=tc puts the FP8 form, which by
+default uses the FFT kernel, on the tensor-core one).  Work items are 16 FFTs of one (subband,
 antenna); the cases cover partial items (nfft not a multiple of 16), several subbands,
 FFTs without data at the subintegration's edges and many items per CTA."""
 import numpy as np
@@ -75,7 +76,7 @@ def test_tc_fstage_edge_ffts_without_data(monkeypatch):
 
 def test_tc_fstage_fp8_form(monkeypatch):
     job = synth.make_job(nant=20, npol=1, nchan=1024, numffts=256, bw=64e6, lo=1.4e9, rho=0.1, seed=13)
-    v8, c8 = run(job, monkeypatch, xmode=fx.FXC_X_TC_FP8)
+    v8, c8 = run(job, monkeypatch, fstage="tc", xmode=fx.FXC_X_TC_FP8)
     v8f, c8f = run(job, monkeypatch, fstage="fft", xmode=fx.FXC_X_TC_FP8)
     np.testing.assert_array_equal(c8, c8f)
     # the two F stages differ by FP16 rounding; the e4m3 quantisation of both dominates
