@@ -244,7 +244,8 @@ const char* fxc_strerror(int status);
 int fxc_last_cuda_error(void);
 /* Which device-side wait expired when a call returned FXC_ERR_TIMEOUT on this
  * thread: tensor-core X stage 1 stage load, 2 stage release, 3 accumulator release,
- * 4 accumulator ready, 5 drain at exit; F stage 6 input staging copy; 0 if none.
+ * 4 accumulator ready, 5 drain at exit; F stage 6 input staging copy, 7 a wait of the
+ * tensor-core F stage (input copy, stage ring, TMEM hand-off or drain); 0 if none.
  * (16 after FXC_ERR_INVALID: an FFT's input was outside its window.) */
 int fxc_last_device_error(void);
 
