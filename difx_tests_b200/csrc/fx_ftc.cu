@@ -15,12 +15,15 @@
 // b = the FFT within a work item of 16 consecutive FFTs of one (subband, antenna).
 //
 // Persistent, warp-specialised CTA (one per SM):
-//   warps 0-3   producer: decode + fringe rotation, two FFTs per A1 stage (ring of 3); the
-//               stage's input bytes arrive by bulk copy one stage ahead
+//   warps 0-3   producer: decode + fringe rotation, two FFTs per A1 stage (ring of 3)
 //   warps 4-7   twiddle: D1 (TMEM ring of 4) -> twiddles -> A2 (all 16 FFTs, 128 KB)
 //   warps 8-11  output: D2 -> fractional-sample rotator -> F16 spectra rows [chan][row][T]
 //               (16 FFTs = one 32-byte sector per row); FP8 form: absmax per (chan, signal)
 //   warp 12     MMA issuer (one thread), TMEM owner
+//   warp 13     helper: up to four pairs ahead of the producer, the input bulk copies, the
+//               fringe rotator tables and the window offsets of each pair
+// The FP8 form uses this kernel only when FXC_TC_FSTAGE=tc (its absmax reduction lands on
+// the output warps, this kernel's busiest role).
 // Every wait is bounded (1 s): on expiry the CTA records code 7 in the error word, stops,
 // drains what it issued and frees TMEM.
 #include "fx_fstage.cuh"
