@@ -82,3 +82,48 @@ def test_tc_fstage_fp8_form(monkeypatch):
     # the two F stages differ by FP16 rounding; the e4m3 quantisation of both dominates
     mx, rms = fo.vis_error(v8[0], v8f[0])
     assert rms.max() < 0.05, f"rms {rms.max():.3e}"
+
+
+def test_tc_fstage_host_windows_equal_whole_device_input(monkeypatch):
+    """Input streamed from the host through the three device windows gives exactly what the
+    whole-subintegration device input gives (windows coincide with the spectra chunks)."""
+    monkeypatch.delenv("FXC_TC_FSTAGE", raising=False)
+    job = synth.make_job(nant=6, npol=1, nchan=1024, numffts=400, bw=64e6, lo=1.4e9, rho=0.1, seed=15, nsubband=2)
+    with corr_for(job, xmode=fx.FXC_X_TC_FP16, chunk_ffts=128) as c:
+        c.upload(job.data)
+        dptr, pitch = c.device_input()
+        c.process_device(dptr, pitch, job.delays, job.fileoffsets)
+        ref = c.visibilities()
+        c.reset()
+        c.process(job.data, job.delays, job.fileoffsets)
+        got = c.visibilities()
+    np.testing.assert_array_equal(got[1], ref[1])
+    np.testing.assert_array_equal(got[0], ref[0])
+
+
+def test_tc_fstage_window_only_context_vs_oracle(monkeypatch):
+    monkeypatch.delenv("FXC_TC_FSTAGE", raising=False)
+    job = synth.make_job(nant=5, npol=1, nchan=1024, numffts=300, bw=64e6, lo=1.4e9, rho=0.1, seed=17)
+    job.fileoffsets[2] -= 20.3 * 2 * job.nchan / (2 * job.bw)   # its first FFTs have no data
+    with corr_for(job, xmode=fx.FXC_X_TC_FP16, chunk_ffts=128, window_ffts=70) as c:
+        c.process_window(job.data, job.delays, job.fileoffsets, 11, 250)
+        vis, counts = c.visibilities()
+    ref, rc = fo.correlate(job.data[0], job.delays, job.fileoffsets, job.bw, job.lo, job.nchan, job.npol,
+                           fftindex=np.arange(11, 261), numffts=job.numffts, maxoffset_ffts=job.numffts)
+    np.testing.assert_array_equal(counts, rc)
+    mx, rms = fo.vis_error(vis[0], ref)
+    assert rms.max() < TC_RMS_TOL and mx.max() < TC_MAX_TOL, f"rms {rms.max():.3e} max {mx.max():.3e}"
+
+
+def test_tc_fstage_subband_groups(monkeypatch):
+    """A spectra budget too small for every subband: chunks over groups of subbands."""
+    monkeypatch.delenv("FXC_TC_FSTAGE", raising=False)
+    monkeypatch.setenv("FXC_SPECTRA_BUDGET_MB", "2")
+    job = synth.make_job(nant=8, npol=1, nchan=1024, numffts=300, bw=64e6, lo=1.4e9, rho=0.1, seed=19, nsubband=3)
+    vis, counts = run(job, monkeypatch, xmode=fx.FXC_X_TC_FP16)
+    for sb in range(job.nsubband):
+        ref, rc = fo.correlate(job.data[sb], job.delays, job.fileoffsets, job.bw, float(job.sb_lo[sb]), job.nchan,
+                               job.npol, numffts=job.numffts, maxoffset_ffts=job.numffts)
+        np.testing.assert_array_equal(counts, rc)
+        mx, rms = fo.vis_error(vis[sb], ref)
+        assert rms.max() < TC_RMS_TOL and mx.max() < TC_MAX_TOL, f"sb {sb}: rms {rms.max():.3e}"
