@@ -187,12 +187,26 @@ def accuracy_sample(w, xmode):
 
 
 # ------------------------------------------------------------------ CPU reference
-REF_GEOM = dict(nant=32, nchan=1024, bw=64e6, lo=1.4e9)   # 64 signals as 32 dual-pol antennas
+# The reference reads only interleaved dual-polarisation input and needs a square channel count
+# (kernel.c:31-35), so its sample of a workload keeps the workload's signal count as dual-pol
+# antennas: 64 signals as 32 dual-pol antennas x 1024 ch for the cfg2 geometry (the default, also
+# used for workloads the reference cannot run), the dual-pol variant of cfg0 (4 ant x 2 pol x 256 ch).
+REF_GEOMS = {"cfg0": dict(nant=4, nchan=256, bw=32e6, lo=1.4e9, nfft=20000,
+                          what="4 ant x 2 pol (the P=2 variant of this workload)"),
+             "default": dict(nant=32, nchan=1024, bw=64e6, lo=1.4e9, nfft=600,
+                             what="32 ant x 2 pol (the reference's only input format; 64 signals like the GPU "
+                                  "workload)")}
+REF_GEOM = REF_GEOMS["default"]
+
+
+def ref_geom_for(workload):
+    global REF_GEOM
+    REF_GEOM = REF_GEOMS.get(workload, REF_GEOMS["default"])
+    return REF_GEOM
 
 
 def ref_workload_desc(nfft):
-    return (f"reference kernel.c (+ IPP stand-in) on {REF_GEOM['nant']} ant x 2 pol (the reference's only input "
-            f"format; 64 signals like the GPU workload) x {REF_GEOM['nchan']} ch, {nfft} FFTs")
+    return f"reference kernel.c (+ IPP stand-in) on {REF_GEOM['what']} x {REF_GEOM['nchan']} ch, {nfft} FFTs"
 
 
 def ref_run_shard(nfft, seed):
@@ -223,10 +237,11 @@ def _quiet_call(fn, *a):
         os.close(devnull)
 
 
-def cpu_baseline_one_core(nfft=600):
+def cpu_baseline_one_core(nfft=None):
     from oracle import refcall
     if not refcall.available():
         return None
+    nfft = nfft or REF_GEOM["nfft"]
     dt, samp = _quiet_call(ref_run_shard, nfft, 99)
     return {"value": samp / dt / 1e9, "unit": UNIT, "cores": 1, "kind": "reference",
             "sample": ref_workload_desc(nfft) + f", 1 process, {dt:.1f} s"}
@@ -271,13 +286,14 @@ def run_reference_arm(args):
         return 0
     from oracle import refcall
     w = WORKLOADS[args.workload]
+    ref_geom_for(args.workload)
     if not refcall.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libfxref.so not built"}))
         return 0
     nproc = len(os.sched_getaffinity(0))
     # bound the leak: <= ~24 GB in flight over all processes
     per_call_kb = 75.0
-    nfft = int(max(8, min(160, 24e6 / (nproc * REF_GEOM["nant"] * per_call_kb))))
+    nfft = int(max(8, min(160 * 32 // REF_GEOM["nant"], 24e6 / (nproc * REF_GEOM["nant"] * per_call_kb))))
     for _ in range(args.warmup):
         ref_parallel_step(nproc, nfft, 7)
     times, samples = [], []
@@ -491,6 +507,7 @@ def run_gpu_arm(args):
     if rank == 0 and not args.no_accuracy:
         line["accuracy"] = {f: accuracy_sample(w, XMODES[f]) for f in forms}
     if rank == 0 and world == 1 and not args.no_cpu:
+        ref_geom_for(args.workload)
         cb = cpu_baseline_one_core()
         if cb is not None:
             line["cpu_baseline"] = cb
