@@ -62,7 +62,6 @@ struct Smem {
     float2 rtab[NIB][2][NROT];                   // [pair % NIB][FFT of the pair] fringe sub | step
     int2 pwin[NIB][2];                           // [pair % NIB][FFT] (bit of sample 0 in inb, valid)
     DelayEntry oent[2][TB];                      // output: delay entries [item parity][FFT]
-    double olo[2];                               // LO of the item's subband
     float2 fsub[TB][F1 + 1];                     // output: [b][k1] (padded row)
     float2 fstep[K2H][TB];                       // output: [k2][b]
     float2 lut[16];                              // two 2-bit codes -> two levels
@@ -137,21 +136,19 @@ __device__ __forceinline__ void window(const DelayEntry& d, int& base, int& nvec
     nvec = (F / 4 + 1 + (first - base) + 15) >> 4;
 }
 
-// Rotator entry e (the F stage's table order) from the same FP64 phase argument, evaluated by
-// the special-function unit: absolute error ~1e-6, far below the FP16 rounding of these spectra
-__device__ __forceinline__ float2 rot_fast(int e, const DelayEntry& d, double lo, double lofrac, bool fraclo,
-                                           const float* ctab)
-{
-    float sn, cs;
-    __sincosf(3.14159265358979f * rot_arg<F, false>(e, d, lo, lofrac, fraclo, ctab), &sn, &cs);
-    return make_float2(cs, sn);
-}
-
 // (cos, sin)(pi x) by the special-function unit
 __device__ __forceinline__ float2 cis_half_turns(float x)
 {
     float sn, cs;
     __sincosf(3.14159265358979f * x, &sn, &cs);
+    return make_float2(cs, sn);
+}
+
+// Fractional-sample rotator entry: e^{i ctab[j] frac} (kernel.c:512-523), j < FS + FST
+__device__ __forceinline__ float2 frac_rot(int j, const DelayEntry& d, const float* ctab)
+{
+    float sn, cs;
+    __sincosf(__fmul_rn(ctab[j], __double2float_rn(d.frac)), &sn, &cs);
     return make_float2(cs, sn);
 }
 
@@ -372,38 +369,29 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc(FArgs a)
         // item i's entries are in oent[i & 1] before the item's first barrier (written after the
         // previous item's second barrier, loaded into registers one item earlier)
         DelayEntry dnext;
-        double lonext = 0.0;
         if (to < TB && nitem > 0) sm.oent[0][to] = item_entry(a, 0, ntb, to);
-        if (to == 0 && nitem > 0) sm.olo[0] = a.sb_lo[item_of(blockIdx.x, a.nant, ntb).sb];
         if (to < TB && nitem > 1) dnext = item_entry(a, 1, ntb, to);
-        if (to == 0 && nitem > 1) lonext = a.sb_lo[item_of(blockIdx.x + gridDim.x, a.nant, ntb).sb];
         bool ok = true;
         for (int i = 0; i < nitem; i++) {
             const Item it = item_of(blockIdx.x + i * gridDim.x, a.nant, ntb);
             // item i's entries visible; every thread is done with item i - 1's tables
             if (bar_or(2, 128, !ok || *abort_flag)) break;
-            const double lo = sm.olo[i & 1];
-            const double lofrac = dsub(lo, trunc(lo));
-            const bool fraclo = lofrac > 1e-11;
 #pragma unroll
             for (int e = to; e < TB * K2H; e += 128) {
                 const int bb = e % TB, k2 = e / TB;
                 const DelayEntry& d = sm.oent[i & 1][bb];
-                sm.fstep[k2][bb] = d.valid ? rot_fast(F2 + F1 + P::FS + k2, d, lo, lofrac, fraclo, sm.ctab)
-                                           : make_float2(0.f, 0.f);
+                sm.fstep[k2][bb] = d.valid ? frac_rot(P::FS + k2, d, sm.ctab) : make_float2(0.f, 0.f);
             }
 #pragma unroll
             for (int e = to; e < TB * F1; e += 128) {
                 const int bb = e / F1, k1 = e % F1;
                 const DelayEntry& d = sm.oent[i & 1][bb];
-                sm.fsub[bb][k1] = d.valid ? rot_fast(F2 + F1 + k1, d, lo, lofrac, fraclo, sm.ctab) : make_float2(0.f, 0.f);
+                sm.fsub[bb][k1] = d.valid ? frac_rot(k1, d, sm.ctab) : make_float2(0.f, 0.f);
             }
             if (bar_or(2, 128, !ok || *abort_flag)) break;
             if (i + 1 < nitem) {
                 if (to < TB) sm.oent[(i + 1) & 1][to] = dnext;
-                if (to == 0) sm.olo[(i + 1) & 1] = lonext;
                 if (to < TB && i + 2 < nitem) dnext = item_entry(a, i + 2, ntb, to);
-                if (to == 0 && i + 2 < nitem) lonext = a.sb_lo[item_of(blockIdx.x + (i + 2) * gridDim.x, a.nant, ntb).sb];
             }
             if (!__all_sync(0xffffffffu, mbar_wait(&sm.d2_full, i & 1, abort_flag))) {
                 ok = false;
