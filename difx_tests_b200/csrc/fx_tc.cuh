@@ -25,6 +25,7 @@ __device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count)
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
 }
 
+// One arrival on the barrier that also adds `bytes` to the transaction count its phase waits for
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes)
 {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes)
