@@ -107,6 +107,7 @@ SIGNATURES = {
     "fxc_debug_unpack": (_I, [_P, _DP, _DP, _I, _I, _FP]),
     "fxc_debug_spectra": (_I, [_P, _DP, _DP, _I, _I, _FP]),
     "fxc_debug_expire_wait": (_I, [_P]),
+    "fxc_debug_expire_wait_tc": (_I, [_P]),
 }
 
 

@@ -1016,6 +1016,14 @@ int fxc_debug_expire_wait(fxc_ctx* x)
     return FXC_OK;
 }
 
+int fxc_debug_expire_wait_tc(fxc_ctx* x)
+{
+    if (!x) return FXC_ERR_INVALID;
+    FXC_CK(cudaSetDevice(x->device));
+    FXC_CK(launch_expire_wait_tc(x->d_err, x->stream));
+    return FXC_OK;
+}
+
 int fxc_debug_spectra(fxc_ctx* x, const double* delays, const double* offs, int first, int nfft, float* out)
 {
     if (!x || !out || nfft > x->T) return FXC_ERR_INVALID;

@@ -566,6 +566,27 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc(FArgs a)
 
 }  // namespace ftc
 
+// Failure-path check of the tensor-core kernels' bounded wait: an mbarrier that nothing completes
+// (no copy or MMA is ever issued, so nothing is left in flight) runs out after 1 s and records
+// code 7, as an expired wait of the tensor-core F stage would.
+__global__ void k_expire_wait_tc(int* err)
+{
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ int abort_flag;
+    if (threadIdx.x == 0) {
+        tc::mbar_init(&bar, 1);
+        abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        if (!tc::mbar_wait(&bar, 0, &abort_flag)) atomicCAS(err, 0, ftc::ERR_WAIT);
+    }
+}
+
+cudaError_t launch_expire_wait_tc(int* err, cudaStream_t st)
+{
+    k_expire_wait_tc<<<1, 32, 0, st>>>(err);
+    return cudaGetLastError();
+}
+
 bool ftc_supported(int nchan, int mode, const FArgs& a)
 {
     return mode == kSpecF16 && nchan == ftc::C && a.npol == 1 && !a.cpx && a.T % ftc::TB == 0 &&

@@ -41,5 +41,7 @@ size_t xtc_smem_bytes();
 cudaError_t launch_unpack_debug(int nchan, const FArgs& a, float* out, cudaStream_t st);
 // a bounded device wait that runs out (error word code 6), for tests of the failure path
 cudaError_t launch_expire_wait(int* err, cudaStream_t st);
+// the same for the tensor-core kernels' mbarrier wait (error word code 7)
+cudaError_t launch_expire_wait_tc(int* err, cudaStream_t st);
 
 }  // namespace fx

@@ -275,6 +275,11 @@ int fxc_debug_spectra(fxc_ctx* ctx, const double* delays, const double* fileoffs
  * path of the device waits without faulting the GPU; the context stays usable. */
 int fxc_debug_expire_wait(fxc_ctx* ctx);
 
+/* As fxc_debug_expire_wait, for the bounded wait of the tensor-core kernels (the mbarrier
+ * wait that the tensor-core F and X stages use for their stage rings and TMEM hand-offs):
+ * the next synchronising call returns FXC_ERR_TIMEOUT and fxc_last_device_error() gives 7. */
+int fxc_debug_expire_wait_tc(fxc_ctx* ctx);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

@@ -127,3 +127,26 @@ def test_tc_fstage_subband_groups(monkeypatch):
         np.testing.assert_array_equal(counts, rc)
         mx, rms = fo.vis_error(vis[sb], ref)
         assert rms.max() < TC_RMS_TOL and mx.max() < TC_MAX_TOL, f"sb {sb}: rms {rms.max():.3e}"
+
+
+def test_tensor_core_wait_expiry_is_reported_and_context_survives(monkeypatch):
+    """The tensor-core kernels' bounded mbarrier wait, run out on a barrier that nothing
+    completes, comes back as FXC_ERR_TIMEOUT with code 7; the next tensor-core correlation on
+    the same context is correct."""
+    import ctypes as C
+    monkeypatch.delenv("FXC_TC_FSTAGE", raising=False)
+    job = synth.make_job(nant=6, npol=1, nchan=1024, numffts=64, bw=64e6, lo=1.4e9, rho=0.1, seed=23)
+    with corr_for(job, xmode=fx.FXC_X_TC_FP16) as c:
+        assert fx.lib().fxc_debug_expire_wait_tc(C.c_void_p(c.handle.value)) == fx.FXC_OK
+        with pytest.raises(fx.FxcError) as e:
+            c.synchronize()
+        assert e.value.status == fx.FXC_ERR_TIMEOUT
+        assert fx.lib().fxc_last_device_error() == 7
+        c.reset()
+        c.process(job.data, job.delays, job.fileoffsets)
+        vis, counts = c.visibilities()
+    ref, rc = fo.correlate(job.data[0], job.delays, job.fileoffsets, job.bw, job.lo, job.nchan, job.npol,
+                           numffts=job.numffts, maxoffset_ffts=job.numffts)
+    np.testing.assert_array_equal(counts, rc)
+    mx, rms = fo.vis_error(vis[0], ref)
+    assert rms.max() < TC_RMS_TOL and mx.max() < TC_MAX_TOL
