@@ -1,0 +1,24 @@
+"""CPU checks of bench.py's reference sampling: the reference CPU correlator reads only
+interleaved dual-polarisation input with a square channel count, so each workload's CPU
+baseline and reference arm run the reference on a dual-pol geometry it accepts, stated in
+the sample description."""
+import math
+import os
+import sys
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, REPO)
+
+import bench  # noqa: E402
+
+
+def test_reference_geometry_per_workload():
+    g0 = bench.ref_geom_for("cfg0")
+    assert (g0["nant"], g0["nchan"]) == (4, 256)          # the dual-pol variant of cfg0
+    assert "4 ant x 2 pol" in bench.ref_workload_desc(10)
+    for wl in ("cfg1", "cfg2", "cfg4", "cfg3"):
+        g = bench.ref_geom_for(wl)
+        assert (g["nant"], g["nchan"]) == (32, 1024)      # 64 signals as 32 dual-pol antennas
+    for g in bench.REF_GEOMS.values():
+        assert math.isqrt(g["nchan"]) ** 2 == g["nchan"]  # kernel.c:31-35 needs a square channel count
+    bench.ref_geom_for("cfg2")
