@@ -1,0 +1,94 @@
+"""CPU checks of the tensor-core F stage's shared-memory and TMEM layout arithmetic
+(difx_tests_b200/csrc/fx_ftc.cu), restated here from the kernel's formulas: every role
+writes and reads the rows and swizzled 16-byte chunks the other roles expect, the
+stores land in distinct shared-memory banks, and the staged-input reads stay inside the
+staging buffer for every sample offset.  A change to one role's index mapping that the
+others do not follow fails here before any GPU run."""
+import itertools
+
+F = 2048          # FFT length
+F1, F2 = 32, 64   # n = 64 n1 + n2, k = k1 + 32 k2
+TB = 16           # FFTs per work item
+INB = 544         # staged bytes per FFT
+
+
+def a1_row(b, o, i2):
+    """A1 row of sample n2 = 4 o + i2 of FFT b of a pair (producer)."""
+    return b * 64 + 8 * i2 + (o & 7) + 32 * (o >> 3)
+
+
+def sw128(r, c):
+    """Byte offset of 16-byte chunk c of row r in a K-major SWIZZLE_128B tile."""
+    return r * 128 + ((c ^ (r & 7)) << 4)
+
+
+def twiddle_row_to_n2(r):
+    """(b % 2, n2) of D1 row r as the twiddle warps decode it."""
+    bl, rr = r >> 6, r & 63
+    return bl, 4 * ((rr & 7) + 8 * (rr >> 5)) + ((rr >> 3) & 3)
+
+
+def test_a1_rows_are_a_bijection_the_twiddle_inverts():
+    rows = {a1_row(b, o, i2) for b in range(2) for o in range(16) for i2 in range(4)}
+    assert rows == set(range(128))
+    for r in range(128):
+        bl, n2 = twiddle_row_to_n2(r)
+        assert a1_row(bl, n2 // 4, n2 % 4) == r
+
+
+def test_producer_quarter_warps_store_to_eight_bank_groups():
+    # thread tp: FFT tp >> 6, o = tp & 15, h = (tp & 63) >> 4; store (i2, jj) writes row a1_row(.., o, i2),
+    # chunk 2 h + jj.  A 16-byte store is served a quarter-warp (8 lanes) at a time.
+    for warp, i2, jj in itertools.product(range(4), range(4), range(2)):
+        for q in range(4):
+            banks = set()
+            for lane in range(8 * q, 8 * q + 8):
+                tp = 32 * warp + lane
+                b, o, h = tp >> 6, tp & 15, (tp & 63) >> 4
+                off = sw128(a1_row(b, o, i2), 2 * h + jj)
+                banks.add((off % 128) // 16)      # 16-byte bank group within the 128-byte line
+            assert len(banks) == 8, (warp, i2, jj, q)
+
+
+def test_twiddle_stores_fill_a2_without_conflicts_and_cover_every_element():
+    seen = set()
+    for p, k1 in itertools.product(range(TB // 2), range(F1)):
+        for q in range(4):                        # warp q of the twiddle group: D1 lanes 32q..32q+31
+            words = set()
+            for lane in range(32):
+                bl, n2 = twiddle_row_to_n2(32 * q + lane)
+                b = 2 * p + bl
+                R = ((k1 & 7) << 4) + b
+                khalf, cl, wd = n2 >> 5, (n2 & 31) >> 2, n2 & 3
+                off = sw128(R, cl) + wd * 4
+                words.add(off // 4 % 32)          # 4-byte bank
+                seen.add((k1 >> 3, khalf, off))
+            assert len(words) == 32               # one store instruction, 32 distinct banks
+    # every (tile, K half, row, 4-byte word) of A2 written exactly once per item
+    assert len(seen) == 4 * 2 * 128 * 32
+
+
+def test_output_rows_match_a2_rows():
+    # step-2 row R of tile j = (k1 % 8, b); the output thread of TMEM lane r takes k1 % 8 = r >> 4, b = r & 15
+    for r in range(128):
+        kl, b = r >> 4, r & 15
+        assert ((kl & 7) << 4) + b == r
+
+
+def test_staged_input_reads_stay_inside_the_buffer():
+    # window: base = (offset >> 2) & ~15, nvec = (F/4 + 1 + first - base + 15) >> 4 vectors of 16 bytes;
+    # bit of sample 0 in the window P = 2 (offset - 4 base); thread (o, h) reads words w0 + 4 n1 and + 1
+    for offset in range(0, 256):
+        first = offset >> 2
+        base = first & ~15
+        nvec = (F // 4 + 1 + (first - base) + 15) >> 4
+        assert 16 * nvec <= INB - 16
+        p_bit = 2 * (offset - 4 * base)
+        for o, h in itertools.product(range(16), range(4)):
+            w0 = (p_bit + 8 * o) >> 5
+            sh = (p_bit + 8 * o) & 31
+            for i1 in range(8):
+                idx = w0 + 4 * (8 * h + i1)
+                assert 4 * (idx + 2) <= INB              # the second word of the funnel shift is in the buffer
+                last_bit = 32 * idx + sh + 7             # the 8 bits (4 samples) this read uses
+                assert last_bit < 8 * 16 * nvec          # ... lie inside the copied window
