@@ -156,7 +156,7 @@ __device__ __forceinline__ float2 frac_rot(int j, const DelayEntry& d, const flo
 __device__ __forceinline__ DelayEntry item_entry(const FArgs& a, int i, int ntb, int t)
 {
     const Item it = item_of(blockIdx.x + i * gridDim.x, a.nant, ntb);
-    DelayEntry d;
+    DelayEntry d{};   // slots without data: all zero
     if (!entry(a, it.ant, it.tb0 + t, d)) d.valid = 0;
     return d;
 }
