@@ -7,11 +7,12 @@ subintegration = 31250 FFTs per subband at 128 MS/s, 2-bit real samples.
 One step = one subintegration (all subbands) through the whole hot path:
 delay table, fused unpack/shift/fringe/FFT/fractional-sample F stage, X stage.
 
-  python bench.py [--gpus N --steps K --warmup W] [--xmode all|both|tc|fp8|plain] [--impl reference]
+  python bench.py [--gpus N --steps K --warmup W] [--xmode all|both|tc|tc16f|fp8|plain] [--impl reference]
 
-The headline `value` is the tensor-core form (FP32 F stage, FP16 X inputs with
-FP32 accumulation); the FP8-E4M3 tensor-core form and the FP32 plain form run on
-the same input in the same invocation and are reported under "fp8" and "plain".
+The headline `value` is the tensor-core form: FP32 F stage (FFT on the CUDA cores), its
+spectra cast to FP16 for the tcgen05 X stage with FP32 accumulation.  The same X form on the
+FP16 tensor-core F stage ("tc16f"), the FP8-E4M3 tensor-core form and the FP32 plain form run
+on the same input in the same invocation and are reported under their names.
 
 Under torchrun (N > 1) every rank correlates its own subintegration (weak
 scaling, no data-path collective) and rank 0 prints one JSON line; time is the
@@ -165,7 +166,7 @@ def delay_model(nant, nchan, bw, seed):
 
 
 # ------------------------------------------------------------------ accuracy
-def accuracy_sample(w, xmode):
+def accuracy_sample(w, xmode, fstage=0):
     """max / RMS relative visibility error vs the FP64 oracle on a bounded sample
     of the workload's geometry (1 subband, 128 FFTs, full generator)."""
     import difx_tests_b200 as fx
@@ -174,7 +175,7 @@ def accuracy_sample(w, xmode):
     nf = 128
     job = synth.make_job(nant=w["nant"], npol=w["npol"], nchan=w["nchan"], numffts=nf, bw=w["bw"], lo=w["lo"],
                          rho=w["rho"], seed=1234)
-    cfg = fx.make_config(job.nant, job.nchan, nf, job.bw, job.lo, npol=job.npol, xmode=xmode)
+    cfg = fx.make_config(job.nant, job.nchan, nf, job.bw, job.lo, npol=job.npol, xmode=xmode, fstage=fstage)
     with fx.Correlator(cfg) as c:
         c.process(job.data, job.delays, job.fileoffsets)
         vis, counts = c.visibilities()
@@ -209,15 +210,17 @@ def ref_workload_desc(nfft):
     return f"reference kernel.c (+ IPP stand-in) on {REF_GEOM['what']} x {REF_GEOM['nchan']} ch, {nfft} FFTs"
 
 
-def ref_run_shard(nfft, seed):
-    """One bounded run of the reference CPU correlator; returns (seconds, samples)."""
+def ref_run_shard(nfft, seed, hoisted=False):
+    """One bounded run of the reference CPU correlator (as written, or with allocKernel hoisted
+    out of its FFT x antenna loop); returns (seconds, samples)."""
     from difx_tests_b200 import synth
     from oracle import refcall
     g = REF_GEOM
     job = synth.random_job(nant=g["nant"], npol=2, nchan=g["nchan"], numffts=nfft, bw=g["bw"], lo=g["lo"],
                            seed=seed)
     t0 = time.perf_counter()
-    refcall.run_reference(job.data[0], job.delays, job.fileoffsets, g["nchan"], nfft, g["bw"], g["lo"])
+    refcall.run_reference(job.data[0], job.delays, job.fileoffsets, g["nchan"], nfft, g["bw"], g["lo"],
+                          hoisted=hoisted)
     dt = time.perf_counter() - t0
     return dt, g["nant"] * 2 * nfft * 2 * g["nchan"]
 
@@ -243,14 +246,20 @@ def cpu_baseline_one_core(nfft=None):
         return None
     nfft = nfft or REF_GEOM["nfft"]
     dt, samp = _quiet_call(ref_run_shard, nfft, 99)
-    return {"value": samp / dt / 1e9, "unit": UNIT, "cores": 1, "kind": "reference",
-            "sample": ref_workload_desc(nfft) + f", 1 process, {dt:.1f} s"}
+    out = {"value": samp / dt / 1e9, "unit": UNIT, "cores": 1, "kind": "reference",
+           "sample": ref_workload_desc(nfft) + f", 1 process, {dt:.1f} s"}
+    if refcall.available(hoisted=True):
+        dh, sh = _quiet_call(ref_run_shard, nfft, 99, True)
+        out["allockernel_hoisted"] = {"value": sh / dh / 1e9, "unit": UNIT, "cores": 1,
+                                      "sample": "the same, kernel.c with allocKernel moved out of its FFT x antenna "
+                                                f"loop (kernel.c:727-728), {dh:.1f} s"}
+    return out
 
 
-def ref_parallel_step(nproc, nfft_per_proc, seed):
+def ref_parallel_step(nproc, nfft_per_proc, seed, hoisted=False):
     """All host cores: nproc forked processes over FFT shards (the reference's own
     split decomposition, main.c:398-408); each exits after its shard (kernel.c
-    leaks ~75 KB per FFT x antenna)."""
+    leaks ~75 KB per FFT x antenna unless allocKernel is hoisted)."""
     pipes = []
     t0 = time.perf_counter()
     for i in range(nproc):
@@ -259,7 +268,7 @@ def ref_parallel_step(nproc, nfft_per_proc, seed):
         if pid == 0:
             os.close(r)
             try:
-                dt, samp = _quiet_call(ref_run_shard, nfft_per_proc, seed + i)
+                dt, samp = _quiet_call(ref_run_shard, nfft_per_proc, seed + i, hoisted)
                 os.write(wfd, f"{dt} {samp}".encode())
             finally:
                 os._exit(0)
@@ -290,6 +299,11 @@ def run_reference_arm(args):
     if not refcall.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libfxref.so not built"}))
         return 0
+    # load the reference library in this process too (the forked children inherit the mapping)
+    refcall.lib()
+    hoisted = refcall.available(hoisted=True)
+    if hoisted:
+        refcall.lib(hoisted=True)
     nproc = len(os.sched_getaffinity(0))
     # bound the leak: <= ~24 GB in flight over all processes
     per_call_kb = 75.0
@@ -303,6 +317,20 @@ def run_reference_arm(args):
         samples.append(s)
     tot = sum(times)
     val = sum(samples) / tot / 1e9
+    extra = {}
+    if hoisted:
+        # the secondary figure: kernel.c with allocKernel hoisted out of its FFT x antenna loop
+        ref_parallel_step(nproc, nfft, 7, True)
+        th, sh = [], []
+        for k in range(args.steps):
+            dt, s_ = ref_parallel_step(nproc, nfft, 1000 + 37 * k, True)
+            th.append(dt)
+            sh.append(s_)
+        extra["allockernel_hoisted"] = {
+            "value": sum(sh) / sum(th) / 1e9, "unit": UNIT, "cores": nproc,
+            "ms_per_step": 1e3 * sum(th) / args.steps,
+            "sample": f"as the headline, kernel.c with allocKernel moved out of its FFT x antenna loop "
+                      f"(kernel.c:727-728; oracle/hoist_allockernel.py), {nproc} processes x {nfft} FFTs"}
     line = {
         "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
@@ -312,30 +340,43 @@ def run_reference_arm(args):
                          "sample": f"{nproc} forked processes x {nfft} FFTs each per step"},
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    line.update(extra)
     print(json.dumps(line))
     return 0
 
 
 # ------------------------------------------------------------------ GPU arm
-# DRAM bytes per input sample of the tensor-core F stage (k_ftc, 2048-point FFTs, FP16
-# spectra), dram__bytes_read.sum + dram__bytes_write.sum from one ncu capture on the
-# 64-antenna x 1024-channel profiling case, divided by the samples of that launch
-# (profiles/k_ftc_cfg2s_ncu.txt).
-FSTAGE_TC_DRAM_BYTES_PER_SAMPLE = 2.17
+# DRAM bytes per input sample of the F-stage kernels (2048-point FFTs), dram__bytes_read.sum +
+# dram__bytes_write.sum from one ncu capture each on the 64-antenna x 1024-channel profiling case,
+# divided by the samples of that launch: key (fstage, F16 output)
+# (profiles/kernels_cfg2s_ncu_full.txt for k_fstage, profiles/k_ftc_cfg2s_ncu.txt for k_ftc).
+FSTAGE_DRAM_BYTES_PER_SAMPLE = {(1, True): 2.17, (1, False): 4.16, (2, True): 2.17}
 
 
-XMODES = {"plain": 0, "tc": 1, "fp8": 2}    # FXC_X_PLAIN_FP32, FXC_X_TC_FP16, FXC_X_TC_FP8
-DTYPES = {"plain": "f32",
-          "tc": "f32 F stage / f16 X inputs, f32 accumulate",
-          "fp8": "f32 F stage / e4m3 X inputs scaled per signal and channel, f32 accumulate"}
+# form -> (fxc_config.xmode, fxc_config.fstage)
+FORMS = {"plain": (0, 1),     # FXC_X_PLAIN_FP32, FXC_F_FFT32
+         "tc": (1, 1),        # FXC_X_TC_FP16 on the FP32 FFT F stage (the headline form)
+         "tc16f": (1, 2),     # FXC_X_TC_FP16 on the FP16 tensor-core F stage (FXC_F_TC16)
+         "fp8": (2, 1)}       # FXC_X_TC_FP8 on the FP32 FFT F stage
+XMODES = {k: v[0] for k, v in FORMS.items()}
+DTYPES = {"plain": "f32 (FFT F stage and X stage on the CUDA cores)",
+          "tc": "f32 FFT F stage (CUDA cores), spectra cast to f16 for the tensor-core X stage, f32 accumulate",
+          "tc16f": "f16 tensor-core F stage (k_ftc: f16 DFT matrices and intermediate), f16 X inputs, "
+                   "f32 accumulate",
+          "fp8": "f32 FFT F stage (CUDA cores), spectra cast to e4m3 scaled per signal and channel for the "
+                 "tensor-core X stage, f32 accumulate"}
+F_KERNELS = {1: "k_fstage (fused unpack/shift/fringe/FFT/frac-delay, FP32 radix-16 FFT on the CUDA cores)",
+             2: "k_ftc (tcgen05 F stage: unpack/fringe, 32x64 DFT as two FP16 tensor-core GEMMs, twiddles, "
+                "frac-delay, F16 store)"}
 
 
-def time_form(torch, dist, fx, w, xmode, data, pitch, delays, offs, steps, warmup, world, dev, stream):
-    """Warm up, then time `steps` subintegrations of one X form; returns a result dict."""
+def time_form(torch, dist, fx, w, form, data, pitch, delays, offs, steps, warmup, world, dev, stream):
+    """Warm up, then time `steps` subintegrations of one form; returns a result dict."""
     F = 2 * w["nchan"]
     nsig = w["nant"] * w["npol"]
+    xmode, fstage = FORMS[form]
     cfg = fx.make_config(w["nant"], w["nchan"], w["numffts"], w["bw"], w["lo"], npol=w["npol"], nsubband=w["nsb"],
-                         xmode=xmode)
+                         xmode=xmode, fstage=fstage)
     corr = fx.Correlator(cfg)
     corr.set_stream(stream.cuda_stream)
     samples = w["nant"] * w["npol"] * w["nsb"] * w["numffts"] * F
@@ -410,37 +451,36 @@ def run_gpu_arm(args):
                            device=dev)
     torch.cuda.synchronize()
 
-    forms = {"all": ["tc", "fp8", "plain"], "both": ["tc", "plain"]}.get(args.xmode, [args.xmode])
+    forms = {"all": ["tc", "tc16f", "fp8", "plain"], "both": ["tc", "plain"]}.get(args.xmode, [args.xmode])
+    if w["nchan"] != 1024 or w["npol"] != 1:
+        forms = [f for f in forms if f != "tc16f"]   # the FP16 tensor-core F stage covers 1024 ch x 1 pol only
     res = {}
     for form in forms:
-        xm = XMODES[form]
-        res[form] = time_form(torch, dist, fx, w, xm, data, pitch, delays, offs, args.steps, args.warmup, world, dev,
+        res[form] = time_form(torch, dist, fx, w, form, data, pitch, delays, offs, args.steps, args.warmup, world, dev,
                               stream)
         if form != forms[0]:
             res[form]["corr"].close()
     head = res[forms[0]]
-    xmode = XMODES[forms[0]]
+    xmode, fstage = FORMS[forms[0]]
 
     # ---- roofline of the dominant kernel of the headline form (the F stage)
     hbm, tc_peak, peak_kind = peaks()
-    spec_bpc = 8 if xmode == fx.FXC_X_PLAIN_FP32 else 4       # bytes per complex spectrum value written
+    f16 = xmode != fx.FXC_X_PLAIN_FP32
+    spec_bpc = 4 if f16 else 8       # bytes per complex spectrum value written
     f_bytes = head["samples_per_launch"] * (0.25 + 0.5 * spec_bpc)
     f_gbs = f_bytes / (head["f_ms_launch"] / 1e3) / 1e9
     sm = head["stage_ms"]
-    traffic = (FSTAGE_TC_DRAM_BYTES_PER_SAMPLE * head["samples_per_launch"]
-               if xmode == fx.FXC_X_TC_FP16 and args.workload.startswith("cfg2") else None)
-    ftc = xmode != fx.FXC_X_PLAIN_FP32 and w["nchan"] == 1024 and w["npol"] == 1
-    roof = {"kernel": ("k_ftc (tcgen05 F stage: unpack/fringe, 32x64 DFT as two tensor-core GEMMs, twiddles, "
-                       "frac-delay, F16 store)" if ftc else
-                       "k_fstage (fused unpack/shift/fringe/FFT/frac-delay)"),
+    dram = FSTAGE_DRAM_BYTES_PER_SAMPLE.get((fstage, f16)) if w["nchan"] == 1024 else None
+    roof = {"kernel": F_KERNELS[fstage] + (", FP16 spectra out" if f16 else ", FP32 spectra out"),
             "bound": "hbm", "achieved": f_gbs,
-            "peak": hbm, "unit": "GB/s", "frac": f_gbs / hbm, "traffic": traffic,
+            "peak": hbm, "unit": "GB/s", "frac": f_gbs / hbm,
+            "traffic": dram * head["samples_per_launch"] if dram else None,
             "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
             "algorithmic_bytes_per_launch": f_bytes, "launch_ms": head["f_ms_launch"],
             "share": sm[1] / max(1e-9, sm.sum()),
-            "note": ("latency-bound warp-specialised pipeline (the output warpgroup saturates first); "
-                     "HBM fraction shown for its algorithmic bytes" if ftc else
-                     "F stage is FP32-issue-bound; HBM fraction shown for its algorithmic bytes")}
+            "note": ("latency-bound warp-specialised pipeline; HBM fraction shown for its algorithmic bytes"
+                     if fstage == 2 else
+                     "FP32 FFT is issue-bound on the CUDA cores; HBM fraction shown for its algorithmic bytes")}
 
     line = {
         "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -467,10 +507,12 @@ def run_gpu_arm(args):
     if "plain" in res and forms[0] != "plain":
         p = res["plain"]
         line["tc_vs_plain"] = {"gsamps": head["value"] / p["value"],
-                               "x_stage_only": (p["stage_ms"][2] / max(1e-9, sm[2]))}
-        if "fp8" in res:
-            line["fp8_vs_plain"] = {"gsamps": res["fp8"]["value"] / p["value"],
-                                    "x_stage_only": p["stage_ms"][2] / max(1e-9, res["fp8"]["stage_ms"][2])}
+                               "x_stage_only": (p["stage_ms"][2] / max(1e-9, sm[2])),
+                               "form": forms[0]}
+        for f in ("tc16f", "fp8"):
+            if f in res and f != forms[0]:
+                line[f + "_vs_plain"] = {"gsamps": res[f]["value"] / p["value"],
+                                         "x_stage_only": p["stage_ms"][2] / max(1e-9, res[f]["stage_ms"][2])}
 
     corr = head["corr"]
     # ---- end to end through the C ABI with pinned host buffers (rank-local)
@@ -505,7 +547,7 @@ def run_gpu_arm(args):
                        "path": "fxc_process_host + fxc_get_visibilities, pinned host input and output buffers"}
 
     if rank == 0 and not args.no_accuracy:
-        line["accuracy"] = {f: accuracy_sample(w, XMODES[f]) for f in forms}
+        line["accuracy"] = {f: accuracy_sample(w, *FORMS[f]) for f in forms}
     if rank == 0 and world == 1 and not args.no_cpu:
         ref_geom_for(args.workload)
         cb = cpu_baseline_one_core()
@@ -762,9 +804,10 @@ def main():
     ap.add_argument("--workload", default="cfg2", choices=sorted(WORKLOADS) + ["cfg3", "cfg4"],
                     help="cfg3: the batched uneven workload (12 jobs through fxc_batch_*); cfg4: the large "
                          "array (512 signals x 4096 channels x 16 subbands) streamed through device windows")
-    ap.add_argument("--xmode", default="all", choices=["all", "both", "tc", "fp8", "plain"],
-                    help="all: the FP16 tensor-core form is the headline value, the FP8 tensor-core and FP32 "
-                         "plain forms are timed beside it; both: FP16 tensor-core and plain")
+    ap.add_argument("--xmode", default="all", choices=["all", "both"] + sorted(FORMS),
+                    help="all: the FP16 tensor-core X form on the FP32 FFT F stage is the headline value; the same "
+                         "X form on the FP16 tensor-core F stage (tc16f), the FP8 form and the FP32 plain form are "
+                         "timed beside it; both: the headline and plain")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")

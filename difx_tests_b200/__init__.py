@@ -30,6 +30,10 @@ FXC_X_PLAIN_FP32 = 0
 FXC_X_TC_FP16 = 1
 FXC_X_TC_FP8 = 2
 
+FXC_F_AUTO = 0
+FXC_F_FFT32 = 1
+FXC_F_TC16 = 2
+
 
 class FxcConfig(C.Structure):
     """Mirror of ``fxc_config`` (include/fxcorr.h)."""
@@ -37,7 +41,7 @@ class FxcConfig(C.Structure):
         ("nant", C.c_int), ("npol", C.c_int), ("nchan", C.c_int), ("nbit", C.c_int),
         ("iscomplex", C.c_int), ("numffts", C.c_int), ("nsubband", C.c_int), ("xmode", C.c_int),
         ("lo", C.c_double), ("bw", C.c_double), ("sb_spacing", C.c_double), ("chunk_ffts", C.c_int),
-        ("window_ffts", C.c_int),
+        ("window_ffts", C.c_int), ("fstage", C.c_int),
     ]
 
 
@@ -141,8 +145,9 @@ def _dp(a):
 
 
 def make_config(nant, nchan, numffts, bw, lo, npol=2, nsubband=1, sb_spacing=None, xmode=FXC_X_PLAIN_FP32,
-                chunk_ffts=0, window_ffts=0, cpx=False) -> FxcConfig:
-    """cpx: 8-bit complex input (FFT length nchan) instead of the reference's 2-bit real."""
+                chunk_ffts=0, window_ffts=0, cpx=False, fstage=FXC_F_AUTO) -> FxcConfig:
+    """cpx: 8-bit complex input (FFT length nchan) instead of the reference's 2-bit real;
+    fstage: F-stage arithmetic (FXC_F_*)."""
     cfg = FxcConfig()
     _lib().fxc_config_default(C.byref(cfg))
     cfg.nant, cfg.npol, cfg.nchan, cfg.numffts = nant, npol, nchan, numffts
@@ -152,6 +157,7 @@ def make_config(nant, nchan, numffts, bw, lo, npol=2, nsubband=1, sb_spacing=Non
     cfg.xmode = xmode
     cfg.chunk_ffts = chunk_ffts
     cfg.window_ffts = window_ffts
+    cfg.fstage = fstage
     if cpx:
         cfg.nbit, cfg.iscomplex = 8, 1
     return cfg

@@ -134,6 +134,10 @@ static int validate(const fxc_config* c)
     // plain X: 8x8 register tiles, one CTA per channel group (<= 64 signals) or per pair of
     // 64-signal super-blocks; tensor-core X: 128x128 block pairs of the Gram
     if (c->nant * c->npol > 512) return FXC_ERR_UNSUPPORTED;
+    if (c->fstage < FXC_F_AUTO || c->fstage > FXC_F_TC16) return FXC_ERR_INVALID;
+    if (c->fstage == FXC_F_TC16 &&
+        !(c->xmode != FXC_X_PLAIN_FP32 && c->nchan == 1024 && c->npol == 1 && !c->iscomplex))
+        return FXC_ERR_UNSUPPORTED;
     return FXC_OK;
 }
 
@@ -524,6 +528,7 @@ FArgs ctx_fargs(fxc_ctx* x, const uint8_t* d_data, size_t pitch, int ld)
     a.tb = x->plan_tb;
     a.cpx = x->cfg.iscomplex;
     a.err = x->d_err;
+    a.fkind = x->cfg.fstage == FXC_F_AUTO ? FXC_F_FFT32 : x->cfg.fstage;
     return a;
 }
 

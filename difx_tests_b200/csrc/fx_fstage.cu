@@ -1,8 +1,5 @@
 // fx_fstage.cu -- dispatch of the fused F stage by FFT length (kernels in
 // fx_fstage.cuh, one translation unit per length) and the debug unpack export.
-#include <cstdlib>
-#include <cstring>
-
 #include "fx_fstage.cuh"
 
 namespace fx {
@@ -32,21 +29,14 @@ cudaError_t launch_fstage_batch_8192(int mode, int npol, int tb, const FArgs* d_
                                   cudaStream_t st);
 size_t fstage_smem_8192(int mode, int tb, int npol);
 
-// The F16 layout's F stage runs on the tensor cores where that kernel covers the geometry, for
-// the FP16 form (the FP8 form's per-channel absmax lands on that kernel's busiest warps and the
-// FP32 FFT kernel is faster there).  FXC_TC_FSTAGE=fft selects the FFT kernel for both forms,
-// FXC_TC_FSTAGE=tc the tensor-core kernel for both (the two agree within FP16 rounding).
-static bool ftc_wanted(const FArgs& a)
-{
-    const char* v = std::getenv("FXC_TC_FSTAGE");
-    if (v && std::strcmp(v, "fft") == 0) return false;
-    if (v && std::strcmp(v, "tc") == 0) return true;
-    return a.amax == nullptr;
-}
-
 cudaError_t launch_fstage(int nchan, int mode, const FArgs& a, cudaStream_t st)
 {
-    if (ftc_supported(nchan, mode, a) && ftc_wanted(a)) return launch_ftc(a, st);
+    // the FP16 tensor-core DFT only where the context asked for it (fxc_config.fstage);
+    // the configuration check admits it only for geometries it covers
+    if (a.fkind == FXC_F_TC16) {
+        if (!ftc_supported(nchan, mode, a)) return cudaErrorInvalidValue;
+        return launch_ftc(a, st);
+    }
     switch (a.cpx ? nchan : 2 * nchan) {   // FFT length: complex samples fill every bin
     case 256: return launch_fstage_256(mode, a, st);
     case 512: return launch_fstage_512(mode, a, st);

@@ -22,8 +22,8 @@
 //   warp 12     MMA issuer (one thread), TMEM owner
 //   warp 13     helper: up to four pairs ahead of the producer, the input bulk copies, the
 //               fringe rotator tables and the window offsets of each pair
-// The FP8 form uses this kernel only when FXC_TC_FSTAGE=tc (its absmax reduction lands on
-// the output warps, this kernel's busiest role).
+// Selected by fxc_config.fstage = FXC_F_TC16 (FP16 DFT matrices and intermediate: not FP32
+// accuracy); the FP8 form's absmax lands on the output warps, this kernel's busiest role.
 // Every wait is bounded (1 s): on expiry the CTA records code 7 in the error word, stops,
 // drains what it issued and frees TMEM.
 #include "fx_fstage.cuh"
@@ -71,6 +71,7 @@ struct Smem {
     uint64_t cp_full[NIB], tab_full[NIB], tab_empty[NIB];
     uint32_t tmem_base;
     int abort;
+    int drain_fail;                              // a drain wait expired: copies or MMAs may be in flight
 };
 static_assert(sizeof(Smem) + 1024 <= 232448, "fits the opt-in shared memory of one CTA");
 
@@ -211,6 +212,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc(FArgs a)
             mbar_init(&sm.tab_empty[s], 128);
         }
         sm.abort = 0;
+        sm.drain_fail = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 12) tmem_alloc(&sm.tmem_base, TMEM_COLS);
@@ -511,7 +513,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc(FArgs a)
         // copies must land before the CTA exits (phases already complete return at once)
         if (lane == 0)
             for (int g = issued - (NIB - 1); g <= issued; g++)
-                if (g >= 0 && !mbar_drain(&sm.cp_full[g % NIB], (g / NIB) & 1)) atomicCAS(a.err, 0, ERR_WAIT);
+                if (g >= 0 && !mbar_drain(&sm.cp_full[g % NIB], (g / NIB) & 1)) {
+                    atomicCAS(a.err, 0, ERR_WAIT);
+                    sm.drain_fail = 1;
+                }
     } else if (lane == 0) {
         // ================================================================ MMA issuer
         bool ok = true;
@@ -554,11 +559,16 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc(FArgs a)
         }
         // every MMA issued must have retired before TMEM is freed
         umma_commit(&sm.drain);
-        if (!mbar_drain(&sm.drain, 0)) atomicCAS(a.err, 0, ERR_WAIT);
+        if (!mbar_drain(&sm.drain, 0)) {
+            atomicCAS(a.err, 0, ERR_WAIT);
+            sm.drain_fail = 1;
+        }
     }
 
     __syncthreads();
-    if (warp == 12) {
+    // after an expired drain, MMAs may still write TMEM: it stays allocated (code 7 was recorded;
+    // the context's later tensor-core launches cannot be trusted and the process should reset)
+    if (warp == 12 && !sm.drain_fail) {
         tc_fence_after();
         tmem_dealloc(tmem, TMEM_COLS);
     }

@@ -1,13 +1,14 @@
 // fx_noalloc.cu -- one-shot correlation that allocates no device memory.
 //
 // Some callers cannot allocate GPU memory at the point they want to correlate:
-// code running inside a CUDA stream capture (cudaMalloc is not capturable),
-// real-time paths that must not hit the allocator's locks or latency, and
-// hosts whose device memory is fully reserved up front by another framework.
+// real-time paths that must not take the allocator's locks or wait on its
+// latency, and hosts whose device memory another framework reserved up front
+// (an allocation there fails or evicts that framework's pool).
 // fxc_correlate_noalloc serves them: the caller passes the packed input and the
 // output buffers (device memory it already owns); every intermediate (delay
-// model, delay table, validity bits, baseline counts, accumulators, spectra)
-// lives in one file-scope __device__ array of FXC_NOALLOC_SCRATCH_BYTES.
+// model, delay table, validity bits, baseline counts, accumulators, spectra, and
+// an error word) lives in one file-scope __device__ array of
+// FXC_NOALLOC_SCRATCH_BYTES.
 //
 // The array is part of the library image, so every GPU that loads this library
 // holds it until the process exits.  All calls share it and it keeps the last
@@ -19,6 +20,11 @@
 // address is obtained once per device with cudaGetSymbolAddress (with that
 // device current) and cached.  The first call on a device performs that
 // lookup, so make the first call before any stream capture begins.
+//
+// A bounded device wait of the F stage that runs out (its input copy never
+// completed) is reported in the outputs, since the call returns before the GPU
+// finishes: every visibility becomes NaN and every entry of d_counts (when
+// given) becomes -6.
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -77,6 +83,20 @@ __global__ void k_counts_to_output(const int* __restrict__ pair_counts, int nant
     }
 }
 
+// An expired device wait (error word != 0) poisons the outputs: NaN visibilities and
+// counts of -code, so a caller that cannot synchronise on the call still sees it.
+__global__ void k_noalloc_flag_error(const int* __restrict__ err, float* __restrict__ vis, size_t nvis_floats,
+                                     int* __restrict__ counts, int ncounts)
+{
+    const int code = *err;
+    if (code == 0) return;
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t nth = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = tid; i < nvis_floats; i += nth) vis[i] = __int_as_float(0x7fc00000);
+    if (counts)
+        for (size_t i = tid; i < (size_t)ncounts; i += nth) counts[i] = -code;
+}
+
 }  // namespace
 
 #define NA_CK(call)                                   \
@@ -113,6 +133,7 @@ extern "C" int fxc_correlate_noalloc(const fxc_config* cfg, const uint8_t* d_dat
     const int ld = (int)(((size_t)nfft + 127) / 128 * 128);
     const int stride = 1 << ((int)std::log2((double)c.nchan) / 2);
     size_t off = 0;
+    const size_t o_err = off;     off = align256(off + sizeof(int));
     const size_t o_model = off;   off = align256(off + 4 * sizeof(double) * c.nant);
     const size_t o_sblo = off;    off = align256(off + sizeof(double) * c.nsubband);
     const size_t o_csub = off;    off = align256(off + sizeof(float) * stride);
@@ -147,6 +168,7 @@ extern "C" int fxc_correlate_noalloc(const fxc_config* cfg, const uint8_t* d_dat
     NA_CK(cudaMemcpyAsync(scratch + o_sblo, sblo.data(), sblo.size() * sizeof(double), cudaMemcpyHostToDevice, st));
     NA_CK(cudaMemcpyAsync(scratch + o_csub, csub.data(), csub.size() * sizeof(float), cudaMemcpyHostToDevice, st));
     NA_CK(cudaMemcpyAsync(scratch + o_cstep, cstep.data(), cstep.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+    NA_CK(cudaMemsetAsync(scratch + o_err, 0, sizeof(int), st));
     NA_CK(cudaMemsetAsync(scratch + o_counts, 0, sizeof(int) * npair_ant, st));
     NA_CK(cudaMemsetAsync(scratch + o_acc, 0, sizeof(float2) * (size_t)c.nsubband * npair * c.nchan, st));
     NA_CK(cudaMemsetAsync(scratch + o_spec, 0, per_slot * T, st));
@@ -174,6 +196,7 @@ extern "C" int fxc_correlate_noalloc(const fxc_config* cfg, const uint8_t* d_dat
     fa.chan_step = reinterpret_cast<const float*>(scratch + o_cstep);
     fa.spec = scratch + o_spec;
     fa.T = (int)T;
+    fa.err = reinterpret_cast<int*>(scratch + o_err);
     XArgs xa{};
     xa.spec = scratch + o_spec;
     xa.acc = d_acc;
@@ -190,9 +213,13 @@ extern "C" int fxc_correlate_noalloc(const fxc_config* cfg, const uint8_t* d_dat
     }
     NA_CK(launch_finalize(d_acc, 0, nsig, c.npol, c.nant, c.nchan, c.nsubband, d_pc, normalize,
                           reinterpret_cast<float2*>(d_vis), st));
+    const int nout = c.nant * (c.nant - 1) / 2 + c.nant;
     if (d_counts) {
-        k_counts_to_output<<<(c.nant * (c.nant + 1) / 2 + 255) / 256, 256, 0, st>>>(d_pc, c.nant, d_counts);
+        k_counts_to_output<<<(nout + 255) / 256, 256, 0, st>>>(d_pc, c.nant, d_counts);
         NA_CK(cudaGetLastError());
     }
+    k_noalloc_flag_error<<<148, 256, 0, st>>>(reinterpret_cast<const int*>(scratch + o_err), d_vis,
+                                              2 * fxc_vis_count(cfg), d_counts, nout);
+    NA_CK(cudaGetLastError());
     return FXC_OK;
 }

@@ -61,6 +61,7 @@ struct Smem {
     uint64_t drain;          // final tcgen05.commit: every MMA of this CTA retired
     uint32_t tmem_base;
     int abort;
+    int drain_fail;          // a drain wait expired: copies or MMAs may still be in flight
 };
 
 }  // namespace tc
@@ -113,6 +114,7 @@ k_xtc(const __grid_constant__ CUtensorMap tmap, XArgs a, int* err)
         }
         mbar_init(&sm.drain, 1);
         sm.abort = 0;
+        sm.drain_fail = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -163,6 +165,7 @@ k_xtc(const __grid_constant__ CUtensorMap tmap, XArgs a, int* err)
                 while (!mbar_try(&sm.full[st], ph)) {
                     if (globaltimer() - t0 > WAIT_NS) {
                         atomicCAS(err, 0, 5);
+                        sm.drain_fail = 1;
                         break;
                     }
                 }
@@ -221,6 +224,7 @@ k_xtc(const __grid_constant__ CUtensorMap tmap, XArgs a, int* err)
             while (!mbar_try(fin, 0)) {
                 if (globaltimer() - t0 > WAIT_NS) {
                     atomicCAS(err, 0, 5);
+                    sm.drain_fail = 1;
                     break;
                 }
             }
@@ -282,7 +286,9 @@ k_xtc(const __grid_constant__ CUtensorMap tmap, XArgs a, int* err)
     }
 
     __syncthreads();
-    if (warp == 0) {
+    // after an expired drain, MMAs may still write TMEM: it stays allocated (code 5 was recorded;
+    // the context's later tensor-core launches cannot be trusted and the process should reset)
+    if (warp == 0 && !sm.drain_fail) {
         tc_fence_after();
         tc::tmem_dealloc(tmem, TMEM_COLS);
     }

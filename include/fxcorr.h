@@ -69,7 +69,23 @@ typedef struct fxc_config {
                           > 0 also drops the whole-subintegration device input buffer, so the
                           subintegration never has to fit in device memory (fxc_upload_input and
                           fxc_device_input then return FXC_ERR_UNSUPPORTED) */
+    int fstage;        /* F-stage arithmetic, FXC_F_* (0 = FXC_F_AUTO) */
 } fxc_config;
+
+/* F-stage arithmetic (fxc_config.fstage).  The reference's F stage is an FP32 FFT
+ * (kernel.c:499-510, IPP ippsFFTFwd_CToC_32fc); every choice but FXC_F_TC16 keeps FP32
+ * accuracy.  The X forms read the F stage's output as FP32 (plain) or cast to FP16 / e4m3
+ * (tensor-core forms).
+ *   FXC_F_AUTO   FXC_F_FFT32.
+ *   FXC_F_FFT32  FP32 radix-16 Stockham FFT on the CUDA cores; every geometry and form.
+ *   FXC_F_TC16   FP16 DFT on the tensor cores: the 2048-point FFT as two tcgen05 GEMMs with
+ *                FP16 DFT matrices and an FP16 intermediate (three FP16 roundings inside the
+ *                F stage, spectra RMS error ~2x the FP32 FFT's after the FP16 cast).  Tensor-core
+ *                X forms at 1024 channels, one polarisation, 2-bit real input only
+ *                (FXC_ERR_UNSUPPORTED otherwise). */
+#define FXC_F_AUTO   0
+#define FXC_F_FFT32  1
+#define FXC_F_TC16   2
 
 typedef struct fxc_ctx fxc_ctx;
 
@@ -162,21 +178,22 @@ int fxc_host_free(void* p);
 
 /* One-shot correlation that allocates no memory.  No counterpart in the
  * reference: it is for callers that cannot call cudaMalloc at the point where
- * they correlate -- code inside a CUDA stream capture (allocation is not
- * capturable), real-time paths that must not take the allocator's locks or
- * latency, and hosts whose device memory another framework reserved up front.
- * The caller passes the input (device rows as for fxc_process_device, host
- * delay model) and the outputs it owns: d_vis (fxc_vis_count complex values,
+ * they correlate -- real-time paths that must not take the allocator's locks or
+ * wait on its latency, and hosts whose device memory another framework reserved
+ * up front.  The caller passes the input (device rows as for fxc_process_device,
+ * host delay model) and the outputs it owns: d_vis (fxc_vis_count complex values,
  * layout of fxc_get_visibilities) and optionally d_counts (nbl + nant ints).
  * Every intermediate lives in one static device array of
  * FXC_NOALLOC_SCRATCH_BYTES that each GPU loading this library holds until the
  * process exits; a problem whose delay table, accumulators and at least 64 FFT
  * slots of spectra do not fit returns FXC_ERR_INVALID.  Plain FP32 X stage only
  * (FXC_ERR_UNSUPPORTED otherwise).  Work is queued on `stream` (a cudaStream_t,
- * NULL = legacy default stream); the call returns before it completes.
- * The first call on a device looks up the array's device address, so make it
- * before any stream capture starts.  All calls share the array: calls that
- * overlap on the GPU race, so order them (one stream, or events). */
+ * NULL = legacy default stream); the call returns before it completes, so a
+ * device wait that runs out is reported in the outputs instead: every
+ * visibility NaN and every count -6.  The first call on a device looks up the
+ * array's device address, so make it before any stream capture starts.  All
+ * calls share the array: calls that overlap on the GPU race, so order them (one
+ * stream, or events). */
 #define FXC_NOALLOC_SCRATCH_BYTES (64u << 20)
 int fxc_correlate_noalloc(const fxc_config* cfg, const uint8_t* d_data, size_t pitch, const double* delays,
                           const double* fileoffsets, int first_fft, int nfft, float* d_vis, int* d_counts,

@@ -6,6 +6,9 @@ points exactly the way its host does (main.c:371-441): init_FxKernel ->
 processAntennasAndBaselinePara over split FFT ranges -> merge -> (optionally)
 processNormalize.  The reference always treats input as dual-polarisation
 interleaved (kernel.c:397-426) and needs a square channel count (kernel.c:31-35).
+``hoisted=True`` selects ``oracle/_ref/libfxref_hoisted.so``: the same sources with
+the per-(FFT, antenna) allocKernel call of kernel.c:727-728 moved before the FFT loop
+(``oracle/hoist_allockernel.py``), the secondary CPU baseline.
 """
 from __future__ import annotations
 
@@ -16,19 +19,21 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.path.join(HERE, "_ref", "libfxref.so")
+REF_LIB_HOISTED = os.path.join(HERE, "_ref", "libfxref_hoisted.so")
 REF_CLI = os.path.join(HERE, "_ref", "tests_difx")
 
-_lib = None
+_libs = {}
 
 
-def available() -> bool:
-    return os.path.exists(REF_LIB)
+def available(hoisted=False) -> bool:
+    return os.path.exists(REF_LIB_HOISTED if hoisted else REF_LIB)
 
 
-def lib():
-    global _lib
+def lib(hoisted=False):
+    _lib = _libs.get(hoisted)
     if _lib is None:
-        _lib = C.CDLL(REF_LIB)
+        _lib = C.CDLL(REF_LIB_HOISTED if hoisted else REF_LIB)
+        _libs[hoisted] = _lib
         ip, dp, vp = C.POINTER(C.c_int), C.POINTER(C.c_double), C.c_void_p
         _lib.init_FxKernel.argtypes = [ip, ip, ip, dp, dp, vp, C.c_char_p, ip, dp, ip, ip, ip,
                                        vp, vp, vp, vp, ip, ip, C.c_int]
@@ -49,7 +54,7 @@ def _ptr_array(n):
 
 
 def run_reference(data, delays, fileoffsets, nchan, numffts, bw, lo, split=1, first_fft=0,
-                  nfft=None, normalise=False):
+                  nfft=None, normalise=False, hoisted=False):
     """Run kernel.c on dual-pol packed input.
 
     data: uint8 [nant][subintbytes]; delays [nant][3]; fileoffsets [nant].
@@ -57,7 +62,7 @@ def run_reference(data, delays, fileoffsets, nchan, numffts, bw, lo, split=1, fi
     equal ranges as in main.c:398-408 (numffts = total FFTs of the subint sets
     maxoffset, kernel.c:730).  Returns (vis complex64 [nbl][4][nchan], counts int [nbl]).
     """
-    L = lib()
+    L = lib(hoisted)
     data = np.ascontiguousarray(data, dtype=np.uint8)
     nant = data.shape[0]
     if nfft is None:

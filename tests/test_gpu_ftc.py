@@ -1,9 +1,9 @@
-"""GPU parity of the tensor-core F stage (2048-point FFTs, one polarisation, F16 spectra):
-visibilities against the FP64 oracle at the tensor-core bar, and against the FP32-FFT
-F stage that FXC_TC_FSTAGE=fft selects (FXC_TC_FSTAGE=tc puts the FP8 form, which by
-default uses the FFT kernel, on the tensor-core one).  Work items are 16 FFTs of one (subband,
-antenna); the cases cover partial items (nfft not a multiple of 16), several subbands,
-FFTs without data at the subintegration's edges and many items per CTA."""
+"""GPU parity of the FP16 tensor-core F stage (fxc_config.fstage = FXC_F_TC16; 2048-point
+FFTs, one polarisation, F16 spectra): visibilities against the FP64 oracle at the tensor-core
+bar, and against the FP32-FFT F stage (FXC_F_FFT32, the tensor-core forms' default).  Work
+items are 16 FFTs of one (subband, antenna); the cases cover partial items (nfft not a multiple
+of 16), several subbands, FFTs without data at the subintegration's edges and many items per
+CTA."""
 import numpy as np
 import pytest
 
@@ -23,12 +23,8 @@ def corr_for(job, **kw):
     return fx.Correlator(cfg)
 
 
-def run(job, monkeypatch, fstage=None, **kw):
-    if fstage:
-        monkeypatch.setenv("FXC_TC_FSTAGE", fstage)
-    else:
-        monkeypatch.delenv("FXC_TC_FSTAGE", raising=False)
-    with corr_for(job, **kw) as c:
+def run(job, monkeypatch, fstage=fx.FXC_F_TC16, **kw):
+    with corr_for(job, fstage=fstage, **kw) as c:
         c.process(job.data, job.delays, job.fileoffsets)
         return c.visibilities()
 
@@ -53,7 +49,7 @@ def test_tc_fstage_vs_fp64_oracle(nant, nsb, numffts, seed, monkeypatch):
 def test_tc_fstage_matches_fft_fstage(monkeypatch):
     job = synth.make_job(nant=24, npol=1, nchan=1024, numffts=300, bw=64e6, lo=1.4e9, rho=0.1, seed=5)
     v_tc, c_tc = run(job, monkeypatch, xmode=fx.FXC_X_TC_FP16)
-    v_fft, c_fft = run(job, monkeypatch, fstage="fft", xmode=fx.FXC_X_TC_FP16)
+    v_fft, c_fft = run(job, monkeypatch, fstage=fx.FXC_F_FFT32, xmode=fx.FXC_X_TC_FP16)
     np.testing.assert_array_equal(c_tc, c_fft)
     mx, rms = fo.vis_error(v_tc[0], v_fft[0])
     assert rms.max() < TC_RMS_TOL and mx.max() < TC_MAX_TOL, f"rms {rms.max():.3e} max {mx.max():.3e}"
@@ -76,8 +72,8 @@ def test_tc_fstage_edge_ffts_without_data(monkeypatch):
 
 def test_tc_fstage_fp8_form(monkeypatch):
     job = synth.make_job(nant=20, npol=1, nchan=1024, numffts=256, bw=64e6, lo=1.4e9, rho=0.1, seed=13)
-    v8, c8 = run(job, monkeypatch, fstage="tc", xmode=fx.FXC_X_TC_FP8)
-    v8f, c8f = run(job, monkeypatch, fstage="fft", xmode=fx.FXC_X_TC_FP8)
+    v8, c8 = run(job, monkeypatch, fstage=fx.FXC_F_TC16, xmode=fx.FXC_X_TC_FP8)
+    v8f, c8f = run(job, monkeypatch, fstage=fx.FXC_F_FFT32, xmode=fx.FXC_X_TC_FP8)
     np.testing.assert_array_equal(c8, c8f)
     # the two F stages differ by FP16 rounding; the e4m3 quantisation of both dominates
     mx, rms = fo.vis_error(v8[0], v8f[0])
@@ -87,9 +83,8 @@ def test_tc_fstage_fp8_form(monkeypatch):
 def test_tc_fstage_host_windows_equal_whole_device_input(monkeypatch):
     """Input streamed from the host through the three device windows gives exactly what the
     whole-subintegration device input gives (windows coincide with the spectra chunks)."""
-    monkeypatch.delenv("FXC_TC_FSTAGE", raising=False)
     job = synth.make_job(nant=6, npol=1, nchan=1024, numffts=400, bw=64e6, lo=1.4e9, rho=0.1, seed=15, nsubband=2)
-    with corr_for(job, xmode=fx.FXC_X_TC_FP16, chunk_ffts=128) as c:
+    with corr_for(job, fstage=fx.FXC_F_TC16, xmode=fx.FXC_X_TC_FP16, chunk_ffts=128) as c:
         c.upload(job.data)
         dptr, pitch = c.device_input()
         c.process_device(dptr, pitch, job.delays, job.fileoffsets)
@@ -102,10 +97,9 @@ def test_tc_fstage_host_windows_equal_whole_device_input(monkeypatch):
 
 
 def test_tc_fstage_window_only_context_vs_oracle(monkeypatch):
-    monkeypatch.delenv("FXC_TC_FSTAGE", raising=False)
     job = synth.make_job(nant=5, npol=1, nchan=1024, numffts=300, bw=64e6, lo=1.4e9, rho=0.1, seed=17)
     job.fileoffsets[2] -= 20.3 * 2 * job.nchan / (2 * job.bw)   # its first FFTs have no data
-    with corr_for(job, xmode=fx.FXC_X_TC_FP16, chunk_ffts=128, window_ffts=70) as c:
+    with corr_for(job, fstage=fx.FXC_F_TC16, xmode=fx.FXC_X_TC_FP16, chunk_ffts=128, window_ffts=70) as c:
         c.process_window(job.data, job.delays, job.fileoffsets, 11, 250)
         vis, counts = c.visibilities()
     ref, rc = fo.correlate(job.data[0], job.delays, job.fileoffsets, job.bw, job.lo, job.nchan, job.npol,
@@ -117,7 +111,6 @@ def test_tc_fstage_window_only_context_vs_oracle(monkeypatch):
 
 def test_tc_fstage_subband_groups(monkeypatch):
     """A spectra budget too small for every subband: chunks over groups of subbands."""
-    monkeypatch.delenv("FXC_TC_FSTAGE", raising=False)
     monkeypatch.setenv("FXC_SPECTRA_BUDGET_MB", "2")
     job = synth.make_job(nant=8, npol=1, nchan=1024, numffts=300, bw=64e6, lo=1.4e9, rho=0.1, seed=19, nsubband=3)
     vis, counts = run(job, monkeypatch, xmode=fx.FXC_X_TC_FP16)
@@ -134,9 +127,8 @@ def test_tensor_core_wait_expiry_is_reported_and_context_survives(monkeypatch):
     completes, comes back as FXC_ERR_TIMEOUT with code 7; the next tensor-core correlation on
     the same context is correct."""
     import ctypes as C
-    monkeypatch.delenv("FXC_TC_FSTAGE", raising=False)
     job = synth.make_job(nant=6, npol=1, nchan=1024, numffts=64, bw=64e6, lo=1.4e9, rho=0.1, seed=23)
-    with corr_for(job, xmode=fx.FXC_X_TC_FP16) as c:
+    with corr_for(job, fstage=fx.FXC_F_TC16, xmode=fx.FXC_X_TC_FP16) as c:
         assert fx.lib().fxc_debug_expire_wait_tc(C.c_void_p(c.handle.value)) == fx.FXC_OK
         with pytest.raises(fx.FxcError) as e:
             c.synchronize()

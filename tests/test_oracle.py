@@ -5,6 +5,8 @@ reference kernel.c built against the IPP stand-in) pin the oracle everywhere;
 when oracle/_ref is present the oracle is also compared with the reference live
 on fresh seeded inputs.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -12,6 +14,7 @@ from difx_tests_b200 import synth
 from oracle import fxoracle as fo
 from oracle import refcall
 
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 needs_ref = pytest.mark.skipif(not refcall.available(), reason="oracle/_ref (reference build) not present")
 
 
@@ -89,6 +92,34 @@ def test_end_to_end_vs_reference_live(nchan, numffts, split):
     np.testing.assert_array_equal(co[:6], cr)
     mx, _ = fo.vis_error(vr, vo[:6])
     assert mx.max() < 1e-5
+
+
+@pytest.mark.skipif(not refcall.available(hoisted=True), reason="oracle/_ref (reference build) not present")
+def test_hoisted_allockernel_variant_is_bit_identical():
+    """The secondary CPU baseline (kernel.c with allocKernel moved out of the FFT x antenna
+    loop, kernel.c:727-728) computes exactly what the as-written reference computes."""
+    job = synth.make_job(nant=4, npol=2, nchan=256, numffts=24, bw=32e6, lo=1.4e9, rho=0.1, seed=77)
+    va, ca = refcall.run_reference(job.data[0], job.delays, job.fileoffsets, 256, 24, 32e6, 1.4e9, split=2)
+    vh, ch = refcall.run_reference(job.data[0], job.delays, job.fileoffsets, 256, 24, 32e6, 1.4e9, split=2,
+                                   hoisted=True)
+    np.testing.assert_array_equal(ca, ch)
+    np.testing.assert_array_equal(va, vh)
+
+
+def test_hoist_script_moves_exactly_the_per_iteration_alloc():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("hoist", os.path.join(REPO, "oracle", "hoist_allockernel.py"))
+    h = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(h)
+    src = ("void processAntennasAndBaselinePara(int *n) {\n    int netdelaysamples, offset;\n"
+           "    for (k = 0; k < 2; k++) {\n        for (j = 0; j < 2; j++) {\n            FxKernel kernel;\n"
+           "            allocKernel(&kernel, a, b);\n            use(&kernel);\n        }\n    }\n}\n"
+           "\nvoid processBaselinePara(int *n) {}\n")
+    out = h.hoist(src)
+    assert out.count("allocKernel(&kernel") == 1
+    assert out.index("allocKernel(&kernel") < out.index("for (k = 0")
+    with pytest.raises(SystemExit):
+        h.hoist(src.replace("allocKernel(&kernel, a, b);", ""))
 
 
 def test_normalise_matches_reference_semantics():
