@@ -357,17 +357,22 @@ FSTAGE_DRAM_BYTES_PER_SAMPLE = {(1, True): 2.17, (1, False): 4.16, (2, True): 2.
 FORMS = {"plain": (0, 1),     # FXC_X_PLAIN_FP32, FXC_F_FFT32
          "tc": (1, 1),        # FXC_X_TC_FP16 on the FP32 FFT F stage (the headline form)
          "tc16f": (1, 2),     # FXC_X_TC_FP16 on the FP16 tensor-core F stage (FXC_F_TC16)
+         "tc32f": (1, 3),     # FXC_X_TC_FP16 on the FP32-grade tensor-core F stage (FXC_F_TC32)
          "fp8": (2, 1)}       # FXC_X_TC_FP8 on the FP32 FFT F stage
 XMODES = {k: v[0] for k, v in FORMS.items()}
 DTYPES = {"plain": "f32 (FFT F stage and X stage on the CUDA cores)",
           "tc": "f32 FFT F stage (CUDA cores), spectra cast to f16 for the tensor-core X stage, f32 accumulate",
           "tc16f": "f16 tensor-core F stage (k_ftc: f16 DFT matrices and intermediate), f16 X inputs, "
                    "f32 accumulate",
+          "tc32f": "f32-grade tensor-core F stage (k_ftc32: f16 hi+lo operand pairs, three products per GEMM, "
+                   "f32 accumulate), spectra cast to f16 for the tensor-core X stage, f32 accumulate",
           "fp8": "f32 FFT F stage (CUDA cores), spectra cast to e4m3 scaled per signal and channel for the "
                  "tensor-core X stage, f32 accumulate"}
 F_KERNELS = {1: "k_fstage (fused unpack/shift/fringe/FFT/frac-delay, FP32 radix-16 FFT on the CUDA cores)",
              2: "k_ftc (tcgen05 F stage: unpack/fringe, 32x64 DFT as two FP16 tensor-core GEMMs, twiddles, "
-                "frac-delay, F16 store)"}
+                "frac-delay, F16 store)",
+             3: "k_ftc32 (tcgen05 F stage, FP32-grade: 32x64 DFT as two tensor-core GEMMs on FP16 hi+lo pairs, "
+                "three products each, twiddles, frac-delay)"}
 
 
 def time_form(torch, dist, fx, w, form, data, pitch, delays, offs, steps, warmup, world, dev, stream):
@@ -451,15 +456,22 @@ def run_gpu_arm(args):
                            device=dev)
     torch.cuda.synchronize()
 
-    forms = {"all": ["tc", "tc16f", "fp8", "plain"], "both": ["tc", "plain"]}.get(args.xmode, [args.xmode])
-    if w["nchan"] != 1024 or w["npol"] != 1:
-        forms = [f for f in forms if f != "tc16f"]   # the FP16 tensor-core F stage covers 1024 ch x 1 pol only
-    res = {}
+    forms = {"all": ["tc", "tc32f", "tc16f", "fp8", "plain"], "both": ["tc", "plain"]}.get(args.xmode, [args.xmode])
+    if w["nchan"] != 1024 or w["npol"] != 1:   # the tensor-core F stages cover 1024 ch x 1 pol only
+        forms = [f for f in forms if f not in ("tc16f", "tc32f")]
+    res, failed = {}, {}
     for form in forms:
-        res[form] = time_form(torch, dist, fx, w, form, data, pitch, delays, offs, args.steps, args.warmup, world, dev,
-                              stream)
+        try:
+            res[form] = time_form(torch, dist, fx, w, form, data, pitch, delays, offs, args.steps, args.warmup, world,
+                                  dev, stream)
+        except fx.FxcError as e:
+            if form == forms[0]:
+                raise
+            failed[form] = str(e)      # recorded in the line; the other forms still run
+            continue
         if form != forms[0]:
             res[form]["corr"].close()
+    forms = [f for f in forms if f in res]
     head = res[forms[0]]
     xmode, fstage = FORMS[forms[0]]
 
@@ -479,7 +491,7 @@ def run_gpu_arm(args):
             "algorithmic_bytes_per_launch": f_bytes, "launch_ms": head["f_ms_launch"],
             "share": sm[1] / max(1e-9, sm.sum()),
             "note": ("latency-bound warp-specialised pipeline; HBM fraction shown for its algorithmic bytes"
-                     if fstage == 2 else
+                     if fstage in (2, 3) else
                      "FP32 FFT is issue-bound on the CUDA cores; HBM fraction shown for its algorithmic bytes")}
 
     line = {
@@ -509,7 +521,7 @@ def run_gpu_arm(args):
         line["tc_vs_plain"] = {"gsamps": head["value"] / p["value"],
                                "x_stage_only": (p["stage_ms"][2] / max(1e-9, sm[2])),
                                "form": forms[0]}
-        for f in ("tc16f", "fp8"):
+        for f in ("tc", "tc32f", "tc16f", "fp8"):
             if f in res and f != forms[0]:
                 line[f + "_vs_plain"] = {"gsamps": res[f]["value"] / p["value"],
                                          "x_stage_only": p["stage_ms"][2] / max(1e-9, res[f]["stage_ms"][2])}
@@ -546,6 +558,8 @@ def run_gpu_arm(args):
                        "steps": e2e_steps, "ms_per_step": 1e3 * t_max,
                        "path": "fxc_process_host + fxc_get_visibilities, pinned host input and output buffers"}
 
+    for f, msg in failed.items():
+        line[f] = {"error": msg}
     if rank == 0 and not args.no_accuracy:
         line["accuracy"] = {f: accuracy_sample(w, *FORMS[f]) for f in forms}
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -554,6 +568,18 @@ def run_gpu_arm(args):
         if cb is not None:
             line["cpu_baseline"] = cb
     corr.close()
+    if rank == 0 and world == 1 and args.workload == "cfg2" and not args.no_extra:
+        # bounded runs of the batched (cfg3) and large-array (cfg4) workloads, each with its own
+        # clocks and accuracy, recorded beside the headline
+        del data, res, head
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        sub = argparse.Namespace(**vars(args))
+        sub.steps, sub.warmup = 3, 3
+        line["cfg3"] = run_batch_arm(sub, emit=False)
+        torch.cuda.empty_cache()
+        sub.steps, sub.warmup = 2, 1
+        line["cfg4"] = run_large_arm(sub, emit=False, max_windows=2)
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
@@ -562,9 +588,10 @@ def run_gpu_arm(args):
     return 0
 
 
-def run_batch_arm(args):
+def run_batch_arm(args, emit=True):
     """12 uneven jobs through fxc_batch_* (grouped persistent launches, CUDA graph replay,
-    autotuned plans) against the same jobs run one after another through the single-job path."""
+    autotuned plans) against the same jobs run one after another through the single-job path.
+    Returns the result line (printed when emit)."""
     import torch
 
     import difx_tests_b200 as fx
@@ -659,8 +686,9 @@ def run_batch_arm(args):
         "clocks": clk,
         "gpu_launches": launches * args.steps,
     }
-    print(json.dumps(line))
-    return 0
+    if emit:
+        print(json.dumps(line))
+    return line
 
 
 # Large array: 256 antennas x 2 polarisations (512 signals) x 16 subbands x 4096 channels,
@@ -697,7 +725,9 @@ def large_subset_accuracy(xmode, nsub=16, nf=64):
             "counts_match": bool(np.array_equal(counts[rows], rc))}
 
 
-def run_large_arm(args):
+def run_large_arm(args, emit=True, max_windows=None):
+    """The large array streamed through device windows; max_windows bounds the sample (the first
+    windows of the subintegration).  Returns the result line (printed when emit)."""
     import torch
 
     import difx_tests_b200 as fx
@@ -721,6 +751,8 @@ def run_large_arm(args):
     torch.cuda.synchronize()
     gen_s = time.perf_counter() - t0
     windows = [(w0, min(W, L["numffts"] - w0)) for w0 in range(0, L["numffts"], W)]
+    if max_windows:
+        windows = windows[:max_windows]
 
     def run(corr, wins):
         corr.reset()
@@ -770,7 +802,9 @@ def run_large_arm(args):
         "dtype": DTYPES["tc"], "data": "synthetic (seeded, generated on device; one window reused for every window)",
         "config": {"workload": "256 ant x 2 pol x 16 subbands x 4096 ch, 1 s @ 128 MS/s (15625 FFTs/subband), "
                                f"streamed in windows of {W} FFTs", "form": "tc",
-                   "l2": "262 GB of input per step, far above L2; no flush"},
+                   "l2": "262 GB of input per step, far above L2; no flush",
+                   "sample": (f"first {len(windows)} of {-(-L['numffts'] // W)} windows per step"
+                              if max_windows else "whole subintegration per step")},
         "stages_ms_per_step": {"delay+counts": tc["stage_ms"][0], "F": tc["stage_ms"][1], "X": tc["stage_ms"][2]},
         "x_stage": {"tflops": tc["x_tflops"], "flop_per_step": tc["xflop"], "peak_tflops": tc_peak,
                     "frac": tc["x_tflops"] / tc_peak,
@@ -791,8 +825,9 @@ def run_large_arm(args):
     torch.cuda.empty_cache()
     if not args.no_accuracy:
         line["accuracy"] = {"tc": large_subset_accuracy(fx.FXC_X_TC_FP16)}
-    print(json.dumps(line))
-    return 0
+    if emit:
+        print(json.dumps(line))
+    return line
 
 
 def main():
@@ -811,15 +846,19 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the bounded cfg3 (batch) and cfg4 (large array) runs of the default workload")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
     if args.workload == "cfg3":
-        return run_batch_arm(args)
+        run_batch_arm(args)
+        return 0
     if args.workload == "cfg4":
-        return run_large_arm(args)
+        run_large_arm(args)
+        return 0
     return run_gpu_arm(args)
 
 

@@ -33,6 +33,7 @@ FXC_X_TC_FP8 = 2
 FXC_F_AUTO = 0
 FXC_F_FFT32 = 1
 FXC_F_TC16 = 2
+FXC_F_TC32 = 3
 
 
 class FxcConfig(C.Structure):

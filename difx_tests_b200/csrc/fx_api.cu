@@ -134,9 +134,12 @@ static int validate(const fxc_config* c)
     // plain X: 8x8 register tiles, one CTA per channel group (<= 64 signals) or per pair of
     // 64-signal super-blocks; tensor-core X: 128x128 block pairs of the Gram
     if (c->nant * c->npol > 512) return FXC_ERR_UNSUPPORTED;
-    if (c->fstage < FXC_F_AUTO || c->fstage > FXC_F_TC16) return FXC_ERR_INVALID;
+    if (c->fstage < FXC_F_AUTO || c->fstage > FXC_F_TC32) return FXC_ERR_INVALID;
     if (c->fstage == FXC_F_TC16 &&
         !(c->xmode != FXC_X_PLAIN_FP32 && c->nchan == 1024 && c->npol == 1 && !c->iscomplex))
+        return FXC_ERR_UNSUPPORTED;
+    if (c->fstage == FXC_F_TC32 &&
+        !(c->xmode != FXC_X_TC_FP8 && c->nchan == 1024 && c->npol == 1 && !c->iscomplex))
         return FXC_ERR_UNSUPPORTED;
     return FXC_OK;
 }
@@ -1047,6 +1050,7 @@ int fxc_debug_spectra(fxc_ctx* x, const double* delays, const double* offs, int 
     fa.nfft = nfft;
     fa.T = T;
     fa.spec = d;
+    if (fa.fkind == FXC_F_TC16) fa.fkind = FXC_F_FFT32;   // the FP16 tensor-core DFT has no FP32 output
     cudaError_t e = launch_fstage(c.nchan, kSpecF32, fa, x->stream);
     for (int r = 0; e == cudaSuccess && r < c.nsubband * x->nsig; r++)
         e = cudaMemcpyAsync(out + (size_t)r * nfft * c.nchan * 2, d + (size_t)r * T * c.nchan,

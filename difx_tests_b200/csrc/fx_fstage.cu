@@ -37,6 +37,10 @@ cudaError_t launch_fstage(int nchan, int mode, const FArgs& a, cudaStream_t st)
         if (!ftc_supported(nchan, mode, a)) return cudaErrorInvalidValue;
         return launch_ftc(a, st);
     }
+    if (a.fkind == FXC_F_TC32) {
+        if (!ftc32_supported(nchan, a)) return cudaErrorInvalidValue;
+        return launch_ftc32(mode, a, st);
+    }
     switch (a.cpx ? nchan : 2 * nchan) {   // FFT length: complex samples fill every bin
     case 256: return launch_fstage_256(mode, a, st);
     case 512: return launch_fstage_512(mode, a, st);

@@ -26,11 +26,12 @@
 // accuracy); the FP8 form's absmax lands on the output warps, this kernel's busiest role.
 // Every wait is bounded (1 s): on expiry the CTA records code 7 in the error word, stops,
 // drains what it issued and frees TMEM.
-#include "fx_fstage.cuh"
-#include "fx_tc.cuh"
+#include "fx_ftc_common.cuh"
 
 namespace fx {
 namespace ftc {
+
+using namespace ftcc;
 
 using P = FPlan<2048>;
 constexpr int F = 2048;
@@ -44,14 +45,12 @@ constexpr int NPAIR = TB / 2;             // A1 stages per item
 constexpr int NA1 = 3;                    // A1 ring
 constexpr int ND1 = 4;                    // D1 ring (64 TMEM columns each)
 constexpr int NTHREADS = 448;             // 14 warps
-constexpr int INB = 544;                  // staged bytes per FFT: the window plus read-ahead
 constexpr int NIB = 4;                    // pair slots the helper fills ahead of the producer
 constexpr int NROT = F2 + F1;             // fringe sub[64] | step[32] per FFT
 constexpr uint32_t TMEM_COLS = 512;
 constexpr uint32_t D2_COL = ND1 * 64;     // D2: 4 tiles x 64 columns
 constexpr int ERR_WAIT = 7;
 constexpr uint32_t kIdesc = tc::idesc_f16(128, 64);
-static_assert(fstage_inb<2048, 1, false>() + 16 <= INB, "staging buffer holds the window and read-ahead");
 
 struct Smem {
     alignas(1024) uint8_t a2[4][2][128 * 128];   // [k1 / 8][K half][row (k1 % 8) * 16 + b]
@@ -79,64 +78,6 @@ static_assert(sizeof(Smem) + 1024 <= 232448, "fits the opt-in shared memory of o
 // land in eight different rows mod 8, so its 16-byte stores hit eight different bank groups
 __device__ __forceinline__ int a1_row(int b, int o, int i2) { return b * 64 + 8 * i2 + (o & 7) + 32 * (o >> 3); }
 
-// 16-byte chunk c of row r of a K-major SWIZZLE_128B tile
-__device__ __forceinline__ uint32_t sw128(int r, int c) { return (uint32_t)(r * 128 + ((c ^ (r & 7)) << 4)); }
-
-__device__ __forceinline__ bool bar_or(int id, int n, bool p)
-{
-    uint32_t r;
-    asm volatile(
-        "{\n\t.reg .pred pi, po;\n\t"
-        "setp.ne.u32 pi, %1, 0;\n\t"
-        "bar.red.or.pred po, %2, %3, pi;\n\t"
-        "selp.u32 %0, 1, 0, po;\n\t}"
-        : "=r"(r)
-        : "r"((uint32_t)p), "r"(id), "r"(n)
-        : "memory");
-    return r != 0;
-}
-
-__device__ __forceinline__ uint32_t h2u(__half2 h) { return *reinterpret_cast<uint32_t*>(&h); }
-
-struct Item {
-    int sb, ant, tb0;
-};
-
-__device__ __forceinline__ Item item_of(int task, int nant, int ntb)
-{
-    Item it;
-    it.tb0 = (task % ntb) * TB;
-    const int r = task / ntb;
-    it.ant = r % nant;
-    it.sb = r / nant;
-    return it;
-}
-
-// delay entry of FFT slot tc of antenna ant; valid only for FFTs that carry data
-__device__ __forceinline__ bool entry(const FArgs& a, int ant, int tc, DelayEntry& d)
-{
-    if (tc >= a.nfft) return false;
-    d = a.dtab[(size_t)ant * a.ld + a.t_base + tc];
-    return d.valid != 0;
-}
-
-__device__ __forceinline__ void bulk_copy(uint64_t* bar, void* dst, const void* src, uint32_t bytes)
-{
-    size_t gsrc;
-    asm volatile("cvta.to.global.u64 %0, %1;" : "=l"(gsrc) : "l"(src));
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                 ::"r"(tc::smem_u32(dst)), "l"(gsrc), "r"(bytes), "r"(tc::smem_u32(bar))
-                 : "memory");
-}
-
-// Input window of an FFT (2-bit real, one polarisation): 16-byte aligned base byte and vectors
-__device__ __forceinline__ void window(const DelayEntry& d, int& base, int& nvec)
-{
-    const int first = d.offset >> 2;
-    base = first & ~15;
-    nvec = (F / 4 + 1 + (first - base) + 15) >> 4;
-}
-
 // (cos, sin)(pi x) by the special-function unit
 __device__ __forceinline__ float2 cis_half_turns(float x)
 {
@@ -151,29 +92,6 @@ __device__ __forceinline__ float2 frac_rot(int j, const DelayEntry& d, const flo
     float sn, cs;
     __sincosf(__fmul_rn(ctab[j], __double2float_rn(d.frac)), &sn, &cs);
     return make_float2(cs, sn);
-}
-
-// Delay entry of FFT t of item i of this CTA (valid = 0 for slots without data)
-__device__ __forceinline__ DelayEntry item_entry(const FArgs& a, int i, int ntb, int t)
-{
-    const Item it = item_of(blockIdx.x + i * gridDim.x, a.nant, ntb);
-    DelayEntry d{};   // slots without data: all zero
-    if (!entry(a, it.ant, it.tb0 + t, d)) d.valid = 0;
-    return d;
-}
-
-// Input bytes of the two FFTs of a pair (entries d0, d1 of subband/antenna row `row`) into pair
-// slot x, by one thread: one arrive.expect_tx for both, then the copies.
-__device__ __forceinline__ void issue_pair(Smem& sm, int x, const uint8_t* row, const DelayEntry& d0,
-                                           const DelayEntry& d1)
-{
-    int base[2] = {0, 0}, nvec[2] = {0, 0};
-    if (d0.valid) window(d0, base[0], nvec[0]);
-    if (d1.valid) window(d1, base[1], nvec[1]);
-    // the producers' earlier reads of this slot are ordered before the copy by tab_empty
-    tc::mbar_expect_tx(&sm.cp_full[x], 16u * (nvec[0] + nvec[1]));
-    if (d0.valid) bulk_copy(&sm.cp_full[x], sm.inb[x][0], row + base[0], 16u * nvec[0]);
-    if (d1.valid) bulk_copy(&sm.cp_full[x], sm.inb[x][1], row + base[1], 16u * nvec[1]);
 }
 
 template <bool AMAX>
@@ -371,11 +289,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc(FArgs a)
         // item i's entries are in oent[i & 1] before the item's first barrier (written after the
         // previous item's second barrier, loaded into registers one item earlier)
         DelayEntry dnext;
-        if (to < TB && nitem > 0) sm.oent[0][to] = item_entry(a, 0, ntb, to);
-        if (to < TB && nitem > 1) dnext = item_entry(a, 1, ntb, to);
+        if (to < TB && nitem > 0) sm.oent[0][to] = item_entry<TB>(a, 0, ntb, to);
+        if (to < TB && nitem > 1) dnext = item_entry<TB>(a, 1, ntb, to);
         bool ok = true;
         for (int i = 0; i < nitem; i++) {
-            const Item it = item_of(blockIdx.x + i * gridDim.x, a.nant, ntb);
+            const Item it = item_of<TB>(blockIdx.x + i * gridDim.x, a.nant, ntb);
             // item i's entries visible; every thread is done with item i - 1's tables
             if (bar_or(2, 128, !ok || *abort_flag)) break;
 #pragma unroll
@@ -393,7 +311,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc(FArgs a)
             if (bar_or(2, 128, !ok || *abort_flag)) break;
             if (i + 1 < nitem) {
                 if (to < TB) sm.oent[(i + 1) & 1][to] = dnext;
-                if (to < TB && i + 2 < nitem) dnext = item_entry(a, i + 2, ntb, to);
+                if (to < TB && i + 2 < nitem) dnext = item_entry<TB>(a, i + 2, ntb, to);
             }
             if (!__all_sync(0xffffffffu, mbar_wait(&sm.d2_full, i & 1, abort_flag))) {
                 ok = false;
@@ -460,9 +378,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc(FArgs a)
         const uint8_t* rown = nullptr;
         auto fetch = [&](int g, DelayEntry& d0, DelayEntry& d1, double& lo, const uint8_t*& row) {
             const int i = g / NPAIR, p = g % NPAIR;
-            d0 = item_entry(a, i, ntb, 2 * p);
-            d1 = item_entry(a, i, ntb, 2 * p + 1);
-            const Item it = item_of(blockIdx.x + i * gridDim.x, a.nant, ntb);
+            d0 = item_entry<TB>(a, i, ntb, 2 * p);
+            d1 = item_entry<TB>(a, i, ntb, 2 * p + 1);
+            const Item it = item_of<TB>(blockIdx.x + i * gridDim.x, a.nant, ntb);
             lo = a.sb_lo[it.sb];
             row = a.data + ((size_t)it.sb * a.nant + it.ant) * a.pitch;
         };
@@ -480,7 +398,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc(FArgs a)
                 break;
             }
             if (lane == 0) {
-                issue_pair(sm, x, row, d0, d1);
+                issue_pair(&sm.cp_full[x], sm.inb[x][0], sm.inb[x][1], row, d0, d1);
                 issued = g;
             }
             const double lofrac = lo - trunc(lo);
@@ -501,11 +419,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc(FArgs a)
                 const double phs = (double)(lane * F1) * slope;
                 sm.rtab[x][b][F2 + lane] = d.valid ? cis_half_turns((float)(-2.0 * (phs - trunc(phs))))
                                                    : make_float2(0.f, 0.f);
-                if (lane == b) {
-                    int base = 0, nvec = 0;
-                    if (d.valid) window(d, base, nvec);
-                    sm.pwin[x][b] = make_int2(2 * (d.offset - 4 * base), d.valid);
-                }
+                if (lane == b) sm.pwin[x][b] = window_bits(d);
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(&sm.tab_full[x]);

@@ -1,0 +1,563 @@
+// fx_ftc32.cu -- FP32-grade tensor-core F stage for 2048-point FFTs (1024 channels) of one
+// polarisation of 2-bit real input.
+//
+// The same 32 x 64 split of the DFT as the FP16 tensor-core F stage (fx_ftc.cu), along the
+// factorisation the reference's rotators use (kernel.c:31-36, 160-165), with sample
+// n = 64 n1 + n2 and channel k = k1 + 32 k2:
+//   X[k1 + 32 k2] = fstep[k2] sum_n2 W64^(n2 k2) [sub[n2] W2048^(n2 k1) fsub[k1]] sum_n1 W32^(n1 k1) x[n]
+// with x[n] = level(n) step[n1] (the fringe rotator is sub[n2] step[n1], kernel.c:428-497, and
+// the fractional-sample rotator of channel k is fsub[k1] fstep[k2], kernel.c:512-555).  Every
+// FP16 operand is an error-compensated pair hi + lo (hi = FP16 rounding of the FP32 value,
+// lo = FP16 rounding of the remainder) and each GEMM accumulates the three products
+// hi.hi + lo.hi + hi.lo in FP32 TMEM: the spectra carry FP32-level error (~2e-7 of max|X|),
+// not FP16-level (~3e-4).
+//   step 1   D1[(b, n2)][(k1, re|im)] = A1 . B1^T, A1 = x in TMEM, M128 N64 K64, x3 products
+//            (A1 comes from a per-(FFT, n1) table of the four levels times step[n1]: exact pairs)
+//   twiddle  Z = D1 * sub[n2] W2048^(n2 k1) fsub[k1] on the CUDA cores (FP32; the factor is
+//            e^{i alpha k1} times sub[n2], a complex recurrence over k1 restarted at k1 = 16)
+//   step 2   D2[(k1 % 16, b)][(k2, re|im)] = A2 . B2^T, A2 = Z in shared memory, M128 N64 K128,
+//            x3 products, k2 < 32 (channels < 1024)
+//   output   X = D2 * fstep[k2] -> FP16 K-major spectra (tensor-core X forms) or FP32
+//            channel-contiguous spectra (plain form and the spectra check)
+// b = the FFT within a work item of 8 consecutive FFTs of one (subband, antenna).
+//
+// Persistent, warp-specialised CTA (one per SM, 576 threads):
+//   warps 0-3    producer: 2-bit codes -> table lookups -> A1 pairs (TMEM, two stages)
+//   warps 4-11   twiddle: D1 (TMEM, one slot per pair of the item) -> Z pairs -> A2 (shared);
+//                tile 0 (k1 < 16) for the item's four pairs, then tile 1, so the step-2 MMAs
+//                of one tile run while the other is written
+//   warps 12-15  output: D2 (TMEM, one slot per tile) -> fstep -> spectra
+//   warp 16      MMA issuer (one thread), TMEM owner
+//   warp 17      helper: up to four pairs ahead, the input bulk copies, the level x step tables
+//                and the window offsets
+// Every wait is bounded (1 s): on expiry the CTA records code 7 in the error word, stops,
+// drains what it issued and frees TMEM (or keeps it allocated if the drain itself expires).
+#include "fx_ftc_common.cuh"
+
+namespace fx {
+namespace ftc32 {
+
+using namespace ftcc;
+using P = FPlan<2048>;
+constexpr int C = P::C;                   // 1024 channels
+constexpr int F1 = P::STRIDE;             // 32: n1, k1
+constexpr int F2 = P::S;                  // 64: n2
+constexpr int K2H = C / F1;               // 32: k2 of the kept channels
+static_assert(F1 == 32 && F2 == 64 && K2H == 32 && P::FS == F1 && P::FST == K2H, "2048-point split");
+constexpr int TB = 8;                     // FFTs per work item
+constexpr int NPAIR = TB / 2;             // step-1 tiles (FFT pairs) per item
+constexpr int NA1 = 2;                    // A1 stages (TMEM)
+constexpr int NIB = 4;                    // pair slots the helper fills ahead of the producer
+constexpr int NTHREADS = 576;             // 18 warps
+constexpr int W_TW = 4, W_OUT = 12, W_MMA = 16, W_HELP = 17;
+constexpr uint32_t TMEM_COLS = 512;
+constexpr uint32_t A1_COL = 0;            // [stage] 64 columns: x_hi (n1, re|im) | x_lo
+constexpr uint32_t D1_COL = 128;          // [pair of the item] 64 columns (k1, re|im)
+constexpr uint32_t D2_COL = 384;          // [tile] 64 columns (k2, re|im)
+constexpr int ERR_WAIT = 7;
+constexpr uint32_t kIdesc = tc::idesc_f16(128, 64);
+
+struct Smem {
+    alignas(1024) uint8_t a2[2][2][2][128 * 128];   // [tile][hi|lo][K half] rows 8 (k1 % 16) + b, (n2 % 32, re|im)
+    alignas(1024) uint8_t b1[2][64 * 128];          // [hi|lo] rows (k1, re|im), K (n1, re|im)
+    alignas(1024) uint8_t b2[2][2][64 * 128];       // [hi|lo][K half] rows (k2, re|im), K (n2 % 32, re|im)
+    alignas(16) uint8_t inb[NIB][2][INB];           // [pair % NIB][FFT of the pair] input bytes
+    alignas(16) uint2 lut[NIB][2][F1][4];           // [pair % NIB][FFT][n1][code] (hi, lo) of level * step[n1]
+    int2 pwin[NIB][2];                              // [pair % NIB][FFT] (bit of sample 0 in inb, valid)
+    DelayEntry oent[2][TB];                         // output: delay entries [item parity][FFT]
+    float2 fstep[TB][K2H];                          // output: [b][k2]
+    float ctab[P::FS + P::FST];                     // chan_sub | chan_step
+    uint64_t a1_full[NA1], a1_empty[NA1], d1_full[NPAIR], d1_empty[NPAIR];
+    uint64_t a2_full[2], a2_empty[2], d2_full[2], d2_empty[2], drain;
+    uint64_t cp_full[NIB], tab_full[NIB], tab_empty[NIB];
+    uint32_t tmem_base;
+    int abort;
+    int drain_fail;                                 // a drain wait expired: copies or MMAs may be in flight
+};
+static_assert(sizeof(Smem) + 1024 <= 232448, "fits the opt-in shared memory of one CTA");
+
+// FP16 pair (hi, lo) of an FP32 complex value, each packed (re, im)
+__device__ __forceinline__ uint2 split_pair(float re, float im)
+{
+    const __half2 hi = __floats2half2_rn(re, im);
+    const float2 hf = __half22float2(hi);
+    const __half2 lo = __floats2half2_rn(re - hf.x, im - hf.y);
+    return make_uint2(h2u(hi), h2u(lo));
+}
+
+// e^{i a} for |a| <= 0.25 by its Taylor series to the a^8 / a^9 terms (truncation < 1e-10)
+__device__ __forceinline__ float2 cis_small(float a)
+{
+    const float a2 = a * a;
+    const float c = 1.f - a2 * (0.5f - a2 * (1.f / 24.f - a2 * (1.f / 720.f - a2 * (1.f / 40320.f))));
+    const float s = a * (1.f - a2 * (1.f / 6.f - a2 * (1.f / 120.f - a2 * (1.f / 5040.f - a2 * (1.f / 362880.f)))));
+    return make_float2(c, s);
+}
+
+__device__ __forceinline__ float2 cis_half_turns_acc(float x)
+{
+    float s, c;
+    sincospif(x, &s, &c);
+    return make_float2(c, s);
+}
+
+template <bool OUT16>
+__global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a)
+{
+    using namespace tc;
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    Smem& sm = *reinterpret_cast<Smem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    volatile int* abort_flag = &sm.abort;
+
+    const int tspan = a.tspan ? a.tspan : a.T;
+    const int ntb = tspan / TB;
+    const int ntask = a.nsb * a.nant * ntb;
+    const int nitem = blockIdx.x < ntask ? (ntask - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+
+    // ---- set-up: barriers, TMEM, constant DFT matrices (hi, lo), channel table
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < NA1; s++) {
+            mbar_init(&sm.a1_full[s], 128);
+            mbar_init(&sm.a1_empty[s], 1);
+        }
+        for (int p = 0; p < NPAIR; p++) {
+            mbar_init(&sm.d1_full[p], 1);
+            mbar_init(&sm.d1_empty[p], 128);
+        }
+        for (int j = 0; j < 2; j++) {
+            mbar_init(&sm.a2_full[j], 256);
+            mbar_init(&sm.a2_empty[j], 1);
+            mbar_init(&sm.d2_full[j], 1);
+            mbar_init(&sm.d2_empty[j], 128);
+        }
+        mbar_init(&sm.drain, 1);
+        for (int s = 0; s < NIB; s++) {
+            mbar_init(&sm.cp_full[s], 1);
+            mbar_init(&sm.tab_full[s], 1);
+            mbar_init(&sm.tab_empty[s], 128);
+        }
+        sm.abort = 0;
+        sm.drain_fail = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == W_MMA) tmem_alloc(&sm.tmem_base, TMEM_COLS);
+    // B1[(k1, c)][(n1, c')] and B2[(k2, c)][(n2, c')]: real form of W^(n k), w = (Re, Im) of W:
+    // (c, c') = (0, 0) Re, (0, 1) -Im, (1, 0) Im, (1, 1) Re; each entry as an FP16 pair
+    for (int e = threadIdx.x; e < 64 * 64 * 3; e += NTHREADS) {
+        const int m = e / (64 * 64);          // 0: B1, 1-2: B2 K halves
+        const int rem = e - m * 64 * 64;
+        const int nb = rem >> 6, kk = rem & 63;
+        const int c = nb & 1, cp = kk & 1;
+        float2 w;
+        uint8_t *hi, *lo;
+        if (m == 0) {
+            w = twiddle_exact(((kk >> 1) * (nb >> 1)) & (F1 - 1), F1);
+            hi = sm.b1[0];
+            lo = sm.b1[1];
+        } else {
+            const int n2 = (m - 1) * 32 + (kk >> 1);
+            w = twiddle_exact((n2 * (nb >> 1)) & (F2 - 1), F2);
+            hi = sm.b2[0][m - 1];
+            lo = sm.b2[1][m - 1];
+        }
+        const float v = c == 0 ? (cp == 0 ? w.x : -w.y) : (cp == 0 ? w.y : w.x);
+        const __half h = __float2half_rn(v);
+        const uint32_t o = sw128(nb, kk >> 3) + (kk & 7) * 2;
+        *reinterpret_cast<__half*>(hi + o) = h;
+        *reinterpret_cast<__half*>(lo + o) = __float2half_rn(v - __half2float(h));
+    }
+    for (int i = threadIdx.x; i < P::FS + P::FST; i += NTHREADS)
+        sm.ctab[i] = i < P::FS ? a.chan_sub[i] : a.chan_step[i - P::FS];
+    fence_async_smem();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = sm.tmem_base;
+
+    if (warp < W_TW) {
+        // ================================================================ producer
+        // thread = TMEM lane = A1 row (b, n2) of the pair: b = tp / 64, n2 = tp % 64; its row holds
+        // x_hi (n1, re|im) in columns 0-31 and x_lo in 32-63 of the stage
+        const int tp = threadIdx.x;
+        const int bsel = tp >> 6, n2 = tp & 63;
+        const uint32_t lane_off = (uint32_t)(32 * warp) << 16;
+        const int npair = nitem * NPAIR;
+        for (int g = 0; g < npair; g++) {
+            const int x = g % NIB, s = g % NA1;
+            const uint32_t ph = (g / NIB) & 1;
+            const bool ok = mbar_wait(&sm.cp_full[x], ph, abort_flag) && mbar_wait(&sm.tab_full[x], ph, abort_flag) &&
+                            mbar_wait(&sm.a1_empty[s], ((g / NA1) & 1) ^ 1, abort_flag);
+            if (!__all_sync(0xffffffffu, ok)) {   // warp-uniform: the TMEM stores are .sync.aligned
+                if (!*abort_flag) atomicCAS(a.err, 0, ERR_WAIT);
+                *abort_flag = 1;
+                break;
+            }
+            tc_fence_after();   // the MMAs that read this stage are complete
+            uint32_t hv[32], lv[32];
+            const int2 wv = sm.pwin[x][bsel];
+            if (wv.y) {
+                // sample 64 n1 + n2 sits at bit wv.x + 128 n1 + 2 n2 of the staged window: the same
+                // shift for every n1, four words apart
+                const int bit = wv.x + 2 * n2;
+                const uint32_t* wp = reinterpret_cast<const uint32_t*>(sm.inb[x][bsel]) + (bit >> 5);
+                const int sh = bit & 31;
+                const uint2* lt = sm.lut[x][bsel][0];
+#pragma unroll
+                for (int n1 = 0; n1 < F1; n1++) {
+                    const uint2 e = lt[4 * n1 + ((wp[4 * n1] >> sh) & 3u)];
+                    hv[n1] = e.x;
+                    lv[n1] = e.y;
+                }
+            } else {
+#pragma unroll
+                for (int n1 = 0; n1 < F1; n1++) hv[n1] = lv[n1] = 0u;
+            }
+            mbar_arrive(&sm.tab_empty[x]);   // this thread's last read of slot x
+            tmem_st32(tmem + lane_off + A1_COL + 64 * s, hv);
+            tmem_st32(tmem + lane_off + A1_COL + 64 * s + 32, lv);
+            tmem_wait_st();
+            tc_fence_before();
+            mbar_arrive(&sm.a1_full[s]);
+        }
+    } else if (warp < W_OUT) {
+        // ================================================================ twiddle
+        // warp t: lane quarter q = t % 4 (D1 rows 32 q .. 32 q + 31: FFT bsel = q / 2 of the pair,
+        // n2 = 32 (q % 2) + lane), pairs h and h + 2 of each item (h = t / 4)
+        const int t = warp - W_TW;
+        const int q = t & 3, h = t >> 2;
+        const int bsel = q >> 1, n2 = 32 * (q & 1) + lane;
+        const uint32_t lane_off = (uint32_t)(32 * q) << 16;
+        const int khalf = n2 >> 5;
+        const uint32_t col = (uint32_t)(((n2 & 31) >> 2) << 4) + 4 * (n2 & 3);   // byte of (n2, re|im) in a row
+        const float alpha_n2 = -6.283185307179586f * (float)n2 / (float)F;
+        DelayEntry dn[2];
+        if (nitem > 0)
+            for (int u = 0; u < 2; u++) dn[u] = item_entry<TB>(a, 0, ntb, 2 * (h + 2 * u) + bsel);
+        bool ok = true;
+        for (int i = 0; i < nitem && ok; i++) {
+            const Item it = item_of<TB>(blockIdx.x + i * gridDim.x, a.nant, ntb);
+            // per pair: start of the twiddle row at k1 = 0 and k1 = 16, and its step e^{i alpha}
+            float2 st0[2], st16[2], rho[2];
+            {
+                const double lo = a.sb_lo[it.sb];
+                const double lofrac = lo - trunc(lo);
+                const bool fraclo = lofrac > 1e-11;   // kernel.c:39
+#pragma unroll
+                for (int u = 0; u < 2; u++) {
+                    const DelayEntry d = dn[u];
+                    if (d.valid) {
+                        // sub[n2]: phase lo (a n2 / F + b') (+ lofrac (int)b), kernel.c:434-470
+                        const double intdelay = trunc(d.b);
+                        double v = lo * (d.b - intdelay);
+                        if (fraclo) v = fma(lofrac, intdelay, v);
+                        const double ph = fma((double)n2, lo * d.a * (1.0 / F), v);
+                        const float2 sub = cis_half_turns_acc((float)(-2.0 * (ph - trunc(ph))));
+                        // alpha: -2 pi n2 / F plus the fractional-sample phase per channel
+                        const float al = alpha_n2 + __fmul_rn(sm.ctab[1], __double2float_rn(d.frac));
+                        const float2 r = cis_small(al);
+                        float2 r16 = cmul(r, r);
+                        r16 = cmul(r16, r16);
+                        r16 = cmul(r16, r16);
+                        r16 = cmul(r16, r16);
+                        st0[u] = sub;
+                        st16[u] = cmul(sub, r16);
+                        rho[u] = r;
+                    } else {
+                        st0[u] = st16[u] = rho[u] = make_float2(0.f, 0.f);
+                    }
+                }
+            }
+            if (i + 1 < nitem)
+                for (int u = 0; u < 2; u++) dn[u] = item_entry<TB>(a, i + 1, ntb, 2 * (h + 2 * u) + bsel);
+#pragma unroll 1
+            for (int j = 0; j < 2 && ok; j++) {
+                // tile j = k1 in [16 j, 16 j + 16) of every FFT of the item
+                if (!__all_sync(0xffffffffu, mbar_wait(&sm.a2_empty[j], (i & 1) ^ 1, abort_flag))) {
+                    ok = false;
+                    break;
+                }
+#pragma unroll
+                for (int u = 0; u < 2; u++) {
+                    const int p = h + 2 * u;
+                    if (j == 0 && !__all_sync(0xffffffffu, mbar_wait(&sm.d1_full[p], i & 1, abort_flag))) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    uint32_t v[32];
+                    tmem_ld32(tmem + lane_off + D1_COL + 64 * p + 32 * j, v);
+                    tmem_wait_ld();
+                    if (j == 1) {
+                        tc_fence_before();
+                        mbar_arrive(&sm.d1_empty[p]);
+                    }
+                    const int b = 2 * p + bsel;
+                    float2 cur = j ? st16[u] : st0[u];
+                    const float2 r = rho[u];
+                    uint8_t* hi = sm.a2[j][0][khalf];
+                    uint8_t* lo = sm.a2[j][1][khalf];
+#pragma unroll
+                    for (int kk = 0; kk < 16; kk++) {
+                        const float2 y = make_float2(__uint_as_float(v[2 * kk]), __uint_as_float(v[2 * kk + 1]));
+                        const float2 z = cmul(y, cur);
+                        cur = cmul(cur, r);
+                        const uint2 zz = split_pair(z.x, z.y);
+                        const int R = 8 * kk + b;
+                        const uint32_t o = (uint32_t)(R * 128) + (col ^ (uint32_t)((R & 7) << 4));
+                        *reinterpret_cast<uint32_t*>(hi + o) = zz.x;
+                        *reinterpret_cast<uint32_t*>(lo + o) = zz.y;
+                    }
+                }
+                if (!ok) break;
+                fence_async_smem();
+                mbar_arrive(&sm.a2_full[j]);
+            }
+        }
+        if (!ok) {
+            if (!*abort_flag) atomicCAS(a.err, 0, ERR_WAIT);
+            *abort_flag = 1;
+        }
+    } else if (warp < W_MMA) {
+        // ================================================================ output
+        const int q = warp & 3;
+        const int r = 32 * q + lane;                // D2 row: k1 % 16 = r / 8, b = r % 8
+        const int kl = r >> 3, b = r & 7;
+        const uint32_t lane_off = (uint32_t)(32 * q) << 16;
+        const int to = threadIdx.x - 32 * W_OUT;
+        const int nsig = a.nant;
+        DelayEntry dnext;
+        if (to < TB && nitem > 0) sm.oent[0][to] = item_entry<TB>(a, 0, ntb, to);
+        if (to < TB && nitem > 1) dnext = item_entry<TB>(a, 1, ntb, to);
+        bool ok = true;
+        for (int i = 0; i < nitem; i++) {
+            const Item it = item_of<TB>(blockIdx.x + i * gridDim.x, a.nant, ntb);
+            // item i's entries visible; every thread is done with item i - 1's table
+            if (bar_or(2, 128, !ok || *abort_flag)) break;
+            for (int e = to; e < TB * K2H; e += 128) {
+                const int bb = e / K2H, k2 = e % K2H;
+                const DelayEntry& d = sm.oent[i & 1][bb];
+                float sn = 0.f, cs = 0.f;
+                if (d.valid) sincosf(__fmul_rn(sm.ctab[P::FS + k2], __double2float_rn(d.frac)), &sn, &cs);
+                sm.fstep[bb][k2] = make_float2(cs, sn);   // kernel.c:512-523 (step part)
+            }
+            if (bar_or(2, 128, !ok || *abort_flag)) break;
+            if (i + 1 < nitem) {
+                if (to < TB) sm.oent[(i + 1) & 1][to] = dnext;
+                if (to < TB && i + 2 < nitem) dnext = item_entry<TB>(a, i + 2, ntb, to);
+            }
+#pragma unroll 1
+            for (int j = 0; j < 2; j++) {
+                if (!__all_sync(0xffffffffu, mbar_wait(&sm.d2_full[j], i & 1, abort_flag))) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                uint32_t v[64];
+                tmem_ld32(tmem + lane_off + D2_COL + 64 * j, v);
+                tmem_ld32(tmem + lane_off + D2_COL + 64 * j + 32, v + 32);
+                tmem_wait_ld();
+                tc_fence_before();
+                mbar_arrive(&sm.d2_empty[j]);
+                const int k1 = 16 * j + kl;
+                const float2* fs = sm.fstep[b];
+                if constexpr (OUT16) {
+                    const size_t chan_stride = (size_t)a.rows * a.T;
+                    __half* pk = reinterpret_cast<__half*>(a.spec) + ((size_t)it.sb * C + k1) * chan_stride +
+                                 (size_t)(2 * it.ant) * a.T + it.tb0 + b;
+                    const size_t kstep = (size_t)F1 * chan_stride;
+#pragma unroll
+                    for (int k2 = 0; k2 < K2H; k2++) {
+                        const float2 y = cmul(make_float2(__uint_as_float(v[2 * k2]), __uint_as_float(v[2 * k2 + 1])),
+                                              fs[k2]);
+                        const __half2 hv = __floats2half2_rn(y.x, y.y);
+                        pk[0] = __low2half(hv);
+                        pk[a.T] = __high2half(hv);
+                        pk += kstep;
+                    }
+                } else {
+                    float2* pk = reinterpret_cast<float2*>(a.spec) +
+                                 (((size_t)it.sb * nsig + it.ant) * a.T + it.tb0 + b) * C + k1;
+#pragma unroll
+                    for (int k2 = 0; k2 < K2H; k2++)
+                        pk[F1 * k2] = cmul(make_float2(__uint_as_float(v[2 * k2]), __uint_as_float(v[2 * k2 + 1])),
+                                           fs[k2]);
+                }
+            }
+            if (!ok) break;
+        }
+        if (!ok) {
+            if (!*abort_flag) atomicCAS(a.err, 0, ERR_WAIT);
+            *abort_flag = 1;
+        }
+    } else if (warp == W_HELP) {
+        // ================================================================ helper
+        // For each pair, NIB pairs ahead of the producer: the input copies, the tables
+        // level(code) * step[n1] as FP16 pairs (step phase lo n1 stride a / F, kernel.c:434-470,
+        // one FP64 multiply from the per-FFT slope) and the window offsets.
+        const int npair = nitem * NPAIR;
+        DelayEntry dn0, dn1;
+        double lon = 0.0;
+        const uint8_t* rown = nullptr;
+        auto fetch = [&](int g, DelayEntry& d0, DelayEntry& d1, double& lo, const uint8_t*& row) {
+            const int i = g / NPAIR, p = g % NPAIR;
+            d0 = item_entry<TB>(a, i, ntb, 2 * p);
+            d1 = item_entry<TB>(a, i, ntb, 2 * p + 1);
+            const Item it = item_of<TB>(blockIdx.x + i * gridDim.x, a.nant, ntb);
+            lo = a.sb_lo[it.sb];
+            row = a.data + ((size_t)it.sb * a.nant + it.ant) * a.pitch;
+        };
+        if (npair > 0) fetch(0, dn0, dn1, lon, rown);
+        int issued = -1;
+        for (int g = 0; g < npair; g++) {
+            const int x = g % NIB;
+            const DelayEntry d0 = dn0, d1 = dn1;
+            const double lo = lon;
+            const uint8_t* row = rown;
+            if (g + 1 < npair) fetch(g + 1, dn0, dn1, lon, rown);
+            if (!__all_sync(0xffffffffu, mbar_wait(&sm.tab_empty[x], ((g / NIB) & 1) ^ 1, abort_flag))) {
+                if (!*abort_flag) atomicCAS(a.err, 0, ERR_WAIT);
+                *abort_flag = 1;
+                break;
+            }
+            if (lane == 0) {
+                issue_pair(&sm.cp_full[x], sm.inb[x][0], sm.inb[x][1], row, d0, d1);
+                issued = g;
+            }
+#pragma unroll
+            for (int b = 0; b < 2; b++) {
+                const DelayEntry& d = b ? d1 : d0;
+                uint4 e0 = make_uint4(0u, 0u, 0u, 0u), e1 = e0;
+                if (d.valid) {
+                    const double phs = (double)(lane * F1) * (lo * d.a * (1.0 / F));
+                    const float2 st = cis_half_turns_acc((float)(-2.0 * (phs - trunc(phs))));
+                    uint2 v[4];
+#pragma unroll
+                    for (int c = 0; c < 4; c++) {
+                        const float lv = level2bit((uint32_t)c);
+                        v[c] = split_pair(lv * st.x, lv * st.y);
+                    }
+                    e0 = make_uint4(v[0].x, v[0].y, v[1].x, v[1].y);
+                    e1 = make_uint4(v[2].x, v[2].y, v[3].x, v[3].y);
+                }
+                uint4* dst = reinterpret_cast<uint4*>(sm.lut[x][b][lane]);
+                dst[0] = e0;
+                dst[1] = e1;
+                if (lane == b) sm.pwin[x][b] = window_bits(d);
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&sm.tab_full[x]);
+        }
+        // copies must land before the CTA exits (phases already complete return at once)
+        if (lane == 0)
+            for (int g = issued - (NIB - 1); g <= issued; g++)
+                if (g >= 0 && !mbar_drain(&sm.cp_full[g % NIB], (g / NIB) & 1)) {
+                    atomicCAS(a.err, 0, ERR_WAIT);
+                    sm.drain_fail = 1;
+                }
+    } else if (lane == 0) {
+        // ================================================================ MMA issuer
+        bool ok = true;
+        const uint32_t sb1h = smem_u32(sm.b1[0]), sb1l = smem_u32(sm.b1[1]);
+        for (int i = 0; i < nitem && ok; i++) {
+            for (int p = 0; p < NPAIR; p++) {
+                const int g = i * NPAIR + p;
+                const int s = g % NA1;
+                if (!mbar_wait(&sm.a1_full[s], (g / NA1) & 1, abort_flag) ||
+                    !mbar_wait(&sm.d1_empty[p], (i & 1) ^ 1, abort_flag)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t d1 = tmem + D1_COL + 64 * p, xa = tmem + A1_COL + 64 * s;
+                // x_hi . W_hi + x_lo . W_hi + x_hi . W_lo; K = 64 = 4 steps of 16 (8 columns,
+                // 32 bytes of a 128-byte swizzled row)
+#pragma unroll
+                for (int kk = 0; kk < 4; kk++)
+                    umma_ts(d1, xa + 8 * kk, umma_desc(sb1h + 32 * kk), kIdesc, kk > 0 ? 1u : 0u);
+#pragma unroll
+                for (int kk = 0; kk < 4; kk++) umma_ts(d1, xa + 32 + 8 * kk, umma_desc(sb1h + 32 * kk), kIdesc, 1u);
+#pragma unroll
+                for (int kk = 0; kk < 4; kk++) umma_ts(d1, xa + 8 * kk, umma_desc(sb1l + 32 * kk), kIdesc, 1u);
+                umma_commit(&sm.a1_empty[s]);
+                umma_commit(&sm.d1_full[p]);
+            }
+            if (!ok) break;
+#pragma unroll 1
+            for (int j = 0; j < 2; j++) {
+                if (!mbar_wait(&sm.a2_full[j], i & 1, abort_flag) ||
+                    !mbar_wait(&sm.d2_empty[j], (i & 1) ^ 1, abort_flag)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t d2 = tmem + D2_COL + 64 * j;
+                // Z_hi . W_hi + Z_lo . W_hi + Z_hi . W_lo; K = 128 = two 64-element halves
+#pragma unroll 1
+                for (int t = 0; t < 3; t++) {
+                    const int la = t == 1 ? 1 : 0, lb = t == 2 ? 1 : 0;
+#pragma unroll
+                    for (int kk = 0; kk < 8; kk++)
+                        umma<false>(d2, umma_desc(smem_u32(sm.a2[j][la][kk >> 2]) + (kk & 3) * 32),
+                                    umma_desc(smem_u32(sm.b2[lb][kk >> 2]) + (kk & 3) * 32), kIdesc,
+                                    (t > 0 || kk > 0) ? 1u : 0u);
+                }
+                umma_commit(&sm.a2_empty[j]);
+                umma_commit(&sm.d2_full[j]);
+            }
+        }
+        if (!ok) {
+            if (!*abort_flag) atomicCAS(a.err, 0, ERR_WAIT);
+            *abort_flag = 1;
+        }
+        // every MMA issued must have retired before TMEM is freed
+        umma_commit(&sm.drain);
+        if (!mbar_drain(&sm.drain, 0)) {
+            atomicCAS(a.err, 0, ERR_WAIT);
+            sm.drain_fail = 1;
+        }
+    }
+
+    __syncthreads();
+    // after an expired drain, MMAs may still write TMEM: it stays allocated (code 7 was recorded;
+    // the context's later tensor-core launches cannot be trusted and the process should reset)
+    if (warp == W_MMA && !sm.drain_fail) {
+        tc_fence_after();
+        tmem_dealloc(tmem, TMEM_COLS);
+    }
+}
+
+}  // namespace ftc32
+
+bool ftc32_supported(int nchan, const FArgs& a)
+{
+    return nchan == ftc32::C && a.npol == 1 && !a.cpx && a.amax == nullptr && a.T % ftc32::TB == 0 &&
+           (a.tspan ? a.tspan : a.T) % ftc32::TB == 0 && a.err != nullptr;
+}
+
+cudaError_t launch_ftc32(int mode, const FArgs& a, cudaStream_t st)
+{
+    using namespace ftc32;
+    const size_t sm = sizeof(Smem) + 1024;
+    const int tspan = a.tspan ? a.tspan : a.T;
+    const long long ntask = (long long)a.nsb * a.nant * (tspan / TB);
+    if (ntask <= 0) return cudaSuccess;
+    if (ntask > 0x7fffffffLL) return cudaErrorInvalidValue;
+    int dev = 0, nsm = 0;
+    cudaError_t e;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    const int grid = (int)(ntask < nsm ? ntask : nsm);
+    if (mode == kSpecF16) {
+        static unsigned configured = 0;
+        if ((e = set_smem_once(k_ftc32<true>, sm, &configured)) != cudaSuccess) return e;
+        k_ftc32<true><<<grid, NTHREADS, sm, st>>>(a);
+    } else {
+        static unsigned configured = 0;
+        if ((e = set_smem_once(k_ftc32<false>, sm, &configured)) != cudaSuccess) return e;
+        k_ftc32<false><<<grid, NTHREADS, sm, st>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace fx

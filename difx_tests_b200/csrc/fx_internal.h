@@ -63,7 +63,7 @@ struct FArgs {
     int tspan;                  // slots [0, tspan) written (>= nfft, multiple of 64; 0 = T)
     int cpx;                    // input format: 0 = 2-bit real, 1 = 8-bit complex (FFT length nchan)
     int* err;                   // device error word (code 6: an input staging wait expired), or null
-    int fkind;                  // F-stage arithmetic (FXC_F_FFT32 or FXC_F_TC16; 0 = FFT32)
+    int fkind;                  // F-stage arithmetic (FXC_F_FFT32, FXC_F_TC16 or FXC_F_TC32; 0 = FFT32)
 };
 
 

@@ -147,6 +147,33 @@ def make_job(nant=4, npol=1, nchan=256, numffts=64, bw=32e6, lo=1.4e9, rho=0.1, 
                sb_lo=sb_lo)
 
 
+def make_long_job(nant=4, nchan=1024, numffts=31250, bw=64e6, lo=1.4e9, rho=0.1, seed=0, max_shift=40) -> Job:
+    """A full-length subintegration of one subband, one polarisation, cheap to generate: every
+    antenna sees the common N(0, 1) signal (correlation rho) shifted by a whole number of samples,
+    and the delay model is that constant shift (delay -shift_j samples, file offset 0), so the
+    correlator's integer shift lines the antennas up and its fringe rotation is a constant phase
+    per antenna (kernel.c:428-497 with a zero delay rate).  For tests of accumulation over tens
+    of thousands of FFTs, where make_job's per-sample delay synthesis would take minutes."""
+    rng = np.random.default_rng(seed)
+    Ts = 1.0 / (2.0 * bw)
+    shifts = rng.integers(0, max_shift, nant)
+    delays = np.zeros((nant, 3))
+    delays[:, 2] = -shifts * Ts
+    fileoffsets = np.zeros(nant)
+    sbb = subint_bytes(nchan, numffts, 1)
+    nsamp = sbb * 4
+    common = rng.standard_normal(nsamp + max_shift, dtype=np.float32)
+    data = np.zeros((1, nant, sbb), dtype=np.uint8)
+    for j in range(nant):
+        # stream j at sample i holds the common signal of sample i - shift_j
+        sj = common[max_shift - shifts[j]: max_shift - shifts[j] + nsamp]
+        x = np.sqrt(rho) * sj + np.sqrt(1.0 - rho) * rng.standard_normal(nsamp, dtype=np.float32)
+        packed = quantise_pack(x[None, :], 1)
+        data[0, j, : len(packed)] = packed
+    return Job(nant=nant, npol=1, nchan=nchan, numffts=numffts, bw=bw, lo=lo, nsubband=1, delays=delays,
+               fileoffsets=fileoffsets, data=data, sb_lo=np.array([lo]))
+
+
 def subint_bytes_c8(nchan: int, numffts: int, npol: int) -> int:
     """8-bit complex input: nchan complex samples per FFT, (numffts + 1) FFTs, an int8
     (re, im) pair per sample and polarisation."""

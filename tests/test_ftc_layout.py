@@ -92,3 +92,86 @@ def test_staged_input_reads_stay_inside_the_buffer():
                 assert 4 * (idx + 2) <= INB              # the second word of the funnel shift is in the buffer
                 last_bit = 32 * idx + sh + 7             # the 8 bits (4 samples) this read uses
                 assert last_bit < 8 * 16 * nvec          # ... lie inside the copied window
+
+
+# --------------------------------------------------------------------------------------------
+# FP32-grade tensor-core F stage (difx_tests_b200/csrc/fx_ftc32.cu): 8-FFT items, A1 in TMEM
+# (lane = row (b, n2) of the pair), A2 tiles of rows 8 (k1 % 16) + b, two FP16 limbs.
+TB32 = 8
+
+
+def test_tc32_producer_reads_stay_inside_the_staged_window():
+    # sample 64 n1 + n2 at bit wv + 128 n1 + 2 n2; the thread reads word (wv + 2 n2) / 32 + 4 n1
+    # and two bits at shift (wv + 2 n2) % 32; wv = 2 (offset - 4 base), offset - 4 base < 64
+    for d in range(64):                    # offset - 4 * base: (first - base) * 4 + offset % 4
+        wv = 2 * d
+        first_minus_base, rem = divmod(d, 4)
+        nvec = (F // 4 + 1 + first_minus_base + 15) // 16
+        copied = 16 * nvec
+        assert copied <= INB
+        for n2 in range(64):
+            bit = wv + 2 * n2
+            sh = bit % 32
+            assert sh <= 30                     # the two bits never straddle a word
+            for n1 in range(F1):
+                w = bit // 32 + 4 * n1
+                assert 4 * w + 3 < INB          # the word is inside the staging buffer
+                # the sample's own bits are inside the copied bytes
+                sbit = bit + 128 * n1
+                assert (sbit + 1) // 8 < copied
+
+
+def tc32_a2_offset(R, n2):
+    """Byte of (row R, K element (n2, re|im)) in the 16 KB buffer of K half n2 // 32 (twiddle store)."""
+    col = (((n2 & 31) >> 2) << 4) + 4 * (n2 & 3)
+    return R * 128 + (col ^ ((R & 7) << 4))
+
+
+def test_tc32_a2_stores_cover_each_tile_once_and_match_the_mma_layout():
+    for khalf in range(2):
+        seen = set()
+        for R in range(128):
+            for n2 in range(32 * khalf, 32 * khalf + 32):
+                o = tc32_a2_offset(R, n2)
+                assert 0 <= o and o + 4 <= 128 * 128
+                # the MMA reads K element 2 (n2 % 32) + c of row R from chunk (n2 % 32) // 4 swizzled
+                assert o == sw128(R, (n2 & 31) >> 2) + 4 * (n2 & 3)
+                seen.add(o)
+        assert len(seen) == 128 * 32             # every 4-byte word of the K half exactly once
+
+
+def test_tc32_twiddle_warp_stores_hit_distinct_banks():
+    # one store instruction of a twiddle warp: 32 lanes = 32 consecutive n2 (same K half), one row R
+    for q in range(4):
+        for R in range(128):
+            banks = {(tc32_a2_offset(R, 32 * (q & 1) + lane) // 4) % 32 for lane in range(32)}
+            assert len(banks) == 32
+
+
+def test_tc32_rows_and_tmem_columns():
+    # D1 / A1 rows: lane r = 64 b + n2 of the pair; twiddle warp quarter q covers FFT q // 2,
+    # n2 = 32 (q % 2) + lane; A2 / D2 rows 8 kl + b of tile k1 // 16; output lane r -> (r // 8, r % 8)
+    a1 = {(r >> 6, r & 63) for r in range(128)}
+    assert a1 == {(b, n2) for b in range(2) for n2 in range(64)}
+    tw = {(q >> 1, 32 * (q & 1) + lane) for q in range(4) for lane in range(32)}
+    assert tw == a1
+    rows = {(8 * kl + b) for kl in range(16) for b in range(TB32)}
+    assert rows == set(range(128))
+    out = {(r >> 3, r & 7) for r in range(128)}
+    assert out == {(kl, b) for kl in range(16) for b in range(TB32)}
+    # TMEM: A1 2 stages x 64, D1 4 pairs x 64, D2 2 tiles x 64 inside the 512 allocated columns
+    a1c = [(64 * s, 64 * s + 64) for s in range(2)]
+    d1c = [(128 + 64 * p, 128 + 64 * p + 64) for p in range(TB32 // 2)]
+    d2c = [(384 + 64 * j, 384 + 64 * j + 64) for j in range(2)]
+    spans = sorted(a1c + d1c + d2c)
+    assert spans[0][0] == 0 and spans[-1][1] == 512
+    assert all(a[1] == b[0] for a, b in zip(spans, spans[1:]))
+
+
+def test_tc32_output_indices_cover_the_item_once():
+    # F16 layout [chan][row][T]: output thread (k1 = 16 j + kl, b) writes channel k1 + 32 k2 of slot tb0 + b
+    for j in range(2):
+        got = {(16 * j + (r >> 3) + 32 * k2, r & 7) for r in range(128) for k2 in range(32)}
+        assert len(got) == 16 * 32 * TB32
+    allk = {(16 * j + (r >> 3) + 32 * k2) for j in range(2) for r in range(128) for k2 in range(32)}
+    assert allk == set(range(1024))
