@@ -588,6 +588,79 @@ def run_gpu_arm(args):
     return 0
 
 
+def run_shard_arm(args):
+    """One subintegration of the workload split over the ranks (strong scaling): "time" shards
+    (each rank a range of FFTs of every subband, one all-reduce of visibilities and counts) or
+    "subband" shards (each rank whole subbands, one all-gather), correlated through the library
+    and merged inside the timed step (NCCL on the device).  Time = max over ranks of CUDA-event
+    time on each rank's stream."""
+    import torch
+    import torch.distributed as dist
+
+    import difx_tests_b200 as fx
+    from difx_tests_b200 import sharding
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    w = WORKLOADS[args.workload]
+    xmode, fstage = FORMS[args.xmode if args.xmode in FORMS else "tc"]
+    cfg = fx.make_config(w["nant"], w["nchan"], w["numffts"], w["bw"], w["lo"], npol=w["npol"], nsubband=w["nsb"],
+                         xmode=xmode, fstage=fstage)
+    subint = fx.lib().fxc_subint_bytes(cfg)
+    pitch = (subint + 16 + 255) // 256 * 256
+    delays, offs = delay_model(w["nant"], w["nchan"], w["bw"], seed=42)
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
+    data = gen_device_data(torch, w["nsb"], w["nant"], w["npol"], subint, pitch, w["rho"], seed=1000, device=dev)
+    rcfg, f0, n, s0 = sharding.shard_config(fx, cfg, args.shard, world, rank)
+    corr = fx.Correlator(rcfg)
+    corr.set_stream(stream.cuda_stream)
+
+    def step():
+        return sharding.correlate_shard(fx, corr, args.shard, data.data_ptr(), pitch, delays, offs, f0, n, s0,
+                                        w["nsb"], dev)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = sharding.max_over_ranks(e0.elapsed_time(e1) / args.steps, device=dev)
+    samples = w["nant"] * w["npol"] * w["nsb"] * w["numffts"] * 2 * w["nchan"]
+    corr.close()
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": samples / (ms / 1e3) / 1e9, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": DTYPES[args.xmode if args.xmode in FORMS else "tc"],
+            "data": "synthetic (seeded, generated on device)",
+            "config": {"workload": w["desc"], "parallelism": f"{args.shard} shards x{world}",
+                       "merge": "all-reduce of visibilities and counts" if args.shard == "time" else "all-gather",
+                       "l2": "inputs exceed L2; no flush"},
+            "clocks": clk}))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def run_batch_arm(args, emit=True):
     """12 uneven jobs through fxc_batch_* (grouped persistent launches, CUDA graph replay,
     autotuned plans) against the same jobs run one after another through the single-job path.
@@ -846,6 +919,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--shard", default="replica", choices=["replica", "time", "subband"],
+                    help="replica: every rank its own subintegration (weak scaling, the default); time / subband: "
+                         "one subintegration split over the ranks and merged on the device (strong scaling)")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the bounded cfg3 (batch) and cfg4 (large array) runs of the default workload")
     args = ap.parse_args()
@@ -853,6 +929,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.shard != "replica":
+        return run_shard_arm(args)
     if args.workload == "cfg3":
         run_batch_arm(args)
         return 0

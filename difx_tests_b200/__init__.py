@@ -263,6 +263,19 @@ class Correlator:
         vis = out.view(np.complex64).reshape(self.nsb, self.nbl + self.nant, self.npol ** 2, self.nchan)
         return vis, counts
 
+    def visibilities_device(self, d_ptr, normalize=False):
+        """Visibilities into device memory at d_ptr (vis_count complex64 values, the layout of
+        visibilities()); -> counts int32 [nbl + nant] (host)."""
+        _check(_lib().fxc_get_visibilities_device(self._ctx, _P(d_ptr), 1 if normalize else 0),
+               "fxc_get_visibilities_device")
+        counts = np.empty(self.nbl + self.nant, dtype=np.int32)
+        _check(_lib().fxc_get_visibilities(self._ctx, None, counts.ctypes.data_as(_IP), 0), "fxc_get_visibilities")
+        return counts
+
+    @property
+    def vis_count(self):
+        return self.nsb * (self.nbl + self.nant) * self.npol ** 2 * self.nchan
+
     def synchronize(self):
         _check(_lib().fxc_synchronize(self._ctx), "fxc_synchronize")
 

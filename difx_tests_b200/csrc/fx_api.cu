@@ -826,10 +826,10 @@ int fxc_get_visibilities_device(fxc_ctx* x, float* d_vis, int normalize)
 
 int fxc_get_visibilities(fxc_ctx* x, float* vis, int* counts, int normalize)
 {
-    if (!x || !vis) return FXC_ERR_INVALID;
+    if (!x || (!vis && !counts)) return FXC_ERR_INVALID;
     FXC_CK(cudaSetDevice(x->device));
-    // one subband at a time through a one-subband device buffer
-    for (int sb = 0; sb < x->cfg.nsubband; sb++) {
+    // one subband at a time through a one-subband device buffer (vis null: counts only)
+    for (int sb = 0; vis && sb < x->cfg.nsubband; sb++) {
         const int st = finalize_subbands(x, sb, 1, reinterpret_cast<float*>(x->d_vis), normalize);
         if (st != FXC_OK) return st;
         FXC_CK(cudaMemcpyAsync(reinterpret_cast<char*>(vis) + (size_t)sb * x->vis_bytes, x->d_vis, x->vis_bytes,

@@ -10,6 +10,7 @@
  * unknown keywords and carries on, so files with these additional keywords stay
  * readable by it:
  *   XMODE PLAIN|TC|FP8   X-stage form
+ *   FSTAGE FFT|TC32|TC16 F-stage arithmetic (fxc_config.fstage; default FFT)
  *   NSUBBAND n           subbands per antenna: the antenna's file name holds one
  *                        printf "%d" replaced by the subband index 0..n-1
  *   SBSPACING hz         LO step between subbands (default BANDWIDTH)
@@ -21,7 +22,8 @@
  * shifted to the subintegration's first FFT.  A reader thread fills one pinned
  * buffer set while the GPU correlates the other.
  *
- * usage: fxcorr_main [config.conf] [-o vis.out] [-b vis.bin] [-x plain|tc|fp8] [-s nsubint] [-n]
+ * usage: fxcorr_main [config.conf] [-o vis.out] [-b vis.bin] [-x plain|tc|fp8] [-f fft|tc32|tc16]
+ *                    [-s nsubint] [-n]
  *   -o  text output; with several subintegrations one file per subintegration,
  *       named <out>.<s>
  *   -b  also write all visibilities (crosses then autos) and counts in binary, one
@@ -50,8 +52,17 @@ static int parse_xmode(const char* v)
     return FXC_X_PLAIN_FP32;
 }
 
+/* F-stage arithmetic by name: TC32 (FP32-grade tensor cores), TC16 (FP16 tensor cores),
+ * anything else the FP32 FFT */
+static int parse_fstage(const char* v)
+{
+    if (!strcasecmp(v, "TC32")) return FXC_F_TC32;
+    if (!strcasecmp(v, "TC16")) return FXC_F_TC16;
+    return FXC_F_FFT32;
+}
+
 typedef struct {
-    int nbit, npol, iscomplex, nchan, nant, numffts, xmode, nsubband, nsubint;
+    int nbit, npol, iscomplex, nchan, nant, numffts, xmode, fstage, nsubband, nsubint;
     double lo, bw, sbspacing;
     char** names;
     char** files;
@@ -70,6 +81,7 @@ static int parse_conf(const char* path, conf_t* c)
     c->npol = 2;
     c->nbit = 2;
     c->xmode = FXC_X_PLAIN_FP32;
+    c->fstage = FXC_F_FFT32;
     c->nsubband = 1;
     c->nsubint = 1;
     c->sbspacing = -1.0;
@@ -129,6 +141,8 @@ static int parse_conf(const char* path, conf_t* c)
             c->numffts = atoi(val);
         } else if (!strcasecmp(tok, "XMODE")) {
             c->xmode = parse_xmode(val);
+        } else if (!strcasecmp(tok, "FSTAGE")) {
+            c->fstage = parse_fstage(val);
         } else if (!strcasecmp(tok, "NSUBBAND")) {
             c->nsubband = atoi(val);
         } else if (!strcasecmp(tok, "SBSPACING")) {
@@ -235,18 +249,23 @@ int main(int argc, char** argv)
     const char* conf_path = "./test.conf";
     const char* out_path = "vis.out";
     const char* bin_path = NULL;
-    int xmode_cli = -1, normalize = 1, nsubint_cli = 0;
+    int xmode_cli = -1, fstage_cli = -1, normalize = 1, nsubint_cli = 0;
     for (int i = 1; i < argc; i++) {
         if (!strcmp(argv[i], "-o") && i + 1 < argc) out_path = argv[++i];
         else if (!strcmp(argv[i], "-b") && i + 1 < argc) bin_path = argv[++i];
         else if (!strcmp(argv[i], "-x") && i + 1 < argc) {
             i++;
             xmode_cli = parse_xmode(argv[i]);
+        } else if (!strcmp(argv[i], "-f") && i + 1 < argc) {
+            i++;
+            fstage_cli = parse_fstage(argv[i]);
         } else if (!strcmp(argv[i], "-s") && i + 1 < argc) nsubint_cli = atoi(argv[++i]);
         else if (!strcmp(argv[i], "-n")) normalize = 0;
         else if (argv[i][0] != '-') conf_path = argv[i];
         else {
-            fprintf(stderr, "usage: %s [config.conf] [-o vis.out] [-b vis.bin] [-x plain|tc|fp8] [-s nsubint] [-n]\n",
+            fprintf(stderr,
+                    "usage: %s [config.conf] [-o vis.out] [-b vis.bin] [-x plain|tc|fp8] [-f fft|tc32|tc16] "
+                    "[-s nsubint] [-n]\n",
                     argv[0]);
             return 1;
         }
@@ -265,6 +284,7 @@ int main(int argc, char** argv)
     cfg.lo = c.lo;
     cfg.bw = c.bw;
     cfg.xmode = xmode_cli >= 0 ? xmode_cli : c.xmode;
+    cfg.fstage = fstage_cli >= 0 ? fstage_cli : c.fstage;
     cfg.nsubband = c.nsubband;
     cfg.sb_spacing = c.sbspacing;
     const int nsubint = nsubint_cli > 0 ? nsubint_cli : c.nsubint;

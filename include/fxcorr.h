@@ -168,7 +168,8 @@ int fxc_device_input(fxc_ctx* ctx, uint8_t** d_data, size_t* pitch);
  * interleaved float pairs, layout [sb][bl][2*l + m][chan] with bl = crosses in
  * the reference's order then autos; counts (nbl + nant ints, may be NULL) get
  * the number of FFTs accumulated per baseline.  normalize != 0 divides each
- * baseline by its count (processNormalize, kernel.c:348-359). */
+ * baseline by its count (processNormalize, kernel.c:348-359).  vis may be NULL
+ * when counts is not: the counts alone (e.g. beside fxc_get_visibilities_device). */
 int fxc_get_visibilities(fxc_ctx* ctx, float* vis, int* counts, int normalize);
 
 /* Same into device memory (d_vis: fxc_vis_count complex values). */
