@@ -26,10 +26,95 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
+// acc[ii][jj] += sum over the TK FFTs of a stage of xi[ii] * conj(xj[jj]) for one 8 x 8 tile of
+// signal pairs (kernel.c:829-854; the conjugation of kernel.c:557-568 folded in).  pi / pj point at
+// FFT 0 of the tile's first row / column signal in the stage; signals are SK elements apart, FFTs
+// TKS.  The operands of FFT tk + 1 are loaded while FFT tk's 256 FMAs run, so the shared-memory
+// latency hides behind independent arithmetic at two warps per scheduler.
+template <int TK, int SK, int TKS>
+__device__ __forceinline__ void tile_stage(float2 (&acc)[8][8], const float2* pi, const float2* pj)
+{
+    float2 a[8], b[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        a[k] = pi[k * SK];
+        b[k] = pj[k * SK];
+    }
+#pragma unroll 2
+    for (int tk = 0; tk < TK; tk++) {
+        const int tn = (tk + 1 < TK ? tk + 1 : tk) * TKS;   // the last FFT reloads itself (unused)
+        float2 na[8], nb[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            na[k] = pi[tn + k * SK];
+            nb[k] = pj[tn + k * SK];
+        }
+#pragma unroll
+        for (int jj = 0; jj < 8; jj++)
+#pragma unroll
+            for (int ii = 0; ii < 8; ii++) {
+                acc[ii][jj].x = fmaf(a[ii].x, b[jj].x, fmaf(a[ii].y, b[jj].y, acc[ii][jj].x));
+                acc[ii][jj].y = fmaf(a[ii].y, b[jj].x, fmaf(-a[ii].x, b[jj].y, acc[ii][jj].y));
+            }
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            a[k] = na[k];
+            b[k] = nb[k];
+        }
+    }
+}
+
+// The upper triangles (ii <= jj, index jj (jj + 1) / 2 + ii) of two diagonal 8 x 8 blocks, A at
+// pa and B at pb: 72 pairs, the work of one tile, with the same operand prefetch.
+template <int TK, int SK, int TKS>
+__device__ __forceinline__ void diag_pair_stage(float2 (&acc)[2][36], const float2* pa, const float2* pb)
+{
+    float2 a[8], b[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        a[k] = pa[k * SK];
+        b[k] = pb[k * SK];
+    }
+#pragma unroll 2
+    for (int tk = 0; tk < TK; tk++) {
+        const int tn = (tk + 1 < TK ? tk + 1 : tk) * TKS;
+        float2 na[8], nb[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            na[k] = pa[tn + k * SK];
+            nb[k] = pb[tn + k * SK];
+        }
+#pragma unroll
+        for (int jj = 0; jj < 8; jj++)
+#pragma unroll
+            for (int ii = 0; ii <= jj; ii++) {
+                float2& u = acc[0][jj * (jj + 1) / 2 + ii];
+                float2& v = acc[1][jj * (jj + 1) / 2 + ii];
+                u.x = fmaf(a[ii].x, a[jj].x, fmaf(a[ii].y, a[jj].y, u.x));
+                u.y = fmaf(a[ii].y, a[jj].x, fmaf(-a[ii].x, a[jj].y, u.y));
+                v.x = fmaf(b[ii].x, b[jj].x, fmaf(b[ii].y, b[jj].y, v.x));
+                v.y = fmaf(b[ii].y, b[jj].x, fmaf(-b[ii].x, b[jj].y, v.y));
+            }
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            a[k] = na[k];
+            b[k] = nb[k];
+        }
+    }
+}
+
+// Plan of one channel group: NB blocks of 8 signals.  With NB = 8 the 36 upper 8 x 8 tiles are
+// re-cut as 28 off-diagonal tiles plus 4 threads that each take the upper triangles of two
+// diagonal blocks (b, 7 - b): 32 equal threads per channel, so 8 channels fill 8 warps and each
+// thread keeps the registers for the prefetched operands (a scheduler's register file is shared
+// by its warps; 9 warps would leave 168 per thread).
 template <int NB, int CG, int TK>
 struct XPlan {
-    static constexpr int NTILE = NB * (NB + 1) / 2;
+    static constexpr bool PAIRED = NB == 8;
+    static constexpr int NOFF = NB * (NB - 1) / 2;
+    static constexpr int NTILE = PAIRED ? NOFF + NB / 2 : NB * (NB + 1) / 2;
     static constexpr int NTHREADS = CG * NTILE;
+    static constexpr bool PIPE = NTHREADS <= 256;           // prefetch only where the registers allow
     static constexpr int NS = NB * 8;                       // staged signals
     // element (s, tk, cl) at s*TK*CG + (s/8)*8 + tk*CG + cl  (64-byte skew per 8-signal block)
     static constexpr int STAGE = NS * TK * CG + NB * 8;     // float2 per buffer
@@ -41,23 +126,12 @@ __device__ __forceinline__ int xoff(int s, int tk, int cl)
     return s * TK * CG + (s >> 3) * 8 + tk * CG + cl;
 }
 
-// One X-stage block: channels [c0, c0 + CG) of subband sb over all T FFT slots.
-template <int NB, int CG, int TK>
-__device__ __forceinline__ void xplain_block(const XArgs& a, int sb, int c0, unsigned char* smem)
+// Stages of one X-stage block for one thread: tiles (DP false) or diagonal pairs (DP true).
+template <int NB, int CG, int TK, bool DP>
+__device__ __forceinline__ void xplain_stages(const XArgs& a, int sb, int c0, float2* xs, int tid, int cl, int I,
+                                              int J)
 {
     using P = XPlan<NB, CG, TK>;
-    float2* xs = reinterpret_cast<float2*>(smem);   // [2][STAGE]
-
-    const int tid = threadIdx.x;
-    const int tile = tid / CG;
-    const int cl = tid - tile * CG;
-    int I = 0, rem = tile;
-    while (rem >= NB - I) {
-        rem -= NB - I;
-        I++;
-    }
-    const int J = I + rem;
-
     const int nsig = a.nsig;
     const int C = a.nchan;
     const float2* spec = reinterpret_cast<const float2*>(a.spec) + (size_t)sb * nsig * a.T * C;
@@ -81,11 +155,17 @@ __device__ __forceinline__ void xplain_block(const XArgs& a, int sb, int c0, uns
         cp_async_commit();
     };
 
-    float2 acc[8][8];
+    // DP: upper triangles of diagonal blocks I and J; otherwise the I x J tile
+    float2 acc[DP ? 1 : 8][8];
+    float2 dacc[DP ? 2 : 1][36];
 #pragma unroll
-    for (int i = 0; i < 8; i++)
+    for (int i = 0; i < (DP ? 1 : 8); i++)
 #pragma unroll
         for (int j = 0; j < 8; j++) acc[i][j] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int h = 0; h < (DP ? 2 : 1); h++)
+#pragma unroll
+        for (int i = 0; i < 36; i++) dacc[h][i] = make_float2(0.f, 0.f);
 
     const int nblk = (a.ntk ? a.ntk : a.T) / TK;
     issue(0, 0);
@@ -98,18 +178,27 @@ __device__ __forceinline__ void xplain_block(const XArgs& a, int sb, int c0, uns
         }
         __syncthreads();
         const float2* x = xs + (blk & 1) * P::STAGE;
-        for (int tk = 0; tk < TK; tk++) {
-            float2 xi[8];
+        // within a block of 8 signals the skew is constant: signal s + k is k * TK * CG further
+        const float2* pi = x + xoff<NB, CG, TK>(I * 8, 0, cl);
+        const float2* pj = x + xoff<NB, CG, TK>(J * 8, 0, cl);
+        if constexpr (DP) {
+            diag_pair_stage<TK, TK * CG, CG>(dacc, pi, pj);
+        } else if constexpr (P::PIPE) {
+            tile_stage<TK, TK * CG, CG>(acc, pi, pj);
+        } else {
+            for (int tk = 0; tk < TK; tk++) {
+                float2 xi[8];
 #pragma unroll
-            for (int ii = 0; ii < 8; ii++) xi[ii] = x[xoff<NB, CG, TK>(I * 8 + ii, tk, cl)];
+                for (int ii = 0; ii < 8; ii++) xi[ii] = pi[ii * TK * CG + tk * CG];
 #pragma unroll
-            for (int jj = 0; jj < 8; jj++) {
-                const float2 xj = x[xoff<NB, CG, TK>(J * 8 + jj, tk, cl)];
+                for (int jj = 0; jj < 8; jj++) {
+                    const float2 xj = pj[jj * TK * CG + tk * CG];
 #pragma unroll
-                for (int ii = 0; ii < 8; ii++) {
-                    // acc += xi * conj(xj)
-                    acc[ii][jj].x = fmaf(xi[ii].x, xj.x, fmaf(xi[ii].y, xj.y, acc[ii][jj].x));
-                    acc[ii][jj].y = fmaf(xi[ii].y, xj.x, fmaf(-xi[ii].x, xj.y, acc[ii][jj].y));
+                    for (int ii = 0; ii < 8; ii++) {
+                        // acc += xi * conj(xj)
+                        acc[ii][jj].x = fmaf(xi[ii].x, xj.x, fmaf(xi[ii].y, xj.y, acc[ii][jj].x));
+                        acc[ii][jj].y = fmaf(xi[ii].y, xj.x, fmaf(-xi[ii].x, xj.y, acc[ii][jj].y));
+                    }
                 }
             }
         }
@@ -118,22 +207,77 @@ __device__ __forceinline__ void xplain_block(const XArgs& a, int sb, int c0, uns
 
     float2* out = reinterpret_cast<float2*>(a.acc);
     const int npair = nsig * (nsig + 1) / 2;
+    if constexpr (DP) {
 #pragma unroll
-    for (int ii = 0; ii < 8; ii++) {
-        const int i = I * 8 + ii;
+        for (int h = 0; h < 2; h++) {
+            const int B = h ? J : I;
 #pragma unroll
-        for (int jj = 0; jj < 8; jj++) {
-            const int j = J * 8 + jj;
-            if (i <= j && j < nsig) {
-                const int p = i * nsig - (i * (i - 1)) / 2 + (j - i);
-                float2* o = out + ((size_t)sb * npair + p) * C + c0 + cl;
-                float2 cur = *o;
-                cur.x += acc[ii][jj].x;
-                cur.y += acc[ii][jj].y;
-                *o = cur;
+            for (int jj = 0; jj < 8; jj++)
+#pragma unroll
+                for (int ii = 0; ii <= jj; ii++) {
+                    const int i = B * 8 + ii, j = B * 8 + jj;
+                    if (j < nsig) {
+                        const int p = i * nsig - (i * (i - 1)) / 2 + (j - i);
+                        float2* o = out + ((size_t)sb * npair + p) * C + c0 + cl;
+                        float2 cur = *o;
+                        cur.x += dacc[h][jj * (jj + 1) / 2 + ii].x;
+                        cur.y += dacc[h][jj * (jj + 1) / 2 + ii].y;
+                        *o = cur;
+                    }
+                }
+        }
+    } else {
+#pragma unroll
+        for (int ii = 0; ii < 8; ii++) {
+            const int i = I * 8 + ii;
+#pragma unroll
+            for (int jj = 0; jj < 8; jj++) {
+                const int j = J * 8 + jj;
+                if (i <= j && j < nsig) {
+                    const int p = i * nsig - (i * (i - 1)) / 2 + (j - i);
+                    float2* o = out + ((size_t)sb * npair + p) * C + c0 + cl;
+                    float2 cur = *o;
+                    cur.x += acc[ii][jj].x;
+                    cur.y += acc[ii][jj].y;
+                    *o = cur;
+                }
             }
         }
     }
+}
+
+// One X-stage block: channels [c0, c0 + CG) of subband sb over all T FFT slots.
+template <int NB, int CG, int TK>
+__device__ __forceinline__ void xplain_block(const XArgs& a, int sb, int c0, unsigned char* smem)
+{
+    using P = XPlan<NB, CG, TK>;
+    float2* xs = reinterpret_cast<float2*>(smem);   // [2][STAGE]
+
+    const int tid = threadIdx.x;
+    const int tile = tid / CG;
+    const int cl = tid - tile * CG;
+    // tile -> block pair (I, J): off-diagonal I < J first when PAIRED, else the upper triangle I <= J;
+    // PAIRED tiles NOFF.. are diagonal pairs (I, NB - 1 - I) (whole warps: warp-uniform branches)
+    const bool dpair = P::PAIRED && tile >= P::NOFF;
+    int I = 0, J = 0;
+    if (dpair) {
+        I = tile - P::NOFF;
+        J = NB - 1 - I;
+    } else {
+        const int lead = P::PAIRED ? 1 : 0;   // off-diagonal rows hold NB - 1 - I tiles
+        int rem = tile;
+        while (rem >= NB - lead - I) {
+            rem -= NB - lead - I;
+            I++;
+        }
+        J = I + lead + rem;
+    }
+
+    // the two thread kinds in separate instantiations, so each keeps only its own accumulators
+    if (dpair)
+        xplain_stages<NB, CG, TK, true>(a, sb, c0, xs, tid, cl, I, J);
+    else
+        xplain_stages<NB, CG, TK, false>(a, sb, c0, xs, tid, cl, I, J);
 }
 
 template <int NB, int CG, int TK>
@@ -278,22 +422,8 @@ k_xplain_big(XArgs a)
         }
         __syncthreads();
         const float2* x = xs + (blk & 1) * STAGE;
-        if (active) {
-            for (int tk = 0; tk < TK; tk++) {
-                float2 xi[8];
-#pragma unroll
-                for (int ii = 0; ii < 8; ii++) xi[ii] = x[off(ti * 8 + ii, tk, cl)];
-#pragma unroll
-                for (int jj = 0; jj < 8; jj++) {
-                    const float2 xj = x[off(64 + tj * 8 + jj, tk, cl)];
-#pragma unroll
-                    for (int ii = 0; ii < 8; ii++) {
-                        acc[ii][jj].x = fmaf(xi[ii].x, xj.x, fmaf(xi[ii].y, xj.y, acc[ii][jj].x));
-                        acc[ii][jj].y = fmaf(xi[ii].y, xj.x, fmaf(-xi[ii].x, xj.y, acc[ii][jj].y));
-                    }
-                }
-            }
-        }
+        // 256 threads: two warps per scheduler, registers for the prefetched operands
+        if (active) tile_stage<TK, TK * CG, CG>(acc, x + off(ti * 8, 0, cl), x + off(64 + tj * 8, 0, cl));
         __syncthreads();
     }
     if (!active) return;
