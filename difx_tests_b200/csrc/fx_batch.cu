@@ -4,9 +4,11 @@
 //
 // Each job owns an ordinary context (device input, delay table, spectra chunk,
 // accumulators).  Per round r (spectra chunk r of every job that has one):
-//   one k_fstage_batch launch per F group  {FFT length, npol, FFTs per CTA}
-//   one k_xplain_batch launch per X group  {8-signal blocks, tile variant}
-// CTAs of a launch stride over a task table, so small and large jobs share the
+//   one k_fstage_batch launch per F group  {FFT length, npol, spectra precision, FFTs per CTA}
+//   one k_xplain_batch launch per X group  {8-signal blocks, tile variant} (plain form, <= 64 signals)
+//   one X launch per remaining job: the FP16 tensor-core X stage, or the plain X stage of
+//   more than 64 signals
+// CTAs of a grouped launch stride over a task table, so small and large jobs share the
 // machine inside one launch.  The delay tables and baseline counts run first.
 #include <algorithm>
 #include <cmath>
@@ -27,16 +29,17 @@ using namespace fx;
 namespace {
 
 struct FGroup {
-    int nchan, npol, tb;
+    int nchan, npol, mode, tb;   // mode: kSpecF32 (plain X) or kSpecF16 (tensor-core X)
     std::vector<int> jobs;
 };
 struct XGroup {
     int nsig8, alt;   // signal blocks of 8 (jobs with the same count share tile plans)
     std::vector<int> jobs;
 };
-struct Launch {       // one grouped launch of the recorded sequence
-    bool fstage;
-    int group;
+enum LaunchKind { kFGroup = 0, kXGroup = 1, kXJob = 2 };
+struct Launch {       // one launch of the recorded sequence
+    int kind;         // LaunchKind
+    int group;        // F / X group, or the job of a kXJob launch
     size_t task_off;  // into d_tasks (int4)
     int ntask;
 };
@@ -52,7 +55,11 @@ thread_local int g_batch_cuda = 0;
         }                                                                                 \
     } while (0)
 
-std::string fkey(int nchan, int npol) { return "F " + std::to_string(2 * nchan) + " " + std::to_string(npol); }
+// plan-cache keys as the single-job contexts write them ("F" FP32 spectra, "H" FP16)
+std::string fkey(int nchan, int npol, int mode)
+{
+    return std::string(mode == kSpecF16 ? "H " : "F ") + std::to_string(2 * nchan) + " " + std::to_string(npol);
+}
 std::string xkey(int nsig8) { return "X " + std::to_string(nsig8); }
 
 }  // namespace
@@ -63,7 +70,8 @@ struct fxc_batch {
     cudaStream_t own = nullptr, stream = nullptr;
     std::vector<FGroup> fg;
     std::vector<XGroup> xg;
-    std::vector<int> job_fg, job_xg;
+    std::vector<int> job_fg, job_xg;   // job_xg -1: the job's X stage is its own launch
+    std::vector<XArgs> xa_host;        // per job, for its own X launch
     int nrounds = 0;
     // device tables: FArgs [nrounds][J], XArgs [J], tasks (int4) for every recorded launch
     FArgs* d_fargs = nullptr;
@@ -115,9 +123,10 @@ static int build_tables(fxc_batch* b)
         x.nchan = c->cfg.nchan;
         x.nsb = c->cfg.nsubband;
         x.rows = c->rows;
-        x.alt = b->xg[b->job_xg[j]].alt;
+        x.alt = b->job_xg[j] >= 0 ? b->xg[b->job_xg[j]].alt : c->plan_alt;
         xa[j] = x;
     }
+    b->xa_host = xa;
     std::vector<int4> tasks;
     b->launches.clear();
     for (int r = 0; r < b->nrounds; r++) {
@@ -131,7 +140,7 @@ static int build_tables(fxc_batch* b)
                     for (int ant = 0; ant < c->cfg.nant; ant++)
                         for (int t0 = 0; t0 < c->T; t0 += tb) tasks.push_back(make_int4(r * J + j, sb, ant, t0));
             }
-            if (tasks.size() > off) b->launches.push_back({true, g, off, (int)(tasks.size() - off)});
+            if (tasks.size() > off) b->launches.push_back({kFGroup, g, off, (int)(tasks.size() - off)});
         }
         for (int g = 0; g < (int)b->xg.size(); g++) {
             const size_t off = tasks.size();
@@ -142,8 +151,10 @@ static int build_tables(fxc_batch* b)
                 for (int sb = 0; sb < c->cfg.nsubband; sb++)
                     for (int c0 = 0; c0 < c->cfg.nchan; c0 += cg) tasks.push_back(make_int4(j, sb, c0, 0));
             }
-            if (tasks.size() > off) b->launches.push_back({false, g, off, (int)(tasks.size() - off)});
+            if (tasks.size() > off) b->launches.push_back({kXGroup, g, off, (int)(tasks.size() - off)});
         }
+        for (int j = 0; j < J; j++)
+            if (b->job_xg[j] < 0 && r < nchunks(b->ctx[j])) b->launches.push_back({kXJob, j, 0, 0});
     }
     FB_CK(cudaSetDevice(b->device));
     cudaFree(b->d_fargs);
@@ -167,15 +178,28 @@ static int build_tables(fxc_batch* b)
 
 static int enqueue_launch(fxc_batch* b, const Launch& l)
 {
-    if (l.fstage) {
+    if (l.kind == kFGroup) {
         const FGroup& g = b->fg[l.group];
-        FB_CK(launch_fstage_batch(g.nchan, g.npol, kSpecF32, g.tb, b->d_fargs, b->d_tasks + l.task_off, l.ntask,
+        FB_CK(launch_fstage_batch(g.nchan, g.npol, g.mode, g.tb, b->d_fargs, b->d_tasks + l.task_off, l.ntask,
                                   b->stream));
-    } else {
+    } else if (l.kind == kXGroup) {
         const XGroup& g = b->xg[l.group];
         FB_CK(launch_xplain_batch(g.nsig8 * 8, g.alt, b->d_xargs, b->d_tasks + l.task_off, l.ntask, b->stream));
+    } else {
+        fxc_ctx* c = b->ctx[l.group];
+        const XArgs& x = b->xa_host[l.group];
+        FB_CK(c->cfg.xmode == FXC_X_TC_FP16 ? launch_xtc(x, c->d_err, c->nsm, b->stream) : launch_xplain(x, b->stream));
     }
     return FXC_OK;
+}
+
+// FFTs per CTA candidates of an F group: the F16 staging of tb FFTs must fit one CTA's shared memory
+static bool tb_fits(const fxc_batch* b, const FGroup& g, int tb)
+{
+    if (g.mode != kSpecF16) return true;
+    int optin = 0;
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device) != cudaSuccess) return false;
+    return fstage_smem_bytes(g.nchan, g.mode, g.npol, tb) <= (size_t)optin;
 }
 
 // The whole subintegration of every job: delay tables + counts, then the rounds.
@@ -201,8 +225,8 @@ int fxc_batch_create(const fxc_config* cfgs, int njobs, fxc_batch** out)
     if (!cfgs || njobs < 1 || !out) return FXC_ERR_INVALID;
     *out = nullptr;
     for (int j = 0; j < njobs; j++)
-        if (cfgs[j].xmode != FXC_X_PLAIN_FP32 || cfgs[j].nant * cfgs[j].npol > 64 || cfgs[j].window_ffts != 0 ||
-            cfgs[j].iscomplex)
+        if ((cfgs[j].xmode != FXC_X_PLAIN_FP32 && cfgs[j].xmode != FXC_X_TC_FP16) || cfgs[j].window_ffts != 0 ||
+            cfgs[j].iscomplex || (cfgs[j].fstage != FXC_F_AUTO && cfgs[j].fstage != FXC_F_FFT32))
             return FXC_ERR_UNSUPPORTED;
     fxc_batch* b = new fxc_batch();
     int st = FXC_OK;
@@ -224,16 +248,22 @@ int fxc_batch_create(const fxc_config* cfgs, int njobs, fxc_batch** out)
     const auto plans = plan_cache_load();
     for (int j = 0; j < njobs; j++) {
         const fxc_ctx* c = b->ctx[j];
+        const int mode = c->cfg.xmode == FXC_X_PLAIN_FP32 ? kSpecF32 : kSpecF16;
         int g = -1;
         for (int k = 0; k < (int)b->fg.size(); k++)
-            if (b->fg[k].nchan == c->cfg.nchan && b->fg[k].npol == c->cfg.npol) g = k;
+            if (b->fg[k].nchan == c->cfg.nchan && b->fg[k].npol == c->cfg.npol && b->fg[k].mode == mode) g = k;
         if (g < 0) {
-            const auto it = plans.find(fkey(c->cfg.nchan, c->cfg.npol));
-            b->fg.push_back({c->cfg.nchan, c->cfg.npol, it != plans.end() ? it->second : 16, {}});
+            const auto it = plans.find(fkey(c->cfg.nchan, c->cfg.npol, mode));
+            b->fg.push_back({c->cfg.nchan, c->cfg.npol, mode, it != plans.end() ? it->second : 16, {}});
             g = (int)b->fg.size() - 1;
+            while (b->fg[g].tb > 4 && !tb_fits(b, b->fg[g], b->fg[g].tb)) b->fg[g].tb /= 2;
         }
         b->fg[g].jobs.push_back(j);
         b->job_fg.push_back(g);
+        if (c->cfg.xmode != FXC_X_PLAIN_FP32 || c->nsig > 64) {
+            b->job_xg.push_back(-1);   // its own X launch
+            continue;
+        }
         const int n8 = (c->nsig + 7) / 8;
         int h = -1;
         for (int k = 0; k < (int)b->xg.size(); k++)
@@ -377,7 +407,7 @@ int fxc_batch_get_plan(fxc_batch* b, int job, int* fft_block, int* x_variant)
 {
     if (!b || job < 0 || job >= (int)b->ctx.size()) return FXC_ERR_INVALID;
     if (fft_block) *fft_block = b->fg[b->job_fg[job]].tb;
-    if (x_variant) *x_variant = b->xg[b->job_xg[job]].alt;
+    if (x_variant) *x_variant = b->job_xg[job] >= 0 ? b->xg[b->job_xg[job]].alt : b->ctx[job]->plan_alt;
     return FXC_OK;
 }
 
@@ -390,10 +420,10 @@ int fxc_batch_autotune(fxc_batch* b, int reps)
     FB_CK(cudaEventCreate(&e1));
     int st = FXC_OK;
     // time the round-0 launch of one group under each candidate plan
-    auto time_group = [&](bool fstage, int g, float* ms) -> int {
+    auto time_group = [&](int kind, int g, float* ms) -> int {
         if (!b->tables_valid && (st = build_tables(b)) != FXC_OK) return st;
         for (const Launch& l : b->launches) {
-            if (l.fstage != fstage || l.group != g) continue;
+            if (l.kind != kind || l.group != g) continue;
             if ((st = enqueue_launch(b, l)) != FXC_OK) return st;   // warm / sets attributes
             FB_CK(cudaEventRecord(e0, b->stream));
             for (int i = 0; i < reps; i++)
@@ -410,10 +440,11 @@ int fxc_batch_autotune(fxc_batch* b, int reps)
         int best = b->fg[g].tb;
         float best_ms = 1e30f;
         for (int tb : {8, 16, 32}) {
+            if (!tb_fits(b, b->fg[g], tb)) continue;
             b->fg[g].tb = tb;
             b->tables_valid = false;
             float ms = 0.f;
-            if ((st = time_group(true, g, &ms)) != FXC_OK) break;
+            if ((st = time_group(kFGroup, g, &ms)) != FXC_OK) break;
             if (ms < best_ms) {
                 best_ms = ms;
                 best = tb;
@@ -428,7 +459,7 @@ int fxc_batch_autotune(fxc_batch* b, int reps)
             b->xg[g].alt = alt;
             b->tables_valid = false;
             float ms = 0.f;
-            if ((st = time_group(false, g, &ms)) != FXC_OK) break;
+            if ((st = time_group(kXGroup, g, &ms)) != FXC_OK) break;
             if (ms < best_ms) {
                 best_ms = ms;
                 best = alt;
@@ -444,7 +475,7 @@ int fxc_batch_autotune(fxc_batch* b, int reps)
     if (st != FXC_OK) return st;
     {
         std::vector<std::string> lines;
-        for (const auto& g : b->fg) lines.push_back(fkey(g.nchan, g.npol) + " " + std::to_string(g.tb));
+        for (const auto& g : b->fg) lines.push_back(fkey(g.nchan, g.npol, g.mode) + " " + std::to_string(g.tb));
         for (const auto& g : b->xg) lines.push_back(xkey(g.nsig8) + " " + std::to_string(g.alt));
         plan_cache_append(lines);
     }

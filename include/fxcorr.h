@@ -49,7 +49,7 @@ extern "C" {
                                      channel by 448/absmax over each spectra chunk, FP32 accumulation */
 
 typedef struct fxc_config {
-    int nant;          /* antennas, >= 2; nant * npol <= 512 (the multi-job batch: <= 64) */
+    int nant;          /* antennas, >= 2; nant * npol <= 512 */
     int npol;          /* 1, or 2 = the reference's interleaved dual-polarisation format */
     int nchan;         /* channels per subband: power of two in [128, 4096]; FFT length 2*nchan */
     int nbit;          /* bits per sample: 2 (the reference's only unpacker, kernel.c:388-395) */
@@ -208,13 +208,16 @@ int fxc_correlate_noalloc(const fxc_config* cfg, const uint8_t* d_data, size_t p
 
 /* ---- many independent jobs in grouped persistent launches -------------------
  * A batch holds jobs of uneven geometry (antennas, polarisations, channels,
- * subbands, subintegration length).  fxc_batch_process runs every job's whole
- * subintegration: one persistent F-stage launch per group of jobs sharing FFT
- * length and polarisation count, one persistent X-stage launch per group sharing
- * an X tile plan (CTAs stride over a task table of {job, subband, antenna or
- * channel block}), in rounds when a job needs several spectra chunks.  The first
- * call runs eagerly; later calls replay one CUDA graph of the whole sequence.
- * Plain FP32 X stage, up to 64 signals per job (FXC_ERR_UNSUPPORTED otherwise).
+ * subbands, subintegration length) and X form (plain FP32 or FP16 tensor cores).
+ * fxc_batch_process runs every job's whole subintegration: one persistent
+ * F-stage launch per group of jobs sharing FFT length, polarisation count and
+ * spectra precision, one persistent plain X-stage launch per group of jobs of at
+ * most 64 signals sharing an X tile plan (CTAs stride over a task table of {job,
+ * subband, antenna or channel block}), and one X launch per other job (FP16
+ * tensor-core jobs, plain jobs of more than 64 signals), in rounds when a job
+ * needs several spectra chunks.  The first call runs eagerly; later calls replay
+ * one CUDA graph of the whole sequence.  FXC_ERR_UNSUPPORTED for the FP8 form,
+ * input windows, 8-bit complex input and the tensor-core F stages.
  * No counterpart in the reference (one job per run).
  * fxc_batch_autotune times the FFT block size (8/16/32 FFTs per CTA) of every
  * F group and the tile variant of every X group on the uploaded data, keeps the

@@ -142,3 +142,49 @@ def test_graph_off_matches(jobs_and_refs):
         b.process()
         for k in range(len(jobs) - 3):
             np.testing.assert_array_equal(b.visibilities(k)[0], refs[3 + k][0])
+
+
+# mixed batch: FP16 tensor-core jobs (their spectra from a grouped F16 F-stage launch, their X
+# stage its own launch inside the graph) and a plain job of more than 64 signals beside plain
+# grouped jobs
+MIXED = [
+    dict(nant=6, npol=1, nchan=1024, nsubband=2, numffts=150, xmode=fx.FXC_X_TC_FP16),
+    dict(nant=40, npol=2, nchan=256, nsubband=1, numffts=96, xmode=fx.FXC_X_PLAIN_FP32),   # 80 signals
+    dict(nant=9, npol=1, nchan=1024, nsubband=1, numffts=200, xmode=fx.FXC_X_PLAIN_FP32),
+    dict(nant=20, npol=2, nchan=512, nsubband=1, numffts=64, xmode=fx.FXC_X_TC_FP16),
+]
+TC_RMS_TOL = 1e-3
+
+
+def test_mixed_batch_tc_and_large_jobs_vs_oracle():
+    jobs, cfgs = [], []
+    for i, p in enumerate(MIXED):
+        j = synth.make_job(nant=p["nant"], npol=p["npol"], nchan=p["nchan"], numffts=p["numffts"], bw=32e6,
+                           lo=1.4e9, rho=0.1, seed=300 + i, nsubband=p["nsubband"])
+        jobs.append(j)
+        cfgs.append(fx.make_config(j.nant, j.nchan, j.numffts, j.bw, j.lo, npol=j.npol, nsubband=j.nsubband,
+                                   sb_spacing=j.bw, xmode=p["xmode"]))
+    with fx.Batch(cfgs) as b:
+        load(b, jobs)
+        for _ in range(3):               # eager, captured, replayed
+            b.reset()
+            b.process()
+        for i, (j, p) in enumerate(zip(jobs, MIXED)):
+            vis, counts = b.visibilities(i)
+            for sb in range(j.nsubband):
+                ref, rc = fo.correlate(j.data[sb], j.delays, j.fileoffsets, j.bw, float(j.sb_lo[sb]), j.nchan,
+                                       j.npol, numffts=j.numffts, maxoffset_ffts=j.numffts)
+                np.testing.assert_array_equal(counts, rc)
+                mx, rms = fo.vis_error(vis[sb], ref)
+                if p["xmode"] == fx.FXC_X_TC_FP16:
+                    assert rms.max() < TC_RMS_TOL, f"job {i} sb {sb}: rms {rms.max():.3e}"
+                else:
+                    assert mx.max() < VIS_TOL, f"job {i} sb {sb}: max {mx.max():.3e}"
+        b.autotune(reps=1)               # F16 groups only try blocks whose staging fits
+        b.reset()
+        b.process()
+        vis, _ = b.visibilities(0)
+        with fx.Correlator(cfgs[0]) as c:
+            c.process(jobs[0].data, jobs[0].delays, jobs[0].fileoffsets)
+            mx, rms = fo.vis_error(vis[0], c.visibilities()[0][0])
+        assert rms.max() < 1e-5          # same F16 spectra, chunked differently: accumulation order only
