@@ -105,10 +105,10 @@ def test_batch_arguments_rejected():
     cfg = fx.make_config(4, 256, 64, 32e6, 1.4e9)
     assert L.fxc_batch_create(None, 1, C.byref(out)) == fx.FXC_ERR_INVALID
     assert L.fxc_batch_create(C.byref(cfg), 0, C.byref(out)) == fx.FXC_ERR_INVALID
-    tc = fx.make_config(4, 256, 64, 32e6, 1.4e9, xmode=fx.FXC_X_TC_FP16)
-    assert L.fxc_batch_create(C.byref(tc), 1, C.byref(out)) == fx.FXC_ERR_UNSUPPORTED
-    big = fx.make_config(40, 256, 64, 32e6, 1.4e9)   # 80 signals: single-job path only
-    assert L.fxc_batch_create(C.byref(big), 1, C.byref(out)) == fx.FXC_ERR_UNSUPPORTED
+    # forms the batch does not run: FP8 X, input windows, the tensor-core F stages
+    for kw in (dict(xmode=fx.FXC_X_TC_FP8), dict(window_ffts=64), dict(fstage=fx.FXC_F_TC32)):
+        unsup = fx.make_config(4, 256, 64, 32e6, 1.4e9, **kw)
+        assert L.fxc_batch_create(C.byref(unsup), 1, C.byref(out)) == fx.FXC_ERR_UNSUPPORTED
     bad = fx.make_config(4, 300, 64, 32e6, 1.4e9)
     assert L.fxc_batch_create(C.byref(bad), 1, C.byref(out)) == fx.FXC_ERR_INVALID
     assert not out.value
