@@ -138,9 +138,7 @@ static int validate(const fxc_config* c)
     if (c->fstage == FXC_F_TC16 &&
         !(c->xmode != FXC_X_PLAIN_FP32 && c->nchan == 1024 && c->npol == 1 && !c->iscomplex))
         return FXC_ERR_UNSUPPORTED;
-    if (c->fstage == FXC_F_TC32 &&
-        !(c->xmode != FXC_X_TC_FP8 && c->nchan == 1024 && c->npol == 1 && !c->iscomplex))
-        return FXC_ERR_UNSUPPORTED;
+    if (c->fstage == FXC_F_TC32 && !(c->nchan == 1024 && c->npol == 1 && !c->iscomplex)) return FXC_ERR_UNSUPPORTED;
     return FXC_OK;
 }
 

@@ -38,7 +38,7 @@ cudaError_t launch_fstage(int nchan, int mode, const FArgs& a, cudaStream_t st)
         return launch_ftc(a, st);
     }
     if (a.fkind == FXC_F_TC32) {
-        if (!ftc32_supported(nchan, a)) return cudaErrorInvalidValue;
+        if (!ftc32_supported(nchan, mode, a)) return cudaErrorInvalidValue;
         return launch_ftc32(mode, a, st);
     }
     switch (a.cpx ? nchan : 2 * nchan) {   // FFT length: complex samples fill every bin

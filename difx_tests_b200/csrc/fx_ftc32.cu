@@ -17,8 +17,9 @@
 //            e^{i alpha k1} times sub[n2], a complex recurrence over k1 restarted at k1 = 16)
 //   step 2   D2[(k1 % 16, b)][(k2, re|im)] = A2 . B2^T, A2 = Z in shared memory, M128 N64 K128,
 //            x3 products, k2 < 32 (channels < 1024)
-//   output   X = D2 * fstep[k2] -> FP16 K-major spectra (tensor-core X forms) or FP32
-//            channel-contiguous spectra (plain form and the spectra check)
+//   output   X = D2 * fstep[k2] -> FP16 K-major spectra (tensor-core X forms; for the FP8 form also
+//            the absmax of each (channel, signal) over the chunk) or FP32 channel-contiguous
+//            spectra (plain form and the spectra check)
 // b = the FFT within a work item of 8 consecutive FFTs of one (subband, antenna).
 //
 // Persistent, warp-specialised CTA (one per SM, 576 threads):
@@ -101,7 +102,7 @@ __device__ __forceinline__ float2 cis_half_turns_acc(float x)
     return make_float2(c, s);
 }
 
-template <bool OUT16>
+template <bool OUT16, bool AMAX>
 __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a)
 {
     using namespace tc;
@@ -374,6 +375,16 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a)
                         pk[0] = __low2half(hv);
                         pk[a.T] = __high2half(hv);
                         pk += kstep;
+                        if constexpr (AMAX) {
+                            // max(|Re|, |Im|) of the stored values over the item's 8 FFTs: the 8 lanes
+                            // b = 0..7 of a channel are consecutive (lane = 8 (kl % 4) + b)
+                            const __half2 ah = __habs2(hv);
+                            uint32_t m = __float_as_uint(fmaxf(__low2float(ah), __high2float(ah)));
+                            m = max(m, __shfl_xor_sync(0xffffffffu, m, 1));
+                            m = max(m, __shfl_xor_sync(0xffffffffu, m, 2));
+                            m = max(m, __shfl_xor_sync(0xffffffffu, m, 4));
+                            if (b == 0 && m) atomicMax(a.amax + ((size_t)it.sb * C + k1 + F1 * k2) * nsig + it.ant, m);
+                        }
                     }
                 } else {
                     float2* pk = reinterpret_cast<float2*>(a.spec) +
@@ -529,9 +540,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a)
 
 }  // namespace ftc32
 
-bool ftc32_supported(int nchan, const FArgs& a)
+bool ftc32_supported(int nchan, int mode, const FArgs& a)
 {
-    return nchan == ftc32::C && a.npol == 1 && !a.cpx && a.amax == nullptr && a.T % ftc32::TB == 0 &&
+    return nchan == ftc32::C && a.npol == 1 && !a.cpx && (a.amax == nullptr || mode == kSpecF16) &&
+           a.T % ftc32::TB == 0 &&
            (a.tspan ? a.tspan : a.T) % ftc32::TB == 0 && a.err != nullptr;
 }
 
@@ -548,14 +560,18 @@ cudaError_t launch_ftc32(int mode, const FArgs& a, cudaStream_t st)
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
     const int grid = (int)(ntask < nsm ? ntask : nsm);
-    if (mode == kSpecF16) {
+    if (mode == kSpecF16 && a.amax) {
         static unsigned configured = 0;
-        if ((e = set_smem_once(k_ftc32<true>, sm, &configured)) != cudaSuccess) return e;
-        k_ftc32<true><<<grid, NTHREADS, sm, st>>>(a);
+        if ((e = set_smem_once(k_ftc32<true, true>, sm, &configured)) != cudaSuccess) return e;
+        k_ftc32<true, true><<<grid, NTHREADS, sm, st>>>(a);
+    } else if (mode == kSpecF16) {
+        static unsigned configured = 0;
+        if ((e = set_smem_once(k_ftc32<true, false>, sm, &configured)) != cudaSuccess) return e;
+        k_ftc32<true, false><<<grid, NTHREADS, sm, st>>>(a);
     } else {
         static unsigned configured = 0;
-        if ((e = set_smem_once(k_ftc32<false>, sm, &configured)) != cudaSuccess) return e;
-        k_ftc32<false><<<grid, NTHREADS, sm, st>>>(a);
+        if ((e = set_smem_once(k_ftc32<false, false>, sm, &configured)) != cudaSuccess) return e;
+        k_ftc32<false, false><<<grid, NTHREADS, sm, st>>>(a);
     }
     return cudaGetLastError();
 }

@@ -25,7 +25,7 @@ cudaError_t launch_fstage(int nchan, int mode, const FArgs& a, cudaStream_t st);
 bool ftc_supported(int nchan, int mode, const FArgs& a);
 cudaError_t launch_ftc(const FArgs& a, cudaStream_t st);
 // FP32-grade tensor-core F stage (error-compensated FP16 pairs), same geometry, F16 or F32 layout
-bool ftc32_supported(int nchan, const FArgs& a);
+bool ftc32_supported(int nchan, int mode, const FArgs& a);
 cudaError_t launch_ftc32(int mode, const FArgs& a, cudaStream_t st);
 size_t fstage_smem_bytes(int nchan, int mode, int npol, int tb);
 cudaError_t launch_fstage_batch(int nchan, int npol, int mode, int tb, const FArgs* d_jobs, const int4* d_tasks,

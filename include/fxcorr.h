@@ -86,8 +86,8 @@ typedef struct fxc_config {
  *   FXC_F_TC32   FP32-grade DFT on the tensor cores: the same two tcgen05 GEMMs with every FP16
  *                operand an error-compensated pair (hi + lo) and three products per GEMM
  *                (hi.hi + lo.hi + hi.lo, FP32 accumulation): spectra within ~2e-7 of max|X|, as
- *                the FP32 FFT.  Plain and FP16 tensor-core X forms at 1024 channels, one
- *                polarisation, 2-bit real input (FXC_ERR_UNSUPPORTED otherwise). */
+ *                the FP32 FFT.  Every X form at 1024 channels, one polarisation, 2-bit real
+ *                input (FXC_ERR_UNSUPPORTED otherwise). */
 #define FXC_F_AUTO   0
 #define FXC_F_FFT32  1
 #define FXC_F_TC16   2

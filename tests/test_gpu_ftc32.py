@@ -115,9 +115,23 @@ def test_tc32_window_only_context_vs_oracle():
     assert rms.max() < TC_RMS_TOL and mx.max() < TC_MAX_TOL, f"rms {rms.max():.3e} max {mx.max():.3e}"
 
 
+def test_tc32_fp8_form_matches_the_fft_fstage():
+    """The FP8 form's per-(channel, signal) absmax comes from the output warps of the tensor-core F
+    stage: the e4m3 correlation equals the one on the FP32 FFT F stage up to the quantisation."""
+    job = synth.make_job(nant=20, npol=1, nchan=1024, numffts=256, bw=64e6, lo=1.4e9, rho=0.1, seed=13)
+    v32, c32 = run(job, xmode=fx.FXC_X_TC_FP8)
+    vff, cff = run(job, xmode=fx.FXC_X_TC_FP8, fstage=fx.FXC_F_FFT32)
+    np.testing.assert_array_equal(c32, cff)
+    mx, rms = fo.vis_error(v32[0], vff[0])
+    assert rms.max() < 0.05, f"rms {rms.max():.3e}"
+    ref, rc = oracle_vis(job)
+    mx, rms = fo.vis_error(v32[0], ref)
+    assert rms.max() < 0.1, f"vs FP64: rms {rms.max():.3e}"
+
+
 def test_tc32_rejected_where_it_does_not_apply():
     for kw in (dict(nchan=512, npol=1, xmode=fx.FXC_X_TC_FP16), dict(nchan=1024, npol=2, xmode=fx.FXC_X_TC_FP16),
-               dict(nchan=1024, npol=1, xmode=fx.FXC_X_TC_FP8)):
+               dict(nchan=2048, npol=1, xmode=fx.FXC_X_PLAIN_FP32)):
         cfg = fx.make_config(4, kw["nchan"], 64, 64e6, 1.4e9, npol=kw["npol"], xmode=kw["xmode"],
                              fstage=fx.FXC_F_TC32)
         with pytest.raises(fx.FxcError) as e:
