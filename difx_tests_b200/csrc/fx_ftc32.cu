@@ -66,7 +66,7 @@ struct Smem {
     alignas(16) uint2 lut[NIB][2][F1][4];           // [pair % NIB][FFT][n1][code] (hi, lo) of level * step[n1]
     int2 pwin[NIB][2];                              // [pair % NIB][FFT] (bit of sample 0 in inb, valid)
     DelayEntry oent[2][TB];                         // output: delay entries [item parity][FFT]
-    float2 fstep[TB][K2H];                          // output: [b][k2]
+    float2 fstep[K2H][TB];                          // output: [k2][b] (a warp's 8 FFTs: one 64-byte row)
     float ctab[P::FS + P::FST];                     // chan_sub | chan_step
     uint64_t a1_full[NA1], a1_empty[NA1], d1_full[NPAIR], d1_empty[NPAIR];
     uint64_t a2_full[2], a2_empty[2], d2_full[2], d2_empty[2], drain;
@@ -187,9 +187,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a)
         for (int g = 0; g < npair; g++) {
             const int x = g % NIB, s = g % NA1;
             const uint32_t ph = (g / NIB) & 1;
-            const bool ok = mbar_wait(&sm.cp_full[x], ph, abort_flag) && mbar_wait(&sm.tab_full[x], ph, abort_flag) &&
-                            mbar_wait(&sm.a1_empty[s], ((g / NA1) & 1) ^ 1, abort_flag);
-            if (!__all_sync(0xffffffffu, ok)) {   // warp-uniform: the TMEM stores are .sync.aligned
+            const bool ok = mbar_wait_warp(&sm.cp_full[x], ph, abort_flag) &&
+                            mbar_wait_warp(&sm.tab_full[x], ph, abort_flag) &&
+                            mbar_wait_warp(&sm.a1_empty[s], ((g / NA1) & 1) ^ 1, abort_flag);
+            if (!ok) {   // warp-uniform: the TMEM stores are .sync.aligned
                 if (!*abort_flag) atomicCAS(a.err, 0, ERR_WAIT);
                 *abort_flag = 1;
                 break;
@@ -232,16 +233,19 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a)
         const int khalf = n2 >> 5;
         const uint32_t col = (uint32_t)(((n2 & 31) >> 2) << 4) + 4 * (n2 & 3);   // byte of (n2, re|im) in a row
         const float alpha_n2 = -6.283185307179586f * (float)n2 / (float)F;
+        // entries and subband LO of the next item, loaded one item ahead
         DelayEntry dn[2];
-        if (nitem > 0)
+        double lon = 0.0;
+        if (nitem > 0) {
             for (int u = 0; u < 2; u++) dn[u] = item_entry<TB>(a, 0, ntb, 2 * (h + 2 * u) + bsel);
+            lon = a.sb_lo[item_of<TB>(blockIdx.x, a.nant, ntb).sb];
+        }
         bool ok = true;
         for (int i = 0; i < nitem && ok; i++) {
-            const Item it = item_of<TB>(blockIdx.x + i * gridDim.x, a.nant, ntb);
             // per pair: start of the twiddle row at k1 = 0 and k1 = 16, and its step e^{i alpha}
             float2 st0[2], st16[2], rho[2];
             {
-                const double lo = a.sb_lo[it.sb];
+                const double lo = lon;
                 const double lofrac = lo - trunc(lo);
                 const bool fraclo = lofrac > 1e-11;   // kernel.c:39
 #pragma unroll
@@ -269,19 +273,21 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a)
                     }
                 }
             }
-            if (i + 1 < nitem)
+            if (i + 1 < nitem) {
                 for (int u = 0; u < 2; u++) dn[u] = item_entry<TB>(a, i + 1, ntb, 2 * (h + 2 * u) + bsel);
+                lon = a.sb_lo[item_of<TB>(blockIdx.x + (i + 1) * gridDim.x, a.nant, ntb).sb];
+            }
 #pragma unroll 1
             for (int j = 0; j < 2 && ok; j++) {
                 // tile j = k1 in [16 j, 16 j + 16) of every FFT of the item
-                if (!__all_sync(0xffffffffu, mbar_wait(&sm.a2_empty[j], (i & 1) ^ 1, abort_flag))) {
+                if (!mbar_wait_warp(&sm.a2_empty[j], (i & 1) ^ 1, abort_flag)) {
                     ok = false;
                     break;
                 }
 #pragma unroll
                 for (int u = 0; u < 2; u++) {
                     const int p = h + 2 * u;
-                    if (j == 0 && !__all_sync(0xffffffffu, mbar_wait(&sm.d1_full[p], i & 1, abort_flag))) {
+                    if (j == 0 && !mbar_wait_warp(&sm.d1_full[p], i & 1, abort_flag)) {
                         ok = false;
                         break;
                     }
@@ -296,18 +302,18 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a)
                     const int b = 2 * p + bsel;
                     float2 cur = j ? st16[u] : st0[u];
                     const float2 r = rho[u];
-                    uint8_t* hi = sm.a2[j][0][khalf];
-                    uint8_t* lo = sm.a2[j][1][khalf];
+                    // row R = 8 kk + b: R % 8 = b, so the swizzled byte is kk * 1024 + base
+                    const uint32_t base = (uint32_t)(b * 128) + (col ^ (uint32_t)(b << 4));
+                    uint8_t* hi = sm.a2[j][0][khalf] + base;
+                    uint8_t* lo = sm.a2[j][1][khalf] + base;
 #pragma unroll
                     for (int kk = 0; kk < 16; kk++) {
                         const float2 y = make_float2(__uint_as_float(v[2 * kk]), __uint_as_float(v[2 * kk + 1]));
                         const float2 z = cmul(y, cur);
                         cur = cmul(cur, r);
                         const uint2 zz = split_pair(z.x, z.y);
-                        const int R = 8 * kk + b;
-                        const uint32_t o = (uint32_t)(R * 128) + (col ^ (uint32_t)((R & 7) << 4));
-                        *reinterpret_cast<uint32_t*>(hi + o) = zz.x;
-                        *reinterpret_cast<uint32_t*>(lo + o) = zz.y;
+                        *reinterpret_cast<uint32_t*>(hi + kk * 1024) = zz.x;
+                        *reinterpret_cast<uint32_t*>(lo + kk * 1024) = zz.y;
                     }
                 }
                 if (!ok) break;
@@ -340,7 +346,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a)
                 const DelayEntry& d = sm.oent[i & 1][bb];
                 float sn = 0.f, cs = 0.f;
                 if (d.valid) sincosf(__fmul_rn(sm.ctab[P::FS + k2], __double2float_rn(d.frac)), &sn, &cs);
-                sm.fstep[bb][k2] = make_float2(cs, sn);   // kernel.c:512-523 (step part)
+                sm.fstep[k2][bb] = make_float2(cs, sn);   // kernel.c:512-523 (step part)
             }
             if (bar_or(2, 128, !ok || *abort_flag)) break;
             if (i + 1 < nitem) {
@@ -349,28 +355,32 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a)
             }
 #pragma unroll 1
             for (int j = 0; j < 2; j++) {
-                if (!__all_sync(0xffffffffu, mbar_wait(&sm.d2_full[j], i & 1, abort_flag))) {
+                if (!mbar_wait_warp(&sm.d2_full[j], i & 1, abort_flag)) {
                     ok = false;
                     break;
                 }
                 tc_fence_after();
-                uint32_t v[64];
-                tmem_ld32(tmem + lane_off + D2_COL + 64 * j, v);
-                tmem_ld32(tmem + lane_off + D2_COL + 64 * j + 32, v + 32);
-                tmem_wait_ld();
-                tc_fence_before();
-                mbar_arrive(&sm.d2_empty[j]);
                 const int k1 = 16 * j + kl;
-                const float2* fs = sm.fstep[b];
+                // two halves of 16 channels k2 (32 columns each), to keep the registers low
+#pragma unroll 1
+                for (int hf = 0; hf < 2; hf++) {
+                uint32_t v[32];
+                tmem_ld32(tmem + lane_off + D2_COL + 64 * j + 32 * hf, v);
+                tmem_wait_ld();
+                if (hf == 1) {
+                    tc_fence_before();
+                    mbar_arrive(&sm.d2_empty[j]);
+                }
                 if constexpr (OUT16) {
                     const size_t chan_stride = (size_t)a.rows * a.T;
-                    __half* pk = reinterpret_cast<__half*>(a.spec) + ((size_t)it.sb * C + k1) * chan_stride +
-                                 (size_t)(2 * it.ant) * a.T + it.tb0 + b;
                     const size_t kstep = (size_t)F1 * chan_stride;
+                    __half* pk = reinterpret_cast<__half*>(a.spec) + ((size_t)it.sb * C + k1) * chan_stride +
+                                 (size_t)(2 * it.ant) * a.T + it.tb0 + b + (size_t)(16 * hf) * kstep;
 #pragma unroll
-                    for (int k2 = 0; k2 < K2H; k2++) {
-                        const float2 y = cmul(make_float2(__uint_as_float(v[2 * k2]), __uint_as_float(v[2 * k2 + 1])),
-                                              fs[k2]);
+                    for (int kk = 0; kk < 16; kk++) {
+                        const int k2 = 16 * hf + kk;
+                        const float2 y = cmul(make_float2(__uint_as_float(v[2 * kk]), __uint_as_float(v[2 * kk + 1])),
+                                              sm.fstep[k2][b]);
                         const __half2 hv = __floats2half2_rn(y.x, y.y);
                         pk[0] = __low2half(hv);
                         pk[a.T] = __high2half(hv);
@@ -390,9 +400,12 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a)
                     float2* pk = reinterpret_cast<float2*>(a.spec) +
                                  (((size_t)it.sb * nsig + it.ant) * a.T + it.tb0 + b) * C + k1;
 #pragma unroll
-                    for (int k2 = 0; k2 < K2H; k2++)
-                        pk[F1 * k2] = cmul(make_float2(__uint_as_float(v[2 * k2]), __uint_as_float(v[2 * k2 + 1])),
-                                           fs[k2]);
+                    for (int kk = 0; kk < 16; kk++) {
+                        const int k2 = 16 * hf + kk;
+                        pk[F1 * k2] = cmul(make_float2(__uint_as_float(v[2 * kk]), __uint_as_float(v[2 * kk + 1])),
+                                           sm.fstep[k2][b]);
+                    }
+                }
                 }
             }
             if (!ok) break;
@@ -426,7 +439,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a)
             const double lo = lon;
             const uint8_t* row = rown;
             if (g + 1 < npair) fetch(g + 1, dn0, dn1, lon, rown);
-            if (!__all_sync(0xffffffffu, mbar_wait(&sm.tab_empty[x], ((g / NIB) & 1) ^ 1, abort_flag))) {
+            if (!mbar_wait_warp(&sm.tab_empty[x], ((g / NIB) & 1) ^ 1, abort_flag)) {
                 if (!*abort_flag) atomicCAS(a.err, 0, ERR_WAIT);
                 *abort_flag = 1;
                 break;

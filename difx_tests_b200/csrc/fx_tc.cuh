@@ -62,6 +62,17 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile
     }
 }
 
+// Bounded wait by a whole warp (warp-uniform result): lane 0 polls while the other lanes sleep in
+// the shuffle; once the phase has completed every lane observes it itself, for its own acquire
+// (a completed phase returns at once).  One polling thread per warp instead of 32.
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t* b, uint32_t parity, volatile int* abort_flag)
+{
+    bool ok = true;
+    if ((threadIdx.x & 31) == 0) ok = mbar_wait(b, parity, abort_flag);
+    ok = __shfl_sync(0xffffffffu, ok, 0) && mbar_wait(b, parity, abort_flag);
+    return __all_sync(0xffffffffu, ok);
+}
+
 // Bounded wait that ignores the abort flag (draining what this CTA itself issued).
 __device__ __forceinline__ bool mbar_drain(uint64_t* b, uint32_t parity)
 {
