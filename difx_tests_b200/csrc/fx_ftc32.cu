@@ -196,28 +196,27 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a)
                 break;
             }
             tc_fence_after();   // the MMAs that read this stage are complete
-            uint32_t hv[32], lv[32];
             const int2 wv = sm.pwin[x][bsel];
-            if (wv.y) {
-                // sample 64 n1 + n2 sits at bit wv.x + 128 n1 + 2 n2 of the staged window: the same
-                // shift for every n1, four words apart
-                const int bit = wv.x + 2 * n2;
-                const uint32_t* wp = reinterpret_cast<const uint32_t*>(sm.inb[x][bsel]) + (bit >> 5);
-                const int sh = bit & 31;
-                const uint2* lt = sm.lut[x][bsel][0];
+            // sample 64 n1 + n2 sits at bit wv.x + 128 n1 + 2 n2 of the staged window: the same shift
+            // for every n1, four words apart; two halves of 16 n1 (x_hi columns n1, x_lo 32 + n1)
+            const int bit = wv.x + 2 * n2;
+            const uint32_t* wp = reinterpret_cast<const uint32_t*>(sm.inb[x][bsel]) + (bit >> 5);
+            const int sh = bit & 31;
+            const uint2* lt = sm.lut[x][bsel][0];
 #pragma unroll
-                for (int n1 = 0; n1 < F1; n1++) {
-                    const uint2 e = lt[4 * n1 + ((wp[4 * n1] >> sh) & 3u)];
-                    hv[n1] = e.x;
-                    lv[n1] = e.y;
+            for (int hf = 0; hf < 2; hf++) {
+                uint32_t hv[16], lv[16];
+#pragma unroll
+                for (int k = 0; k < 16; k++) {
+                    const int n1 = 16 * hf + k;
+                    const uint2 e = wv.y ? lt[4 * n1 + ((wp[4 * n1] >> sh) & 3u)] : make_uint2(0u, 0u);
+                    hv[k] = e.x;
+                    lv[k] = e.y;
                 }
-            } else {
-#pragma unroll
-                for (int n1 = 0; n1 < F1; n1++) hv[n1] = lv[n1] = 0u;
+                if (hf == 1) mbar_arrive(&sm.tab_empty[x]);   // this thread's last read of slot x
+                tmem_st16(tmem + lane_off + A1_COL + 64 * s + 16 * hf, hv);
+                tmem_st16(tmem + lane_off + A1_COL + 64 * s + 32 + 16 * hf, lv);
             }
-            mbar_arrive(&sm.tab_empty[x]);   // this thread's last read of slot x
-            tmem_st32(tmem + lane_off + A1_COL + 64 * s, hv);
-            tmem_st32(tmem + lane_off + A1_COL + 64 * s + 32, lv);
             tmem_wait_st();
             tc_fence_before();
             mbar_arrive(&sm.a1_full[s]);
@@ -481,17 +480,18 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a)
                 }
     } else if (lane == 0) {
         // ================================================================ MMA issuer
-        bool ok = true;
+        // Issue order: step 1 of item 0, then per item i: step-2 tile 0 of i, step 1 of i + 1, step-2
+        // tile 1 of i.  Item i + 1's step-1 pairs reuse the D1 slots that the twiddle warps release
+        // while they write tile 1 of item i, so those warps find item i + 1's D1 ready instead of
+        // waiting behind a whole step-2 tile.
         const uint32_t sb1h = smem_u32(sm.b1[0]), sb1l = smem_u32(sm.b1[1]);
-        for (int i = 0; i < nitem && ok; i++) {
+        auto step1 = [&](int i) -> bool {
             for (int p = 0; p < NPAIR; p++) {
                 const int g = i * NPAIR + p;
                 const int s = g % NA1;
                 if (!mbar_wait(&sm.a1_full[s], (g / NA1) & 1, abort_flag) ||
-                    !mbar_wait(&sm.d1_empty[p], (i & 1) ^ 1, abort_flag)) {
-                    ok = false;
-                    break;
-                }
+                    !mbar_wait(&sm.d1_empty[p], (i & 1) ^ 1, abort_flag))
+                    return false;
                 tc_fence_after();
                 const uint32_t d1 = tmem + D1_COL + 64 * p, xa = tmem + A1_COL + 64 * s;
                 // x_hi . W_hi + x_lo . W_hi + x_hi . W_lo; K = 64 = 4 steps of 16 (8 columns,
@@ -506,30 +506,30 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a)
                 umma_commit(&sm.a1_empty[s]);
                 umma_commit(&sm.d1_full[p]);
             }
-            if (!ok) break;
+            return true;
+        };
+        auto step2 = [&](int i, int j) -> bool {
+            if (!mbar_wait(&sm.a2_full[j], i & 1, abort_flag) || !mbar_wait(&sm.d2_empty[j], (i & 1) ^ 1, abort_flag))
+                return false;
+            tc_fence_after();
+            const uint32_t d2 = tmem + D2_COL + 64 * j;
+            // Z_hi . W_hi + Z_lo . W_hi + Z_hi . W_lo; K = 128 = two 64-element halves
 #pragma unroll 1
-            for (int j = 0; j < 2; j++) {
-                if (!mbar_wait(&sm.a2_full[j], i & 1, abort_flag) ||
-                    !mbar_wait(&sm.d2_empty[j], (i & 1) ^ 1, abort_flag)) {
-                    ok = false;
-                    break;
-                }
-                tc_fence_after();
-                const uint32_t d2 = tmem + D2_COL + 64 * j;
-                // Z_hi . W_hi + Z_lo . W_hi + Z_hi . W_lo; K = 128 = two 64-element halves
-#pragma unroll 1
-                for (int t = 0; t < 3; t++) {
-                    const int la = t == 1 ? 1 : 0, lb = t == 2 ? 1 : 0;
+            for (int t = 0; t < 3; t++) {
+                const int la = t == 1 ? 1 : 0, lb = t == 2 ? 1 : 0;
 #pragma unroll
-                    for (int kk = 0; kk < 8; kk++)
-                        umma<false>(d2, umma_desc(smem_u32(sm.a2[j][la][kk >> 2]) + (kk & 3) * 32),
-                                    umma_desc(smem_u32(sm.b2[lb][kk >> 2]) + (kk & 3) * 32), kIdesc,
-                                    (t > 0 || kk > 0) ? 1u : 0u);
-                }
-                umma_commit(&sm.a2_empty[j]);
-                umma_commit(&sm.d2_full[j]);
+                for (int kk = 0; kk < 8; kk++)
+                    umma<false>(d2, umma_desc(smem_u32(sm.a2[j][la][kk >> 2]) + (kk & 3) * 32),
+                                umma_desc(smem_u32(sm.b2[lb][kk >> 2]) + (kk & 3) * 32), kIdesc,
+                                (t > 0 || kk > 0) ? 1u : 0u);
             }
-        }
+            umma_commit(&sm.a2_empty[j]);
+            umma_commit(&sm.d2_full[j]);
+            return true;
+        };
+        bool ok = nitem == 0 || step1(0);
+        for (int i = 0; i < nitem && ok; i++)
+            ok = step2(i, 0) && (i + 1 >= nitem || step1(i + 1)) && step2(i, 1);
         if (!ok) {
             if (!*abort_flag) atomicCAS(a.err, 0, ERR_WAIT);
             *abort_flag = 1;
