@@ -50,27 +50,38 @@ __device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity)
     return ok != 0;
 }
 
+// As mbar_try, but the thread may be suspended up to SUSPEND_NS waiting for the phase (it resumes
+// when the phase completes): a waiting warp issues a few instructions per wait, not a spin loop.
+constexpr uint32_t SUSPEND_NS = 20000;
+__device__ __forceinline__ bool mbar_try_suspend(uint64_t* b, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(b)), "r"(parity), "r"(SUSPEND_NS)
+        : "memory");
+    return ok != 0;
+}
+
 // Bounded wait: true when the phase completed, false after WAIT_NS or once *abort_flag is set.
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* abort_flag)
 {
     if (mbar_try(b, parity)) return true;
     const unsigned long long t0 = globaltimer();
     while (true) {
-        if (mbar_try(b, parity)) return true;
+        if (mbar_try_suspend(b, parity)) return true;
         if (*abort_flag) return false;
         if (globaltimer() - t0 > WAIT_NS) return false;
     }
 }
 
-// Bounded wait by a whole warp (warp-uniform result): lane 0 polls while the other lanes sleep in
-// the shuffle; once the phase has completed every lane observes it itself, for its own acquire
-// (a completed phase returns at once).  One polling thread per warp instead of 32.
+// Bounded wait by every lane of a warp, with a warp-uniform result.
 __device__ __forceinline__ bool mbar_wait_warp(uint64_t* b, uint32_t parity, volatile int* abort_flag)
 {
-    bool ok = true;
-    if ((threadIdx.x & 31) == 0) ok = mbar_wait(b, parity, abort_flag);
-    ok = __shfl_sync(0xffffffffu, ok, 0) && mbar_wait(b, parity, abort_flag);
-    return __all_sync(0xffffffffu, ok);
+    return __all_sync(0xffffffffu, mbar_wait(b, parity, abort_flag));
 }
 
 // Bounded wait that ignores the abort flag (draining what this CTA itself issued).
