@@ -32,74 +32,76 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // TKS.  The operands of FFT tk + 1 are loaded while FFT tk's 256 FMAs run, so the shared-memory
 // latency hides behind independent arithmetic at two warps per scheduler.
 template <int TK, int SK, int TKS>
-__device__ __forceinline__ void tile_stage(float2 (&acc)[8][8], const float2* pi, const float2* pj)
+__device__ __forceinline__ void tile_fma(float2 (&acc)[8][8], const float2 (&a)[8], const float2 (&b)[8])
 {
-    float2 a[8], b[8];
+#pragma unroll
+    for (int jj = 0; jj < 8; jj++)
+#pragma unroll
+        for (int ii = 0; ii < 8; ii++) {
+            acc[ii][jj].x = fmaf(a[ii].x, b[jj].x, fmaf(a[ii].y, b[jj].y, acc[ii][jj].x));
+            acc[ii][jj].y = fmaf(a[ii].y, b[jj].x, fmaf(-a[ii].x, b[jj].y, acc[ii][jj].y));
+        }
+}
+
+template <int SK>
+__device__ __forceinline__ void load8(float2 (&a)[8], float2 (&b)[8], const float2* pi, const float2* pj, int off)
+{
 #pragma unroll
     for (int k = 0; k < 8; k++) {
-        a[k] = pi[k * SK];
-        b[k] = pj[k * SK];
+        a[k] = pi[off + k * SK];
+        b[k] = pj[off + k * SK];
     }
-#pragma unroll 2
-    for (int tk = 0; tk < TK; tk++) {
-        const int tn = (tk + 1 < TK ? tk + 1 : tk) * TKS;   // the last FFT reloads itself (unused)
-        float2 na[8], nb[8];
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-            na[k] = pi[tn + k * SK];
-            nb[k] = pj[tn + k * SK];
-        }
-#pragma unroll
-        for (int jj = 0; jj < 8; jj++)
-#pragma unroll
-            for (int ii = 0; ii < 8; ii++) {
-                acc[ii][jj].x = fmaf(a[ii].x, b[jj].x, fmaf(a[ii].y, b[jj].y, acc[ii][jj].x));
-                acc[ii][jj].y = fmaf(a[ii].y, b[jj].x, fmaf(-a[ii].x, b[jj].y, acc[ii][jj].y));
-            }
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-            a[k] = na[k];
-            b[k] = nb[k];
-        }
+}
+
+// acc[ii][jj] += sum over the TK FFTs of a stage of xi[ii] * conj(xj[jj]) for one 8 x 8 tile of
+// signal pairs (kernel.c:829-854; the conjugation of kernel.c:557-568 folded in).  pi / pj point at
+// FFT 0 of the tile's first row / column signal in the stage; signals are SK elements apart, FFTs
+// TKS.  Two operand sets alternate: the operands of FFT tk + 1 are loaded while FFT tk's 256 FMAs
+// run (no register copies between them), so the shared-memory latency hides behind independent
+// arithmetic at two warps per scheduler.
+template <int TK, int SK, int TKS>
+__device__ __forceinline__ void tile_stage(float2 (&acc)[8][8], const float2* pi, const float2* pj)
+{
+    static_assert(TK % 2 == 0, "FFTs of a stage in pairs");
+    float2 a0[8], b0[8], a1[8], b1[8];
+    load8<SK>(a0, b0, pi, pj, 0);
+#pragma unroll 1
+    for (int tk = 0; tk < TK; tk += 2) {
+        load8<SK>(a1, b1, pi, pj, (tk + 1) * TKS);
+        tile_fma<TK, SK, TKS>(acc, a0, b0);
+        if (tk + 2 < TK) load8<SK>(a0, b0, pi, pj, (tk + 2) * TKS);
+        tile_fma<TK, SK, TKS>(acc, a1, b1);
     }
 }
 
 // The upper triangles (ii <= jj, index jj (jj + 1) / 2 + ii) of two diagonal 8 x 8 blocks, A at
-// pa and B at pb: 72 pairs, the work of one tile, with the same operand prefetch.
+// pa and B at pb: 72 pairs, the work of one tile, with the same alternating operand sets.
+__device__ __forceinline__ void diag_fma(float2 (&acc)[2][36], const float2 (&a)[8], const float2 (&b)[8])
+{
+#pragma unroll
+    for (int jj = 0; jj < 8; jj++)
+#pragma unroll
+        for (int ii = 0; ii <= jj; ii++) {
+            float2& u = acc[0][jj * (jj + 1) / 2 + ii];
+            float2& v = acc[1][jj * (jj + 1) / 2 + ii];
+            u.x = fmaf(a[ii].x, a[jj].x, fmaf(a[ii].y, a[jj].y, u.x));
+            u.y = fmaf(a[ii].y, a[jj].x, fmaf(-a[ii].x, a[jj].y, u.y));
+            v.x = fmaf(b[ii].x, b[jj].x, fmaf(b[ii].y, b[jj].y, v.x));
+            v.y = fmaf(b[ii].y, b[jj].x, fmaf(-b[ii].x, b[jj].y, v.y));
+        }
+}
+
 template <int TK, int SK, int TKS>
 __device__ __forceinline__ void diag_pair_stage(float2 (&acc)[2][36], const float2* pa, const float2* pb)
 {
-    float2 a[8], b[8];
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-        a[k] = pa[k * SK];
-        b[k] = pb[k * SK];
-    }
-#pragma unroll 2
-    for (int tk = 0; tk < TK; tk++) {
-        const int tn = (tk + 1 < TK ? tk + 1 : tk) * TKS;
-        float2 na[8], nb[8];
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-            na[k] = pa[tn + k * SK];
-            nb[k] = pb[tn + k * SK];
-        }
-#pragma unroll
-        for (int jj = 0; jj < 8; jj++)
-#pragma unroll
-            for (int ii = 0; ii <= jj; ii++) {
-                float2& u = acc[0][jj * (jj + 1) / 2 + ii];
-                float2& v = acc[1][jj * (jj + 1) / 2 + ii];
-                u.x = fmaf(a[ii].x, a[jj].x, fmaf(a[ii].y, a[jj].y, u.x));
-                u.y = fmaf(a[ii].y, a[jj].x, fmaf(-a[ii].x, a[jj].y, u.y));
-                v.x = fmaf(b[ii].x, b[jj].x, fmaf(b[ii].y, b[jj].y, v.x));
-                v.y = fmaf(b[ii].y, b[jj].x, fmaf(-b[ii].x, b[jj].y, v.y));
-            }
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-            a[k] = na[k];
-            b[k] = nb[k];
-        }
+    float2 a0[8], b0[8], a1[8], b1[8];
+    load8<SK>(a0, b0, pa, pb, 0);
+#pragma unroll 1
+    for (int tk = 0; tk < TK; tk += 2) {
+        load8<SK>(a1, b1, pa, pb, (tk + 1) * TKS);
+        diag_fma(acc, a0, b0);
+        if (tk + 2 < TK) load8<SK>(a0, b0, pa, pb, (tk + 2) * TKS);
+        diag_fma(acc, a1, b1);
     }
 }
 
