@@ -484,7 +484,15 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a)
         // tile 1 of i.  Item i + 1's step-1 pairs reuse the D1 slots that the twiddle warps release
         // while they write tile 1 of item i, so those warps find item i + 1's D1 ready instead of
         // waiting behind a whole step-2 tile.
-        const uint32_t sb1h = smem_u32(sm.b1[0]), sb1l = smem_u32(sm.b1[1]);
+        // Descriptors cost one add each in this thread: only their low words differ between
+        // operands (the high word holds stride, version and swizzle), every operand sits at a fixed
+        // offset from the shared-memory block, and a K step of 16 elements is 32 bytes further,
+        // i.e. +2 in the start-address field (shared addresses stay below 2^18, so the 14-bit field
+        // never carries).
+        const uint32_t dsm = (uint32_t)umma_desc(smem_u32(&sm));
+        auto dlo = [&](const void* p) -> uint32_t {
+            return dsm + (uint32_t)(((const char*)p - (const char*)&sm) >> 4);
+        };
         auto step1 = [&](int i) -> bool {
             for (int p = 0; p < NPAIR; p++) {
                 const int g = i * NPAIR + p;
@@ -496,13 +504,13 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a)
                 const uint32_t d1 = tmem + D1_COL + 64 * p, xa = tmem + A1_COL + 64 * s;
                 // x_hi . W_hi + x_lo . W_hi + x_hi . W_lo; K = 64 = 4 steps of 16 (8 columns,
                 // 32 bytes of a 128-byte swizzled row)
+                umma_ts_acc<false>(d1, xa, udesc(dlo(sm.b1[0])), kIdesc);
 #pragma unroll
-                for (int kk = 0; kk < 4; kk++)
-                    umma_ts(d1, xa + 8 * kk, umma_desc(sb1h + 32 * kk), kIdesc, kk > 0 ? 1u : 0u);
+                for (int kk = 1; kk < 4; kk++) umma_ts_acc<true>(d1, xa + 8 * kk, udesc(dlo(sm.b1[0]) + 2 * kk), kIdesc);
 #pragma unroll
-                for (int kk = 0; kk < 4; kk++) umma_ts(d1, xa + 32 + 8 * kk, umma_desc(sb1h + 32 * kk), kIdesc, 1u);
+                for (int kk = 0; kk < 4; kk++) umma_ts_acc<true>(d1, xa + 32 + 8 * kk, udesc(dlo(sm.b1[0]) + 2 * kk), kIdesc);
 #pragma unroll
-                for (int kk = 0; kk < 4; kk++) umma_ts(d1, xa + 8 * kk, umma_desc(sb1l + 32 * kk), kIdesc, 1u);
+                for (int kk = 0; kk < 4; kk++) umma_ts_acc<true>(d1, xa + 8 * kk, udesc(dlo(sm.b1[1]) + 2 * kk), kIdesc);
                 umma_commit(&sm.a1_empty[s]);
                 umma_commit(&sm.d1_full[p]);
             }
@@ -514,14 +522,18 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a)
             tc_fence_after();
             const uint32_t d2 = tmem + D2_COL + 64 * j;
             // Z_hi . W_hi + Z_lo . W_hi + Z_hi . W_lo; K = 128 = two 64-element halves
+            umma_ss_acc<false>(d2, udesc(dlo(sm.a2[j][0][0])), udesc(dlo(sm.b2[0][0])), kIdesc);
+#pragma unroll
+            for (int kk = 1; kk < 8; kk++)
+                umma_ss_acc<true>(d2, udesc(dlo(sm.a2[j][0][kk >> 2]) + 2 * (kk & 3)),
+                                  udesc(dlo(sm.b2[0][kk >> 2]) + 2 * (kk & 3)), kIdesc);
 #pragma unroll 1
-            for (int t = 0; t < 3; t++) {
-                const int la = t == 1 ? 1 : 0, lb = t == 2 ? 1 : 0;
+            for (int t = 1; t < 3; t++) {
+                const uint32_t da = dlo(sm.a2[j][t == 1 ? 1 : 0][0]), db = dlo(sm.b2[t == 2 ? 1 : 0][0]);
 #pragma unroll
                 for (int kk = 0; kk < 8; kk++)
-                    umma<false>(d2, umma_desc(smem_u32(sm.a2[j][la][kk >> 2]) + (kk & 3) * 32),
-                                umma_desc(smem_u32(sm.b2[lb][kk >> 2]) + (kk & 3) * 32), kIdesc,
-                                (t > 0 || kk > 0) ? 1u : 0u);
+                    umma_ss_acc<true>(d2, udesc(da + (kk >> 2) * (int)(sizeof(sm.a2[0][0][0]) >> 4) + 2 * (kk & 3)),
+                                      udesc(db + (kk >> 2) * (int)(sizeof(sm.b2[0][0]) >> 4) + 2 * (kk & 3)), kIdesc);
             }
             umma_commit(&sm.a2_empty[j]);
             umma_commit(&sm.d2_full[j]);

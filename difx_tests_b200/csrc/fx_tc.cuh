@@ -114,6 +114,9 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr)
     return d;
 }
 
+// A descriptor from its low word: the high word of umma_desc does not depend on the address
+__device__ __forceinline__ uint64_t udesc(uint32_t lo) { return (umma_desc(0) & 0xFFFFFFFF00000000ull) | lo; }
+
 // Instruction descriptor, kind::f16 (and kind::f8f6f4 with E4M3 = format 0): D F32, A/B
 // F16 (E4M3), both K-major, M x N.
 constexpr uint32_t idesc_f16(int m, int n)
@@ -208,6 +211,29 @@ __device__ __forceinline__ void umma_ts(uint32_t tmem_d, uint32_t tmem_a, uint64
         "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}"
         ::"r"(tmem_d), "r"(tmem_a), "l"(b), "r"(idesc), "r"(accumulate)
         : "memory");
+}
+
+// The same MMA forms with the accumulate flag fixed at compile time (no predicate set-up per MMA)
+template <bool ACC>
+__device__ __forceinline__ void umma_ts_acc(uint32_t tmem_d, uint32_t tmem_a, uint64_t b, uint32_t idesc)
+{
+    if constexpr (ACC)
+        asm volatile("tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, 1;"
+                     ::"r"(tmem_d), "r"(tmem_a), "l"(b), "r"(idesc) : "memory");
+    else
+        asm volatile("tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, 0;"
+                     ::"r"(tmem_d), "r"(tmem_a), "l"(b), "r"(idesc) : "memory");
+}
+
+template <bool ACC>
+__device__ __forceinline__ void umma_ss_acc(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc)
+{
+    if constexpr (ACC)
+        asm volatile("tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, 1;"
+                     ::"r"(tmem_d), "l"(a), "l"(b), "r"(idesc) : "memory");
+    else
+        asm volatile("tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, 0;"
+                     ::"r"(tmem_d), "l"(a), "l"(b), "r"(idesc) : "memory");
 }
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
