@@ -484,64 +484,74 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a)
         // tile 1 of i.  Item i + 1's step-1 pairs reuse the D1 slots that the twiddle warps release
         // while they write tile 1 of item i, so those warps find item i + 1's D1 ready instead of
         // waiting behind a whole step-2 tile.
-        // Descriptors cost one add each in this thread: only their low words differ between
-        // operands (the high word holds stride, version and swizzle), every operand sits at a fixed
-        // offset from the shared-memory block, and a K step of 16 elements is 32 bytes further,
-        // i.e. +2 in the start-address field (shared addresses stay below 2^18, so the 14-bit field
-        // never carries).
+        // The issuer's code is kept small (rolled loops, one copy of each step): this one thread
+        // shares its SM's instruction cache with four other roles' code, and an unrolled issue
+        // sequence measured slower than the rolled one.  Descriptors: only their low words differ
+        // (the high word holds stride, version and swizzle); every operand sits at a fixed offset
+        // from the shared-memory block, and a K step of 16 elements is 32 bytes further, i.e. +2
+        // in the start-address field (shared addresses stay below 2^18: the 14-bit field never
+        // carries).
         const uint32_t dsm = (uint32_t)umma_desc(smem_u32(&sm));
         auto dlo = [&](const void* p) -> uint32_t {
             return dsm + (uint32_t)(((const char*)p - (const char*)&sm) >> 4);
         };
-        auto step1 = [&](int i) -> bool {
-            for (int p = 0; p < NPAIR; p++) {
-                const int g = i * NPAIR + p;
-                const int s = g % NA1;
-                if (!mbar_wait(&sm.a1_full[s], (g / NA1) & 1, abort_flag) ||
-                    !mbar_wait(&sm.d1_empty[p], (i & 1) ^ 1, abort_flag))
-                    return false;
-                tc_fence_after();
-                const uint32_t d1 = tmem + D1_COL + 64 * p, xa = tmem + A1_COL + 64 * s;
-                // x_hi . W_hi + x_lo . W_hi + x_hi . W_lo; K = 64 = 4 steps of 16 (8 columns,
-                // 32 bytes of a 128-byte swizzled row)
-                umma_ts_acc<false>(d1, xa, udesc(dlo(sm.b1[0])), kIdesc);
-#pragma unroll
-                for (int kk = 1; kk < 4; kk++) umma_ts_acc<true>(d1, xa + 8 * kk, udesc(dlo(sm.b1[0]) + 2 * kk), kIdesc);
-#pragma unroll
-                for (int kk = 0; kk < 4; kk++) umma_ts_acc<true>(d1, xa + 32 + 8 * kk, udesc(dlo(sm.b1[0]) + 2 * kk), kIdesc);
-#pragma unroll
-                for (int kk = 0; kk < 4; kk++) umma_ts_acc<true>(d1, xa + 8 * kk, udesc(dlo(sm.b1[1]) + 2 * kk), kIdesc);
-                umma_commit(&sm.a1_empty[s]);
-                umma_commit(&sm.d1_full[p]);
-            }
-            return true;
-        };
-        auto step2 = [&](int i, int j) -> bool {
-            if (!mbar_wait(&sm.a2_full[j], i & 1, abort_flag) || !mbar_wait(&sm.d2_empty[j], (i & 1) ^ 1, abort_flag))
-                return false;
-            tc_fence_after();
-            const uint32_t d2 = tmem + D2_COL + 64 * j;
-            // Z_hi . W_hi + Z_lo . W_hi + Z_hi . W_lo; K = 128 = two 64-element halves
-            umma_ss_acc<false>(d2, udesc(dlo(sm.a2[j][0][0])), udesc(dlo(sm.b2[0][0])), kIdesc);
-#pragma unroll
-            for (int kk = 1; kk < 8; kk++)
-                umma_ss_acc<true>(d2, udesc(dlo(sm.a2[j][0][kk >> 2]) + 2 * (kk & 3)),
-                                  udesc(dlo(sm.b2[0][kk >> 2]) + 2 * (kk & 3)), kIdesc);
+        const uint32_t b1h = dlo(sm.b1[0]), b1l = dlo(sm.b1[1]);
+        const uint32_t b2d = dlo(sm.b2[0][0]), b2limb = dlo(sm.b2[1][0]) - b2d, b2half = dlo(sm.b2[0][1]) - b2d;
+        const uint32_t a2d = dlo(sm.a2[0][0][0]), a2tile = dlo(sm.a2[1][0][0]) - a2d,
+                       a2limb = dlo(sm.a2[0][1][0]) - a2d, a2half = dlo(sm.a2[0][0][1]) - a2d;
+        bool ok = true;
+        // events: 0 = step 1 of item 0; 3 i + 1 = step-2 tile 0 of item i; 3 i + 2 = step 1 of
+        // item i + 1 (none after the last item); 3 i + 3 = step-2 tile 1 of item i
 #pragma unroll 1
-            for (int t = 1; t < 3; t++) {
-                const uint32_t da = dlo(sm.a2[j][t == 1 ? 1 : 0][0]), db = dlo(sm.b2[t == 2 ? 1 : 0][0]);
-#pragma unroll
-                for (int kk = 0; kk < 8; kk++)
-                    umma_ss_acc<true>(d2, udesc(da + (kk >> 2) * (int)(sizeof(sm.a2[0][0][0]) >> 4) + 2 * (kk & 3)),
-                                      udesc(db + (kk >> 2) * (int)(sizeof(sm.b2[0][0]) >> 4) + 2 * (kk & 3)), kIdesc);
+        for (int e = 0; e <= 3 * nitem && ok && nitem > 0; e++) {
+            const int i = e == 0 ? 0 : (e - 1) / 3, r = e == 0 ? 1 : (e - 1) % 3;
+            if (r == 1) {
+                const int it = e == 0 ? 0 : i + 1;
+                if (it >= nitem) continue;
+#pragma unroll 1
+                for (int p = 0; p < NPAIR; p++) {
+                    const int g = it * NPAIR + p;
+                    const int st = g % NA1;
+                    if (!mbar_wait(&sm.a1_full[st], (g / NA1) & 1, abort_flag) ||
+                        !mbar_wait(&sm.d1_empty[p], (it & 1) ^ 1, abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t d1 = tmem + D1_COL + 64 * p, xa = tmem + A1_COL + 64 * st;
+                    // x_hi . W_hi + x_lo . W_hi + x_hi . W_lo; K = 64 = 4 steps of 16 (8 columns,
+                    // 32 bytes of a 128-byte swizzled row)
+#pragma unroll 1
+                    for (int q = 0; q < 12; q++) {
+                        const int kk = q & 3, part = q >> 2;
+                        umma_ts(d1, xa + 8 * kk + (part == 1 ? 32 : 0), udesc((part == 2 ? b1l : b1h) + 2 * kk),
+                                kIdesc, (uint32_t)q);
+                    }
+                    umma_commit(&sm.a1_empty[st]);
+                    umma_commit(&sm.d1_full[p]);
+                }
+            } else {
+                const int j = r >> 1;
+                if (!mbar_wait(&sm.a2_full[j], i & 1, abort_flag) ||
+                    !mbar_wait(&sm.d2_empty[j], (i & 1) ^ 1, abort_flag)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t d2 = tmem + D2_COL + 64 * j, aj = a2d + j * a2tile;
+                // Z_hi . W_hi + Z_lo . W_hi + Z_hi . W_lo; K = 128 = two 64-element halves
+#pragma unroll 1
+                for (int q = 0; q < 24; q++) {
+                    const int t = q >> 3, kk = q & 7;
+                    const uint32_t koff = 2 * (kk & 3);
+                    const uint32_t da = aj + (t == 1 ? a2limb : 0u) + (kk >> 2) * a2half + koff;
+                    const uint32_t db = b2d + (t == 2 ? b2limb : 0u) + (kk >> 2) * b2half + koff;
+                    umma<false>(d2, udesc(da), udesc(db), kIdesc, (uint32_t)q);
+                }
+                umma_commit(&sm.a2_empty[j]);
+                umma_commit(&sm.d2_full[j]);
             }
-            umma_commit(&sm.a2_empty[j]);
-            umma_commit(&sm.d2_full[j]);
-            return true;
-        };
-        bool ok = nitem == 0 || step1(0);
-        for (int i = 0; i < nitem && ok; i++)
-            ok = step2(i, 0) && (i + 1 >= nitem || step1(i + 1)) && step2(i, 1);
+        }
         if (!ok) {
             if (!*abort_flag) atomicCAS(a.err, 0, ERR_WAIT);
             *abort_flag = 1;
