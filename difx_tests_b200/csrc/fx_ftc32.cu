@@ -86,6 +86,16 @@ __device__ __forceinline__ uint2 split_pair(float re, float im)
     return make_uint2(h2u(hi), h2u(lo));
 }
 
+// The same pair with hi = v truncated to 11 significant bits (sign, exponent and the top 10
+// fraction bits kept): hi is exact in FP16 (to 2^-25 absolute below FP16's normal range), lo =
+// RN16(v - hi) with v - hi exact in FP32; together ~21 bits.  No FP16 -> FP32 conversions.
+__device__ __forceinline__ uint2 split_pair_t(float re, float im)
+{
+    const float hr = __uint_as_float(__float_as_uint(re) & 0xFFFFE000u);
+    const float hm = __uint_as_float(__float_as_uint(im) & 0xFFFFE000u);
+    return make_uint2(h2u(__floats2half2_rn(hr, hm)), h2u(__floats2half2_rn(re - hr, im - hm)));
+}
+
 // e^{i a} for |a| <= 0.25 by its Taylor series to the a^8 / a^9 terms (truncation < 1e-10)
 __device__ __forceinline__ float2 cis_small(float a)
 {
@@ -310,7 +320,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a)
                         const float2 y = make_float2(__uint_as_float(v[2 * kk]), __uint_as_float(v[2 * kk + 1]));
                         const float2 z = cmul(y, cur);
                         cur = cmul(cur, r);
-                        const uint2 zz = split_pair(z.x, z.y);
+                        const uint2 zz = split_pair_t(z.x, z.y);
                         *reinterpret_cast<uint32_t*>(hi + kk * 1024) = zz.x;
                         *reinterpret_cast<uint32_t*>(lo + kk * 1024) = zz.y;
                     }
@@ -478,90 +488,96 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a)
                     atomicCAS(a.err, 0, ERR_WAIT);
                     sm.drain_fail = 1;
                 }
-    } else if (lane == 0) {
+    } else if (warp == W_MMA) {
         // ================================================================ MMA issuer
         // Issue order: step 1 of item 0, then per item i: step-2 tile 0 of i, step 1 of i + 1, step-2
         // tile 1 of i.  Item i + 1's step-1 pairs reuse the D1 slots that the twiddle warps release
         // while they write tile 1 of item i, so those warps find item i + 1's D1 ready instead of
         // waiting behind a whole step-2 tile.
-        // The issuer's code is kept small (rolled loops, one copy of each step): this one thread
-        // shares its SM's instruction cache with four other roles' code, and an unrolled issue
-        // sequence measured slower than the rolled one.  Descriptors: only their low words differ
-        // (the high word holds stride, version and swizzle); every operand sits at a fixed offset
-        // from the shared-memory block, and a K step of 16 elements is 32 bytes further, i.e. +2
-        // in the start-address field (shared addresses stay below 2^18: the 14-bit field never
-        // carries).
+        // The whole warp runs the issue loop and one elected lane issues each group of MMAs and
+        // its commits: the descriptors are then warp-uniform values formed outside the divergent
+        // issue, and each MMA costs little more than its own instruction in this one thread (a
+        // single lane running the whole loop measured slower).  Descriptors: only their low words
+        // differ (the high word holds stride, version and swizzle); every operand sits at a fixed
+        // offset from the shared-memory block, and a K step of 16 elements is 32 bytes further,
+        // i.e. +2 in the start-address field (shared addresses stay below 2^18: the 14-bit field
+        // never carries).
         const uint32_t dsm = (uint32_t)umma_desc(smem_u32(&sm));
         auto dlo = [&](const void* p) -> uint32_t {
             return dsm + (uint32_t)(((const char*)p - (const char*)&sm) >> 4);
         };
-        const uint32_t b1h = dlo(sm.b1[0]), b1l = dlo(sm.b1[1]);
-        const uint32_t b2d = dlo(sm.b2[0][0]), b2limb = dlo(sm.b2[1][0]) - b2d, b2half = dlo(sm.b2[0][1]) - b2d;
-        const uint32_t a2d = dlo(sm.a2[0][0][0]), a2tile = dlo(sm.a2[1][0][0]) - a2d,
-                       a2limb = dlo(sm.a2[0][1][0]) - a2d, a2half = dlo(sm.a2[0][0][1]) - a2d;
-        bool ok = true;
-        // events: 0 = step 1 of item 0; 3 i + 1 = step-2 tile 0 of item i; 3 i + 2 = step 1 of
-        // item i + 1 (none after the last item); 3 i + 3 = step-2 tile 1 of item i
-#pragma unroll 1
-        for (int e = 0; e <= 3 * nitem && ok && nitem > 0; e++) {
-            const int i = e == 0 ? 0 : (e - 1) / 3, r = e == 0 ? 1 : (e - 1) % 3;
-            if (r == 1) {
-                const int it = e == 0 ? 0 : i + 1;
-                if (it >= nitem) continue;
-#pragma unroll 1
-                for (int p = 0; p < NPAIR; p++) {
-                    const int g = it * NPAIR + p;
-                    const int st = g % NA1;
-                    if (!mbar_wait(&sm.a1_full[st], (g / NA1) & 1, abort_flag) ||
-                        !mbar_wait(&sm.d1_empty[p], (it & 1) ^ 1, abort_flag)) {
-                        ok = false;
-                        break;
-                    }
-                    tc_fence_after();
-                    const uint32_t d1 = tmem + D1_COL + 64 * p, xa = tmem + A1_COL + 64 * st;
-                    // x_hi . W_hi + x_lo . W_hi + x_hi . W_lo; K = 64 = 4 steps of 16 (8 columns,
-                    // 32 bytes of a 128-byte swizzled row)
-#pragma unroll 1
-                    for (int q = 0; q < 12; q++) {
-                        const int kk = q & 3, part = q >> 2;
-                        umma_ts(d1, xa + 8 * kk + (part == 1 ? 32 : 0), udesc((part == 2 ? b1l : b1h) + 2 * kk),
-                                kIdesc, (uint32_t)q);
-                    }
-                    umma_commit(&sm.a1_empty[st]);
+        auto step1 = [&](int i) -> bool {
+            for (int p = 0; p < NPAIR; p++) {
+                const int g = i * NPAIR + p;
+                const int s = g % NA1;
+                if (!mbar_wait_warp(&sm.a1_full[s], (g / NA1) & 1, abort_flag) ||
+                    !mbar_wait_warp(&sm.d1_empty[p], (i & 1) ^ 1, abort_flag))
+                    return false;
+                tc_fence_after();
+                const uint32_t d1 = tmem + D1_COL + 64 * p, xa = tmem + A1_COL + 64 * s;
+                const uint32_t bh = dlo(sm.b1[0]), bl = dlo(sm.b1[1]);
+                // x_hi . W_hi + x_lo . W_hi + x_hi . W_lo; K = 64 = 4 steps of 16 (8 columns,
+                // 32 bytes of a 128-byte swizzled row)
+                if (elect_one()) {
+                    umma_ts_acc<false>(d1, xa, udesc(bh), kIdesc);
+#pragma unroll
+                    for (int kk = 1; kk < 4; kk++) umma_ts_acc<true>(d1, xa + 8 * kk, udesc(bh + 2 * kk), kIdesc);
+#pragma unroll
+                    for (int kk = 0; kk < 4; kk++) umma_ts_acc<true>(d1, xa + 32 + 8 * kk, udesc(bh + 2 * kk), kIdesc);
+#pragma unroll
+                    for (int kk = 0; kk < 4; kk++) umma_ts_acc<true>(d1, xa + 8 * kk, udesc(bl + 2 * kk), kIdesc);
+                    umma_commit(&sm.a1_empty[s]);
                     umma_commit(&sm.d1_full[p]);
                 }
-            } else {
-                const int j = r >> 1;
-                if (!mbar_wait(&sm.a2_full[j], i & 1, abort_flag) ||
-                    !mbar_wait(&sm.d2_empty[j], (i & 1) ^ 1, abort_flag)) {
-                    ok = false;
-                    break;
-                }
-                tc_fence_after();
-                const uint32_t d2 = tmem + D2_COL + 64 * j, aj = a2d + j * a2tile;
-                // Z_hi . W_hi + Z_lo . W_hi + Z_hi . W_lo; K = 128 = two 64-element halves
-#pragma unroll 1
-                for (int q = 0; q < 24; q++) {
-                    const int t = q >> 3, kk = q & 7;
-                    const uint32_t koff = 2 * (kk & 3);
-                    const uint32_t da = aj + (t == 1 ? a2limb : 0u) + (kk >> 2) * a2half + koff;
-                    const uint32_t db = b2d + (t == 2 ? b2limb : 0u) + (kk >> 2) * b2half + koff;
-                    umma<false>(d2, udesc(da), udesc(db), kIdesc, (uint32_t)q);
-                }
-                umma_commit(&sm.a2_empty[j]);
-                umma_commit(&sm.d2_full[j]);
+                __syncwarp();
             }
-        }
-        if (!ok) {
+            return true;
+        };
+        auto step2 = [&](int i, int j) -> bool {
+            if (!mbar_wait_warp(&sm.a2_full[j], i & 1, abort_flag) ||
+                !mbar_wait_warp(&sm.d2_empty[j], (i & 1) ^ 1, abort_flag))
+                return false;
+            tc_fence_after();
+            const uint32_t d2 = tmem + D2_COL + 64 * j;
+            const uint32_t ah = dlo(sm.a2[j][0][0]), al = dlo(sm.a2[j][1][0]);
+            const uint32_t bh = dlo(sm.b2[0][0]), bl = dlo(sm.b2[1][0]);
+            constexpr uint32_t AH = sizeof(sm.a2[0][0][0]) >> 4, BH = sizeof(sm.b2[0][0]) >> 4;   // K halves
+            // Z_hi . W_hi + Z_lo . W_hi + Z_hi . W_lo; K = 128 = two 64-element halves
+#pragma unroll 1
+            for (int t = 0; t < 3; t++) {
+                const uint32_t a0 = t == 1 ? al : ah, b0 = t == 2 ? bl : bh;
+                if (elect_one()) {
+                    umma<false>(d2, udesc(a0), udesc(b0), kIdesc, t > 0 ? 1u : 0u);
+#pragma unroll
+                    for (int kk = 1; kk < 8; kk++)
+                        umma_ss_acc<true>(d2, udesc(a0 + (kk >> 2) * AH + 2 * (kk & 3)),
+                                          udesc(b0 + (kk >> 2) * BH + 2 * (kk & 3)), kIdesc);
+                    if (t == 2) {
+                        umma_commit(&sm.a2_empty[j]);
+                        umma_commit(&sm.d2_full[j]);
+                    }
+                }
+                __syncwarp();
+            }
+            return true;
+        };
+        bool ok = nitem == 0 || step1(0);
+        for (int i = 0; i < nitem && ok; i++)
+            ok = step2(i, 0) && (i + 1 >= nitem || step1(i + 1)) && step2(i, 1);
+        if (!ok && lane == 0) {
             if (!*abort_flag) atomicCAS(a.err, 0, ERR_WAIT);
             *abort_flag = 1;
         }
-        // every MMA issued must have retired before TMEM is freed
-        umma_commit(&sm.drain);
-        if (!mbar_drain(&sm.drain, 0)) {
-            atomicCAS(a.err, 0, ERR_WAIT);
-            sm.drain_fail = 1;
+        // every MMA issued must have retired before TMEM is freed (the commit comes from the lane
+        // that issued them: elect.sync elects the same lowest active lane every time)
+        if (elect_one()) {
+            umma_commit(&sm.drain);
+            if (!mbar_drain(&sm.drain, 0)) {
+                atomicCAS(a.err, 0, ERR_WAIT);
+                sm.drain_fail = 1;
+            }
         }
+        __syncwarp();
     }
 
     __syncthreads();

@@ -213,6 +213,14 @@ __device__ __forceinline__ void umma_ts(uint32_t tmem_d, uint32_t tmem_a, uint64
         : "memory");
 }
 
+// One lane of a converged warp (the lowest active lane), for single-thread issue of tcgen05 work
+__device__ __forceinline__ bool elect_one()
+{
+    uint32_t e;
+    asm volatile("{\n\t.reg .pred P;\n\telect.sync _|P, 0xffffffff;\n\tselp.u32 %0, 1, 0, P;\n\t}" : "=r"(e));
+    return e != 0;
+}
+
 // The same MMA forms with the accumulate flag fixed at compile time (no predicate set-up per MMA)
 template <bool ACC>
 __device__ __forceinline__ void umma_ts_acc(uint32_t tmem_d, uint32_t tmem_a, uint64_t b, uint32_t idesc)

@@ -76,7 +76,8 @@ def test_factorisation_is_the_dft_and_fp16_error_budget():
 
 # ---------------------------------------------------------------------------------------------
 # FP32-grade tensor-core F stage (error-compensated FP16 split).  Every FP16 operand is a pair
-# hi + lo (hi = FP16 rounding, lo = FP16 rounding of the remainder) and each GEMM is the three
+# hi + lo (hi = FP16 rounding, or for the twiddled intermediate the value truncated to 11
+# significant bits, lo = FP16 rounding of the remainder) and each GEMM is the three
 # products hi.hi + lo.hi + hi.lo accumulated in FP32 (the lo.lo term is below FP32 rounding).
 # The fringe rotator is split as the reference builds it (kernel.c:428-497): the step factor of
 # n1 goes into the step-1 operand through a per-(FFT, n1) table of the four levels times step[n1]
@@ -91,6 +92,14 @@ def split16(v):
     hi = v.astype(np.float16)
     lo = (v - hi.astype(np.float32)).astype(np.float16)
     return hi.astype(np.float64), lo.astype(np.float64)
+
+
+def split16t(v):
+    """The twiddle stage's pair: hi = v truncated to 11 significant bits (exact in FP16),
+    lo = RN16(v - hi)."""
+    v = np.asarray(v, np.float32)
+    hi = (v.view(np.uint32) & np.uint32(0xFFFFE000)).view(np.float32)
+    return hi.astype(np.float16).astype(np.float64), (v - hi).astype(np.float16).astype(np.float64)
 
 
 def gemm3(a, b):
@@ -127,7 +136,7 @@ def ftc32_spectrum(codes, levels, sub, step, theta):
     z = cmul32(y, t)                                                                 # [n2][k1]
     zr = interleave(z.T.astype(np.complex128)).astype(np.float32)                   # rows k1, K (n2, c)
     b2 = real_form(np.exp(-2j * np.pi * np.outer(k2, n2) / F2)).astype(np.float32)  # [(k2,c)][(n2,c')]
-    xk = deinterleave(gemm3(split16(zr), split16(b2))).astype(np.complex64)         # D2[k1][k2]
+    xk = deinterleave(gemm3(split16t(zr), split16(b2))).astype(np.complex64)        # D2[k1][k2]
     fst = np.exp(1j * theta * F1 * k2).astype(np.complex64)
     out = cmul32(xk, fst[None, :])                                                   # fstep[k2]
     return out.T.reshape(-1)                                                         # channel k1 + 32 k2
