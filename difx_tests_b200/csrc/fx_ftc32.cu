@@ -33,6 +33,8 @@
 //                and the window offsets
 // Every wait is bounded (1 s): on expiry the CTA records code 7 in the error word, stops,
 // drains what it issued and frees TMEM (or keeps it allocated if the drain itself expires).
+#include <cstring>
+
 #include "fx_ftc_common.cuh"
 
 namespace fx {
@@ -67,6 +69,7 @@ struct Smem {
     int2 pwin[NIB][2];                              // [pair % NIB][FFT] (bit of sample 0 in inb, valid)
     DelayEntry oent[2][TB];                         // output: delay entries [item parity][FFT]
     float2 fstep[K2H][TB];                          // output: [k2][b] (a warp's 8 FFTs: one 64-byte row)
+    alignas(128) __half otile[2][16 * 16 * 2 * TB]; // output: FP16 boxes [k2 % 16][k1 % 16][re|im][b] of the tensor store
     float ctab[P::FS + P::FST];                     // chan_sub | chan_step
     uint64_t a1_full[NA1], a1_empty[NA1], d1_full[NPAIR], d1_empty[NPAIR];
     uint64_t a2_full[2], a2_empty[2], d2_full[2], d2_empty[2], drain;
@@ -113,7 +116,7 @@ __device__ __forceinline__ float2 cis_half_turns_acc(float x)
 }
 
 template <bool OUT16, bool AMAX>
-__global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a)
+__global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a, const __grid_constant__ CUtensorMap omap)
 {
     using namespace tc;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -346,6 +349,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a)
         if (to < TB && nitem > 0) sm.oent[0][to] = item_entry<TB>(a, 0, ntb, to);
         if (to < TB && nitem > 1) dnext = item_entry<TB>(a, 1, ntb, to);
         bool ok = true;
+        int nbox = 0;   // tensor stores issued (FP16 output): buffer nbox & 1 is the next to fill
+        // Every barrier below is reached by all four output warps in the same order: a failed
+        // wait is agreed on through bar_or before any warp leaves the loops.
         for (int i = 0; i < nitem; i++) {
             const Item it = item_of<TB>(blockIdx.x + i * gridDim.x, a.nant, ntb);
             // item i's entries visible; every thread is done with item i - 1's table
@@ -364,7 +370,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a)
             }
 #pragma unroll 1
             for (int j = 0; j < 2; j++) {
-                if (!mbar_wait_warp(&sm.d2_full[j], i & 1, abort_flag)) {
+                const bool got = mbar_wait_warp(&sm.d2_full[j], i & 1, abort_flag);
+                if (bar_or(3, 128, !got)) {
                     ok = false;
                     break;
                 }
@@ -381,19 +388,18 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a)
                     mbar_arrive(&sm.d2_empty[j]);
                 }
                 if constexpr (OUT16) {
-                    const size_t chan_stride = (size_t)a.rows * a.T;
-                    const size_t kstep = (size_t)F1 * chan_stride;
-                    __half* pk = reinterpret_cast<__half*>(a.spec) + ((size_t)it.sb * C + k1) * chan_stride +
-                                 (size_t)(2 * it.ant) * a.T + it.tb0 + b + (size_t)(16 * hf) * kstep;
+                    // the half tile (16 k1 x 16 k2 channels x re|im x 8 FFTs) goes out as one tensor
+                    // store from a double-buffered shared box; the store that last read this
+                    // buffer was waited for before the previous barrier
+                    __half* ot = sm.otile[nbox & 1] + kl * (2 * TB) + b;
 #pragma unroll
                     for (int kk = 0; kk < 16; kk++) {
                         const int k2 = 16 * hf + kk;
                         const float2 y = cmul(make_float2(__uint_as_float(v[2 * kk]), __uint_as_float(v[2 * kk + 1])),
                                               sm.fstep[k2][b]);
                         const __half2 hv = __floats2half2_rn(y.x, y.y);
-                        pk[0] = __low2half(hv);
-                        pk[a.T] = __high2half(hv);
-                        pk += kstep;
+                        ot[kk * (16 * 2 * TB)] = __low2half(hv);
+                        ot[kk * (16 * 2 * TB) + TB] = __high2half(hv);
                         if constexpr (AMAX) {
                             // max(|Re|, |Im|) of the stored values over the item's 8 FFTs: the 8 lanes
                             // b = 0..7 of a channel are consecutive (lane = 8 (kl % 4) + b)
@@ -405,6 +411,15 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a)
                             if (b == 0 && m) atomicMax(a.amax + ((size_t)it.sb * C + k1 + F1 * k2) * nsig + it.ant, m);
                         }
                     }
+                    fence_async_smem();   // these writes, visible to the tensor store
+                    if (to == 0) bulk_wait_read_all();   // the previous store has read the other buffer
+                    named_bar(3, 128);
+                    if (to == 0) {
+                        // box origin: FFT tb0, row 2 ant, k1 = 16 j, k2 = 16 hf of subband sb
+                        tma_store_4d(&omap, sm.otile[nbox & 1], it.tb0, 2 * it.ant, 16 * j, K2H * it.sb + 16 * hf);
+                        bulk_commit();
+                    }
+                    nbox++;
                 } else {
                     float2* pk = reinterpret_cast<float2*>(a.spec) +
                                  (((size_t)it.sb * nsig + it.ant) * a.T + it.tb0 + b) * C + k1;
@@ -418,6 +433,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a)
                 }
             }
             if (!ok) break;
+        }
+        if constexpr (OUT16) {
+            if (to == 0) bulk_wait_all();   // the stores are complete before the CTA exits
         }
         if (!ok) {
             if (!*abort_flag) atomicCAS(a.err, 0, ERR_WAIT);
@@ -611,18 +629,37 @@ cudaError_t launch_ftc32(int mode, const FArgs& a, cudaStream_t st)
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
     const int grid = (int)(ntask < nsm ? ntask : nsm);
+    CUtensorMap omap;
+    std::memset(&omap, 0, sizeof(omap));
+    if (mode == kSpecF16) {
+        // FP16 K-major spectra [sb][k2][k1][row][T] (channel k1 + 32 k2) as a 4-D tensor
+        // (T, row, k1, 32 sb + k2); boxes of 8 FFTs x 2 rows x 16 k1 x 16 k2.  T % 8 == 0 keeps
+        // every stride a multiple of 16 bytes, and box origins at FFT tb0 (a multiple of 8) keep
+        // the innermost coordinate 16-byte aligned.
+        auto enc = tc::tensor_map_encoder();
+        if (!enc) return cudaErrorNotSupported;
+        const cuuint64_t row_b = (cuuint64_t)a.T * 2;
+        const cuuint64_t dims[4] = {(cuuint64_t)a.T, (cuuint64_t)a.rows, (cuuint64_t)F1, (cuuint64_t)K2H * a.nsb};
+        const cuuint64_t strides[3] = {row_b, row_b * a.rows, row_b * a.rows * F1};
+        const cuuint32_t box[4] = {(cuuint32_t)TB, 2, 16, 16};
+        const cuuint32_t estr[4] = {1, 1, 1, 1};
+        if (enc(&omap, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 4, a.spec, dims, strides, box, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return cudaErrorInvalidValue;
+    }
     if (mode == kSpecF16 && a.amax) {
         static unsigned configured = 0;
         if ((e = set_smem_once(k_ftc32<true, true>, sm, &configured)) != cudaSuccess) return e;
-        k_ftc32<true, true><<<grid, NTHREADS, sm, st>>>(a);
+        k_ftc32<true, true><<<grid, NTHREADS, sm, st>>>(a, omap);
     } else if (mode == kSpecF16) {
         static unsigned configured = 0;
         if ((e = set_smem_once(k_ftc32<true, false>, sm, &configured)) != cudaSuccess) return e;
-        k_ftc32<true, false><<<grid, NTHREADS, sm, st>>>(a);
+        k_ftc32<true, false><<<grid, NTHREADS, sm, st>>>(a, omap);
     } else {
         static unsigned configured = 0;
         if ((e = set_smem_once(k_ftc32<false, false>, sm, &configured)) != cudaSuccess) return e;
-        k_ftc32<false, false><<<grid, NTHREADS, sm, st>>>(a);
+        k_ftc32<false, false><<<grid, NTHREADS, sm, st>>>(a, omap);
     }
     return cudaGetLastError();
 }

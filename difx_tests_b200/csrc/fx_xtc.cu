@@ -294,19 +294,6 @@ k_xtc(const __grid_constant__ CUtensorMap tmap, XArgs a, int* err)
     }
 }
 
-static PFN_cuTensorMapEncodeTiled_v12000 get_encode()
-{
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    if (!fn) {
-        cudaDriverEntryPointQueryResult q;
-        void* p = nullptr;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    }
-    return fn;
-}
-
 template <bool MB>
 static size_t xtc_smem_t()
 {
@@ -338,7 +325,7 @@ static cudaError_t launch_xtc_f(const XArgs& a, int* d_err, int nsm, cudaStream_
         return cudaErrorInvalidValue;
     if ((long long)a.nsb * a.nchan * a.rows > 0x7fffffffLL) return cudaErrorInvalidValue;   // int TMA row coordinate
     if (F8 && !a.inv_scale) return cudaErrorInvalidValue;
-    auto enc = get_encode();
+    auto enc = tc::tensor_map_encoder();
     if (!enc) return cudaErrorNotSupported;
     CUtensorMap map;
     const cuuint64_t dims[2] = {(cuuint64_t)a.T, (cuuint64_t)a.nsb * a.nchan * a.rows};
