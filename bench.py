@@ -9,10 +9,14 @@ delay table, fused unpack/shift/fringe/FFT/fractional-sample F stage, X stage.
 
   python bench.py [--gpus N --steps K --warmup W] [--xmode all|both|tc|tc16f|fp8|plain] [--impl reference]
 
-The headline `value` is the tensor-core form: FP32 F stage (FFT on the CUDA cores), its
-spectra cast to FP16 for the tcgen05 X stage with FP32 accumulation.  The same X form on the
-FP16 tensor-core F stage ("tc16f"), the FP8-E4M3 tensor-core form and the FP32 plain form run
-on the same input in the same invocation and are reported under their names.
+The headline `value` is the tensor-core form at FP32 F-stage accuracy: the FP32-grade
+tensor-core F stage (k_ftc32: every operand an FP16 hi + lo pair, three products per GEMM,
+FP32 accumulation; spectra held to the FP32 FFT's error bar), its spectra cast to FP16 for
+the tcgen05 X stage with FP32 accumulation.  The same X form on the FP32 FFT F stage on the
+CUDA cores ("tc"), on the FP16 tensor-core F stage ("tc16f"), the FP8-E4M3 tensor-core form
+and the FP32 plain form run on the same input in the same invocation and are reported under
+their names.  Geometries the tensor-core F stages do not cover (other than 1024 channels x
+one polarisation) take "tc" as the headline.
 
 Under torchrun (N > 1) every rank correlates its own subintegration (weak
 scaling, no data-path collective) and rank 0 prints one JSON line; time is the
@@ -355,9 +359,9 @@ FSTAGE_DRAM_BYTES_PER_SAMPLE = {(1, True): 2.17, (1, False): 4.16, (2, True): 2.
 
 # form -> (fxc_config.xmode, fxc_config.fstage)
 FORMS = {"plain": (0, 1),     # FXC_X_PLAIN_FP32, FXC_F_FFT32
-         "tc": (1, 1),        # FXC_X_TC_FP16 on the FP32 FFT F stage (the headline form)
+         "tc": (1, 1),        # FXC_X_TC_FP16 on the FP32 FFT F stage
          "tc16f": (1, 2),     # FXC_X_TC_FP16 on the FP16 tensor-core F stage (FXC_F_TC16)
-         "tc32f": (1, 3),     # FXC_X_TC_FP16 on the FP32-grade tensor-core F stage (FXC_F_TC32)
+         "tc32f": (1, 3),     # FXC_X_TC_FP16 on the FP32-grade tensor-core F stage (FXC_F_TC32), the headline
          "fp8": (2, 1)}       # FXC_X_TC_FP8 on the FP32 FFT F stage
 XMODES = {k: v[0] for k, v in FORMS.items()}
 DTYPES = {"plain": "f32 (FFT F stage and X stage on the CUDA cores)",
@@ -456,7 +460,7 @@ def run_gpu_arm(args):
                            device=dev)
     torch.cuda.synchronize()
 
-    forms = {"all": ["tc", "tc32f", "tc16f", "fp8", "plain"], "both": ["tc", "plain"]}.get(args.xmode, [args.xmode])
+    forms = {"all": ["tc32f", "tc", "tc16f", "fp8", "plain"], "both": ["tc32f", "plain"]}.get(args.xmode, [args.xmode])
     if w["nchan"] != 1024 or w["npol"] != 1:   # the tensor-core F stages cover 1024 ch x 1 pol only
         forms = [f for f in forms if f not in ("tc16f", "tc32f")]
     res, failed = {}, {}
@@ -609,7 +613,8 @@ def run_shard_arm(args):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
     w = WORKLOADS[args.workload]
-    xmode, fstage = FORMS[args.xmode if args.xmode in FORMS else "tc"]
+    sform = args.xmode if args.xmode in FORMS else ("tc32f" if w["nchan"] == 1024 and w["npol"] == 1 else "tc")
+    xmode, fstage = FORMS[sform]
     cfg = fx.make_config(w["nant"], w["nchan"], w["numffts"], w["bw"], w["lo"], npol=w["npol"], nsubband=w["nsb"],
                          xmode=xmode, fstage=fstage)
     subint = fx.lib().fxc_subint_bytes(cfg)
@@ -649,7 +654,7 @@ def run_shard_arm(args):
         print(json.dumps({
             "metric": METRIC, "value": samples / (ms / 1e3) / 1e9, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-            "scaling": "strong", "vs_baseline": None, "dtype": DTYPES[args.xmode if args.xmode in FORMS else "tc"],
+            "scaling": "strong", "vs_baseline": None, "dtype": DTYPES[sform],
             "data": "synthetic (seeded, generated on device)",
             "config": {"workload": w["desc"], "parallelism": f"{args.shard} shards x{world}",
                        "merge": "all-reduce of visibilities and counts" if args.shard == "time" else "all-gather",
@@ -913,9 +918,10 @@ def main():
                     help="cfg3: the batched uneven workload (12 jobs through fxc_batch_*); cfg4: the large "
                          "array (512 signals x 4096 channels x 16 subbands) streamed through device windows")
     ap.add_argument("--xmode", default="all", choices=["all", "both"] + sorted(FORMS),
-                    help="all: the FP16 tensor-core X form on the FP32 FFT F stage is the headline value; the same "
-                         "X form on the FP16 tensor-core F stage (tc16f), the FP8 form and the FP32 plain form are "
-                         "timed beside it; both: the headline and plain")
+                    help="all: the FP16 tensor-core X form on the FP32-grade tensor-core F stage (tc32f) is the "
+                         "headline value; the same X form on the FP32 FFT F stage (tc) and on the FP16 tensor-core "
+                         "F stage (tc16f), the FP8 form and the FP32 plain form are timed beside it; both: the "
+                         "headline and plain")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
