@@ -351,7 +351,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a, const __grid_con
         bool ok = true;
         int nbox = 0;   // tensor stores issued (FP16 output): buffer nbox & 1 is the next to fill
         // Every barrier below is reached by all four output warps in the same order: a failed
-        // wait is agreed on through bar_or before any warp leaves the loops.
+        // wait is agreed on through bar_or at the top of an item before any warp leaves the loop.
         for (int i = 0; i < nitem; i++) {
             const Item it = item_of<TB>(blockIdx.x + i * gridDim.x, a.nant, ntb);
             // item i's entries visible; every thread is done with item i - 1's table
@@ -370,11 +370,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a, const __grid_con
             }
 #pragma unroll 1
             for (int j = 0; j < 2; j++) {
-                const bool got = mbar_wait_warp(&sm.d2_full[j], i & 1, abort_flag);
-                if (bar_or(3, 128, !got)) {
-                    ok = false;
-                    break;
-                }
+                // on an expired wait the warp still takes every barrier of the item (its data are
+                // void, the error is recorded) and all output warps stop together at the next item
+                if (!mbar_wait_warp(&sm.d2_full[j], i & 1, abort_flag)) ok = false;
                 tc_fence_after();
                 const int k1 = 16 * j + kl;
                 // two halves of 16 channels k2 (32 columns each), to keep the registers low
@@ -391,15 +389,20 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a, const __grid_con
                     // the half tile (16 k1 x 16 k2 channels x re|im x 8 FFTs) goes out as one tensor
                     // store from a double-buffered shared box; the store that last read this
                     // buffer was waited for before the previous barrier
-                    __half* ot = sm.otile[nbox & 1] + kl * (2 * TB) + b;
+                    // lanes b and b ^ 1 swap their (re, im) pair: the even lane stores (re_b, re_b+1)
+                    // in the re row, the odd lane (im_b-1, im_b) in the im row, one whole word each
+                    uint32_t* ot = reinterpret_cast<uint32_t*>(sm.otile[nbox & 1]) + kl * TB + (b & 1) * (TB / 2) +
+                                   (b >> 1);
+                    const uint32_t sel = (b & 1) ? 0x3276u : 0x5410u;
 #pragma unroll
                     for (int kk = 0; kk < 16; kk++) {
                         const int k2 = 16 * hf + kk;
                         const float2 y = cmul(make_float2(__uint_as_float(v[2 * kk]), __uint_as_float(v[2 * kk + 1])),
                                               sm.fstep[k2][b]);
                         const __half2 hv = __floats2half2_rn(y.x, y.y);
-                        ot[kk * (16 * 2 * TB)] = __low2half(hv);
-                        ot[kk * (16 * 2 * TB) + TB] = __high2half(hv);
+                        const uint32_t mine = h2u(hv);
+                        const uint32_t other = __shfl_xor_sync(0xffffffffu, mine, 1);
+                        ot[kk * (16 * TB)] = __byte_perm(mine, other, sel);
                         if constexpr (AMAX) {
                             // max(|Re|, |Im|) of the stored values over the item's 8 FFTs: the 8 lanes
                             // b = 0..7 of a channel are consecutive (lane = 8 (kl % 4) + b)
@@ -432,7 +435,6 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a, const __grid_con
                 }
                 }
             }
-            if (!ok) break;
         }
         if constexpr (OUT16) {
             if (to == 0) bulk_wait_all();   // the stores are complete before the CTA exits
