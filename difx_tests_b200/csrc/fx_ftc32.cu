@@ -67,13 +67,14 @@ struct Smem {
     alignas(16) uint8_t inb[NIB][2][INB];           // [pair % NIB][FFT of the pair] input bytes
     alignas(16) uint2 lut[NIB][2][F1][4];           // [pair % NIB][FFT][n1][code] (hi, lo) of level * step[n1]
     int2 pwin[NIB][2];                              // [pair % NIB][FFT] (bit of sample 0 in inb, valid)
-    DelayEntry oent[2][TB];                         // output: delay entries [item parity][FFT]
-    float2 fstep[K2H][TB];                          // output: [k2][b] (a warp's 8 FFTs: one 64-byte row)
+    float2 fstep[2][K2H][TB];                       // [item parity][k2][b] fstep of the item's FFTs (a warp's
+                                                    // 8 FFTs: one 64-byte row), written by the twiddle warps
     alignas(128) __half otile[2][16 * 16 * 2 * TB]; // output: FP16 boxes [k2 % 16][k1 % 16][re|im][b] of the tensor store
     float ctab[P::FS + P::FST];                     // chan_sub | chan_step
     uint64_t a1_full[NA1], a1_empty[NA1], d1_full[NPAIR], d1_empty[NPAIR];
     uint64_t a2_full[2], a2_empty[2], d2_full[2], d2_empty[2], drain;
     uint64_t cp_full[NIB], tab_full[NIB], tab_empty[NIB];
+    uint64_t fs_full[2], fs_empty[2];
     uint32_t tmem_base;
     int abort;
     int drain_fail;                                 // a drain wait expired: copies or MMAs may be in flight
@@ -147,6 +148,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a, const __grid_con
             mbar_init(&sm.d2_empty[j], 128);
         }
         mbar_init(&sm.drain, 1);
+        for (int s = 0; s < 2; s++) {
+            mbar_init(&sm.fs_full[s], 256);
+            mbar_init(&sm.fs_empty[s], 128);
+        }
         for (int s = 0; s < NIB; s++) {
             mbar_init(&sm.cp_full[s], 1);
             mbar_init(&sm.tab_full[s], 1);
@@ -285,6 +290,20 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a, const __grid_con
                     }
                 }
             }
+            // fstep[k2] (kernel.c:512-523, the step part of the fractional-sample rotator) of FFT
+            // 2 h + bsel + 4 (t % 2) of the item, k2 = lane: warp t covers FFT t's row of the table
+            {
+                const int u = t & 1;
+                if (!mbar_wait_warp(&sm.fs_empty[i & 1], ((i >> 1) & 1) ^ 1, abort_flag)) {
+                    ok = false;
+                    break;
+                }
+                const DelayEntry d = u ? dn[1] : dn[0];
+                float sn = 0.f, cs = 0.f;
+                if (d.valid) sincosf(__fmul_rn(sm.ctab[P::FS + lane], __double2float_rn(d.frac)), &sn, &cs);
+                sm.fstep[i & 1][lane][2 * (h + 2 * u) + bsel] = make_float2(cs, sn);
+                mbar_arrive(&sm.fs_full[i & 1]);
+            }
             if (i + 1 < nitem) {
                 for (int u = 0; u < 2; u++) dn[u] = item_entry<TB>(a, i + 1, ntb, 2 * (h + 2 * u) + bsel);
                 lon = a.sb_lo[item_of<TB>(blockIdx.x + (i + 1) * gridDim.x, a.nant, ntb).sb];
@@ -345,29 +364,16 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a, const __grid_con
         const uint32_t lane_off = (uint32_t)(32 * q) << 16;
         const int to = threadIdx.x - 32 * W_OUT;
         const int nsig = a.nant;
-        DelayEntry dnext;
-        if (to < TB && nitem > 0) sm.oent[0][to] = item_entry<TB>(a, 0, ntb, to);
-        if (to < TB && nitem > 1) dnext = item_entry<TB>(a, 1, ntb, to);
         bool ok = true;
         int nbox = 0;   // tensor stores issued (FP16 output): buffer nbox & 1 is the next to fill
         // Every barrier below is reached by all four output warps in the same order: a failed
         // wait is agreed on through bar_or at the top of an item before any warp leaves the loop.
         for (int i = 0; i < nitem; i++) {
             const Item it = item_of<TB>(blockIdx.x + i * gridDim.x, a.nant, ntb);
-            // item i's entries visible; every thread is done with item i - 1's table
             if (bar_or(2, 128, !ok || *abort_flag)) break;
-            for (int e = to; e < TB * K2H; e += 128) {
-                const int bb = e / K2H, k2 = e % K2H;
-                const DelayEntry& d = sm.oent[i & 1][bb];
-                float sn = 0.f, cs = 0.f;
-                if (d.valid) sincosf(__fmul_rn(sm.ctab[P::FS + k2], __double2float_rn(d.frac)), &sn, &cs);
-                sm.fstep[k2][bb] = make_float2(cs, sn);   // kernel.c:512-523 (step part)
-            }
-            if (bar_or(2, 128, !ok || *abort_flag)) break;
-            if (i + 1 < nitem) {
-                if (to < TB) sm.oent[(i + 1) & 1][to] = dnext;
-                if (to < TB && i + 2 < nitem) dnext = item_entry<TB>(a, i + 2, ntb, to);
-            }
+            // the item's fstep table (twiddle warps)
+            if (!mbar_wait_warp(&sm.fs_full[i & 1], (i >> 1) & 1, abort_flag)) ok = false;
+            const float2 (*fst)[TB] = sm.fstep[i & 1];
 #pragma unroll 1
             for (int j = 0; j < 2; j++) {
                 // on an expired wait the warp still takes every barrier of the item (its data are
@@ -389,20 +395,15 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a, const __grid_con
                     // the half tile (16 k1 x 16 k2 channels x re|im x 8 FFTs) goes out as one tensor
                     // store from a double-buffered shared box; the store that last read this
                     // buffer was waited for before the previous barrier
-                    // lanes b and b ^ 1 swap their (re, im) pair: the even lane stores (re_b, re_b+1)
-                    // in the re row, the odd lane (im_b-1, im_b) in the im row, one whole word each
-                    uint32_t* ot = reinterpret_cast<uint32_t*>(sm.otile[nbox & 1]) + kl * TB + (b & 1) * (TB / 2) +
-                                   (b >> 1);
-                    const uint32_t sel = (b & 1) ? 0x3276u : 0x5410u;
+                    __half* ot = sm.otile[nbox & 1] + kl * (2 * TB) + b;
 #pragma unroll
                     for (int kk = 0; kk < 16; kk++) {
                         const int k2 = 16 * hf + kk;
                         const float2 y = cmul(make_float2(__uint_as_float(v[2 * kk]), __uint_as_float(v[2 * kk + 1])),
-                                              sm.fstep[k2][b]);
+                                              fst[k2][b]);
                         const __half2 hv = __floats2half2_rn(y.x, y.y);
-                        const uint32_t mine = h2u(hv);
-                        const uint32_t other = __shfl_xor_sync(0xffffffffu, mine, 1);
-                        ot[kk * (16 * TB)] = __byte_perm(mine, other, sel);
+                        ot[kk * (16 * 2 * TB)] = __low2half(hv);
+                        ot[kk * (16 * 2 * TB) + TB] = __high2half(hv);
                         if constexpr (AMAX) {
                             // max(|Re|, |Im|) of the stored values over the item's 8 FFTs: the 8 lanes
                             // b = 0..7 of a channel are consecutive (lane = 8 (kl % 4) + b)
@@ -430,11 +431,12 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a, const __grid_con
                     for (int kk = 0; kk < 16; kk++) {
                         const int k2 = 16 * hf + kk;
                         pk[F1 * k2] = cmul(make_float2(__uint_as_float(v[2 * kk]), __uint_as_float(v[2 * kk + 1])),
-                                           sm.fstep[k2][b]);
+                                           fst[k2][b]);
                     }
                 }
                 }
             }
+            mbar_arrive(&sm.fs_empty[i & 1]);   // done with the item's fstep table
         }
         if constexpr (OUT16) {
             if (to == 0) bulk_wait_all();   // the stores are complete before the CTA exits
