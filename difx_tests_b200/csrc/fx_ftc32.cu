@@ -22,15 +22,18 @@
 //            spectra (plain form and the spectra check)
 // b = the FFT within a work item of 8 consecutive FFTs of one (subband, antenna).
 //
-// Persistent, warp-specialised CTA (one per SM, 576 threads):
+// Persistent, warp-specialised CTA (one per SM, 704 threads):
 //   warps 0-3    producer: 2-bit codes -> table lookups -> A1 pairs (TMEM, two stages)
 //   warps 4-11   twiddle: D1 (TMEM, one slot per pair of the item) -> Z pairs -> A2 (shared);
 //                tile 0 (k1 < 16) for the item's four pairs, then tile 1, so the step-2 MMAs
-//                of one tile run while the other is written
-//   warps 12-15  output: D2 (TMEM, one slot per tile) -> fstep -> spectra
-//   warp 16      MMA issuer (one thread), TMEM owner
-//   warp 17      helper: up to four pairs ahead, the input bulk copies, the level x step tables
+//                of one tile run while the other is written; also the item's fstep table
+//   warps 12-19  output, two groups of four: D2 (TMEM, one slot per tile; group g takes
+//                columns 32 g .. 32 g + 31) -> fstep -> FP16 boxes in shared memory written out
+//                by one tensor store each (or FP32 spectra by plain stores)
+//   warp 20      MMA issuer (one elected lane), TMEM owner
+//   warp 21      helper: up to four pairs ahead, the input bulk copies, the level x step tables
 //                and the window offsets
+// 22 warps are 6 on some schedulers, which holds every thread to 80 registers.
 // Every wait is bounded (1 s): on expiry the CTA records code 7 in the error word, stops,
 // drains what it issued and frees TMEM (or keeps it allocated if the drain itself expires).
 #include <cstring>
@@ -51,8 +54,9 @@ constexpr int TB = 8;                     // FFTs per work item
 constexpr int NPAIR = TB / 2;             // step-1 tiles (FFT pairs) per item
 constexpr int NA1 = 2;                    // A1 stages (TMEM)
 constexpr int NIB = 4;                    // pair slots the helper fills ahead of the producer
-constexpr int NTHREADS = 576;             // 18 warps
-constexpr int W_TW = 4, W_OUT = 12, W_MMA = 16, W_HELP = 17;
+constexpr int NOUT = 8;                   // output warps (two per TMEM lane quarter)
+constexpr int NTHREADS = 704;             // 22 warps
+constexpr int W_TW = 4, W_OUT = 12, W_MMA = W_OUT + NOUT, W_HELP = W_MMA + 1;
 constexpr uint32_t TMEM_COLS = 512;
 constexpr uint32_t A1_COL = 0;            // [stage] 64 columns: x_hi (n1, re|im) | x_lo
 constexpr uint32_t D1_COL = 128;          // [pair of the item] 64 columns (k1, re|im)
@@ -69,7 +73,8 @@ struct Smem {
     int2 pwin[NIB][2];                              // [pair % NIB][FFT] (bit of sample 0 in inb, valid)
     float2 fstep[2][K2H][TB];                       // [item parity][k2][b] fstep of the item's FFTs (a warp's
                                                     // 8 FFTs: one 64-byte row), written by the twiddle warps
-    alignas(128) __half otile[2][16 * 16 * 2 * TB]; // output: FP16 boxes [k2 % 16][k1 % 16][re|im][b] of the tensor store
+    alignas(128) __half otile[2][2][16 * 16 * 2 * TB];   // output: [group][buffer] FP16 boxes
+                                                          // [k2 % 16][k1 % 16][re|im][b] of the tensor store
     float ctab[P::FS + P::FST];                     // chan_sub | chan_step
     uint64_t a1_full[NA1], a1_empty[NA1], d1_full[NPAIR], d1_empty[NPAIR];
     uint64_t a2_full[2], a2_empty[2], d2_full[2], d2_empty[2], drain;
@@ -145,12 +150,12 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a, const __grid_con
             mbar_init(&sm.a2_full[j], 256);
             mbar_init(&sm.a2_empty[j], 1);
             mbar_init(&sm.d2_full[j], 1);
-            mbar_init(&sm.d2_empty[j], 128);
+            mbar_init(&sm.d2_empty[j], 32 * NOUT);
         }
         mbar_init(&sm.drain, 1);
         for (int s = 0; s < 2; s++) {
             mbar_init(&sm.fs_full[s], 256);
-            mbar_init(&sm.fs_empty[s], 128);
+            mbar_init(&sm.fs_empty[s], 32 * NOUT);
         }
         for (int s = 0; s < NIB; s++) {
             mbar_init(&sm.cp_full[s], 1);
@@ -358,19 +363,23 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a, const __grid_con
         }
     } else if (warp < W_MMA) {
         // ================================================================ output
+        // Two groups of four warps (one per TMEM lane quarter): group g takes half g of every D2
+        // tile, channels k2 = 16 g .. 16 g + 15 (32 columns)
         const int q = warp & 3;
+        const int g = (warp - W_OUT) >> 2;
         const int r = 32 * q + lane;                // D2 row: k1 % 16 = r / 8, b = r % 8
         const int kl = r >> 3, b = r & 7;
         const uint32_t lane_off = (uint32_t)(32 * q) << 16;
         const int to = threadIdx.x - 32 * W_OUT;
+        const bool issuer = (to & 127) == 0;       // the group's tensor-store thread
         const int nsig = a.nant;
         bool ok = true;
-        int nbox = 0;   // tensor stores issued (FP16 output): buffer nbox & 1 is the next to fill
-        // Every barrier below is reached by all four output warps in the same order: a failed
-        // wait is agreed on through bar_or at the top of an item before any warp leaves the loop.
+        int nbox = 0;   // tensor stores of this group (FP16 output): buffer nbox & 1 is the next to fill
+        // Every barrier below is reached by all output warps of a group (bar_or: of both groups) in
+        // the same order: a failed wait is agreed on at the top of an item before any warp leaves.
         for (int i = 0; i < nitem; i++) {
             const Item it = item_of<TB>(blockIdx.x + i * gridDim.x, a.nant, ntb);
-            if (bar_or(2, 128, !ok || *abort_flag)) break;
+            if (bar_or(2, 32 * NOUT, !ok || *abort_flag)) break;
             // the item's fstep table (twiddle warps)
             if (!mbar_wait_warp(&sm.fs_full[i & 1], (i >> 1) & 1, abort_flag)) ok = false;
             const float2 (*fst)[TB] = sm.fstep[i & 1];
@@ -381,24 +390,19 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a, const __grid_con
                 if (!mbar_wait_warp(&sm.d2_full[j], i & 1, abort_flag)) ok = false;
                 tc_fence_after();
                 const int k1 = 16 * j + kl;
-                // two halves of 16 channels k2 (32 columns each), to keep the registers low
-#pragma unroll 1
-                for (int hf = 0; hf < 2; hf++) {
                 uint32_t v[32];
-                tmem_ld32(tmem + lane_off + D2_COL + 64 * j + 32 * hf, v);
+                tmem_ld32(tmem + lane_off + D2_COL + 64 * j + 32 * g, v);
                 tmem_wait_ld();
-                if (hf == 1) {
-                    tc_fence_before();
-                    mbar_arrive(&sm.d2_empty[j]);
-                }
+                tc_fence_before();
+                mbar_arrive(&sm.d2_empty[j]);
                 if constexpr (OUT16) {
                     // the half tile (16 k1 x 16 k2 channels x re|im x 8 FFTs) goes out as one tensor
-                    // store from a double-buffered shared box; the store that last read this
-                    // buffer was waited for before the previous barrier
-                    __half* ot = sm.otile[nbox & 1] + kl * (2 * TB) + b;
+                    // store from the group's double-buffered shared box; the store that last read
+                    // this buffer was waited for before the group's previous barrier
+                    __half* ot = sm.otile[g][nbox & 1] + kl * (2 * TB) + b;
 #pragma unroll
                     for (int kk = 0; kk < 16; kk++) {
-                        const int k2 = 16 * hf + kk;
+                        const int k2 = 16 * g + kk;
                         const float2 y = cmul(make_float2(__uint_as_float(v[2 * kk]), __uint_as_float(v[2 * kk + 1])),
                                               fst[k2][b]);
                         const __half2 hv = __floats2half2_rn(y.x, y.y);
@@ -416,11 +420,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a, const __grid_con
                         }
                     }
                     fence_async_smem();   // these writes, visible to the tensor store
-                    if (to == 0) bulk_wait_read_all();   // the previous store has read the other buffer
-                    named_bar(3, 128);
-                    if (to == 0) {
-                        // box origin: FFT tb0, row 2 ant, k1 = 16 j, k2 = 16 hf of subband sb
-                        tma_store_4d(&omap, sm.otile[nbox & 1], it.tb0, 2 * it.ant, 16 * j, K2H * it.sb + 16 * hf);
+                    if (issuer) bulk_wait_read_all();   // the group's previous store has read the other buffer
+                    named_bar(3 + g, 128);
+                    if (issuer) {
+                        // box origin: FFT tb0, row 2 ant, k1 = 16 j, k2 = 16 g of subband sb
+                        tma_store_4d(&omap, sm.otile[g][nbox & 1], it.tb0, 2 * it.ant, 16 * j, K2H * it.sb + 16 * g);
                         bulk_commit();
                     }
                     nbox++;
@@ -429,17 +433,16 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a, const __grid_con
                                  (((size_t)it.sb * nsig + it.ant) * a.T + it.tb0 + b) * C + k1;
 #pragma unroll
                     for (int kk = 0; kk < 16; kk++) {
-                        const int k2 = 16 * hf + kk;
+                        const int k2 = 16 * g + kk;
                         pk[F1 * k2] = cmul(make_float2(__uint_as_float(v[2 * kk]), __uint_as_float(v[2 * kk + 1])),
                                            fst[k2][b]);
                     }
-                }
                 }
             }
             mbar_arrive(&sm.fs_empty[i & 1]);   // done with the item's fstep table
         }
         if constexpr (OUT16) {
-            if (to == 0) bulk_wait_all();   // the stores are complete before the CTA exits
+            if (issuer) bulk_wait_all();   // the stores are complete before the CTA exits
         }
         if (!ok) {
             if (!*abort_flag) atomicCAS(a.err, 0, ERR_WAIT);
