@@ -22,7 +22,7 @@
 //            spectra (plain form and the spectra check)
 // b = the FFT within a work item of 8 consecutive FFTs of one (subband, antenna).
 //
-// Persistent, warp-specialised CTA (one per SM, 704 threads):
+// Persistent, warp-specialised CTA (one per SM, 736 threads):
 //   warps 0-3    producer: 2-bit codes -> table lookups -> A1 pairs (TMEM, two stages)
 //   warps 4-11   twiddle: D1 (TMEM, one slot per pair of the item) -> Z pairs -> A2 (shared);
 //                tile 0 (k1 < 16) for the item's four pairs, then tile 1, so the step-2 MMAs
@@ -31,9 +31,9 @@
 //                columns 32 g .. 32 g + 31) -> fstep -> FP16 boxes in shared memory written out
 //                by one tensor store each (or FP32 spectra by plain stores)
 //   warp 20      MMA issuer (one elected lane), TMEM owner
-//   warp 21      helper: up to four pairs ahead, the input bulk copies, the level x step tables
-//                and the window offsets
-// 22 warps are 6 on some schedulers, which holds every thread to 80 registers.
+//   warps 21-22  helpers (alternate pairs): up to four pairs ahead, the input bulk copies, the
+//                level x step tables and the window offsets
+// 23 warps are 6 on three of the four schedulers, which holds every thread to 80 registers.
 // Every wait is bounded (1 s): on expiry the CTA records code 7 in the error word, stops,
 // drains what it issued and frees TMEM (or keeps it allocated if the drain itself expires).
 #include <cstring>
@@ -55,7 +55,8 @@ constexpr int NPAIR = TB / 2;             // step-1 tiles (FFT pairs) per item
 constexpr int NA1 = 2;                    // A1 stages (TMEM)
 constexpr int NIB = 4;                    // pair slots the helper fills ahead of the producer
 constexpr int NOUT = 8;                   // output warps (two per TMEM lane quarter)
-constexpr int NTHREADS = 704;             // 22 warps
+constexpr int NHELP = 2;                  // helper warps (alternate pairs)
+constexpr int NTHREADS = 736;             // 23 warps
 constexpr int W_TW = 4, W_OUT = 12, W_MMA = W_OUT + NOUT, W_HELP = W_MMA + 1;
 constexpr uint32_t TMEM_COLS = 512;
 constexpr uint32_t A1_COL = 0;            // [stage] 64 columns: x_hi (n1, re|im) | x_lo
@@ -448,11 +449,13 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a, const __grid_con
             if (!*abort_flag) atomicCAS(a.err, 0, ERR_WAIT);
             *abort_flag = 1;
         }
-    } else if (warp == W_HELP) {
+    } else if (warp >= W_HELP) {
         // ================================================================ helper
         // For each pair, NIB pairs ahead of the producer: the input copies, the tables
         // level(code) * step[n1] as FP16 pairs (step phase lo n1 stride a / F, kernel.c:434-470,
-        // one FP64 multiply from the per-FFT slope) and the window offsets.
+        // one FP64 multiply from the per-FFT slope) and the window offsets.  Helper warp hs takes
+        // the pairs g = hs (mod NHELP).
+        const int hs = warp - W_HELP;
         const int npair = nitem * NPAIR;
         DelayEntry dn0, dn1;
         double lon = 0.0;
@@ -465,14 +468,14 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a, const __grid_con
             lo = a.sb_lo[it.sb];
             row = a.data + ((size_t)it.sb * a.nant + it.ant) * a.pitch;
         };
-        if (npair > 0) fetch(0, dn0, dn1, lon, rown);
+        if (hs < npair) fetch(hs, dn0, dn1, lon, rown);
         int issued = -1;
-        for (int g = 0; g < npair; g++) {
+        for (int g = hs; g < npair; g += NHELP) {
             const int x = g % NIB;
             const DelayEntry d0 = dn0, d1 = dn1;
             const double lo = lon;
             const uint8_t* row = rown;
-            if (g + 1 < npair) fetch(g + 1, dn0, dn1, lon, rown);
+            if (g + NHELP < npair) fetch(g + NHELP, dn0, dn1, lon, rown);
             if (!mbar_wait_warp(&sm.tab_empty[x], ((g / NIB) & 1) ^ 1, abort_flag)) {
                 if (!*abort_flag) atomicCAS(a.err, 0, ERR_WAIT);
                 *abort_flag = 1;
@@ -506,10 +509,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a, const __grid_con
             __syncwarp();
             if (lane == 0) mbar_arrive(&sm.tab_full[x]);
         }
-        // copies must land before the CTA exits (phases already complete return at once)
+        // this warp's copies must land before the CTA exits (phases already complete return at once)
         if (lane == 0)
-            for (int g = issued - (NIB - 1); g <= issued; g++)
-                if (g >= 0 && !mbar_drain(&sm.cp_full[g % NIB], (g / NIB) & 1)) {
+            for (int g = issued; g >= 0 && g > issued - NIB; g -= NHELP)
+                if (!mbar_drain(&sm.cp_full[g % NIB], (g / NIB) & 1)) {
                     atomicCAS(a.err, 0, ERR_WAIT);
                     sm.drain_fail = 1;
                 }
