@@ -28,8 +28,8 @@
 //                tile 0 (k1 < 16) for the item's four pairs, then tile 1, so the step-2 MMAs
 //                of one tile run while the other is written; also the item's fstep table
 //   warps 12-19  output, two groups of four: D2 (TMEM, one slot per tile; group g takes
-//                columns 32 g .. 32 g + 31) -> fstep -> FP16 boxes in shared memory written out
-//                by one tensor store each (or FP32 spectra by plain stores)
+//                columns 32 g .. 32 g + 31) -> fstep -> an FP16 box per warp in shared memory
+//                written out by one tensor store (or FP32 spectra by plain stores)
 //   warp 20      MMA issuer (one elected lane), TMEM owner
 //   warps 21-22  helpers (alternate pairs): up to four pairs ahead, the input bulk copies, the
 //                level x step tables and the window offsets
@@ -74,8 +74,8 @@ struct Smem {
     int2 pwin[NIB][2];                              // [pair % NIB][FFT] (bit of sample 0 in inb, valid)
     float2 fstep[2][K2H][TB];                       // [item parity][k2][b] fstep of the item's FFTs (a warp's
                                                     // 8 FFTs: one 64-byte row), written by the twiddle warps
-    alignas(128) __half otile[2][2][16 * 16 * 2 * TB];   // output: [group][buffer] FP16 boxes
-                                                          // [k2 % 16][k1 % 16][re|im][b] of the tensor store
+    alignas(128) __half otile[NOUT][2][16 * 4 * 2 * TB]; // output: [warp][buffer] FP16 boxes
+                                                          // [k2 % 16][k1 % 4][re|im][b] of the tensor store
     float ctab[P::FS + P::FST];                     // chan_sub | chan_step
     uint64_t a1_full[NA1], a1_empty[NA1], d1_full[NPAIR], d1_empty[NPAIR];
     uint64_t a2_full[2], a2_empty[2], d2_full[2], d2_empty[2], drain;
@@ -372,12 +372,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a, const __grid_con
         const int kl = r >> 3, b = r & 7;
         const uint32_t lane_off = (uint32_t)(32 * q) << 16;
         const int to = threadIdx.x - 32 * W_OUT;
-        const bool issuer = (to & 127) == 0;       // the group's tensor-store thread
         const int nsig = a.nant;
         bool ok = true;
-        int nbox = 0;   // tensor stores of this group (FP16 output): buffer nbox & 1 is the next to fill
-        // Every barrier below is reached by all output warps of a group (bar_or: of both groups) in
-        // the same order: a failed wait is agreed on at the top of an item before any warp leaves.
+        int nbox = 0;   // tensor stores of this warp (FP16 output): buffer nbox & 1 is the next to fill
+        // bar_or is reached by all output warps in the same order: a failed wait is agreed on at the
+        // top of an item before any warp leaves.
         for (int i = 0; i < nitem; i++) {
             const Item it = item_of<TB>(blockIdx.x + i * gridDim.x, a.nant, ntb);
             if (bar_or(2, 32 * NOUT, !ok || *abort_flag)) break;
@@ -397,18 +396,20 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a, const __grid_con
                 tc_fence_before();
                 mbar_arrive(&sm.d2_empty[j]);
                 if constexpr (OUT16) {
-                    // the half tile (16 k1 x 16 k2 channels x re|im x 8 FFTs) goes out as one tensor
-                    // store from the group's double-buffered shared box; the store that last read
-                    // this buffer was waited for before the group's previous barrier
-                    __half* ot = sm.otile[g][nbox & 1] + kl * (2 * TB) + b;
+                    // the warp's quarter of the half tile (4 k1 x 16 k2 channels x re|im x 8 FFTs)
+                    // goes out as one tensor store from its double-buffered shared box, once the
+                    // store that last read this buffer (two stores ago) has read it
+                    if (lane == 0) bulk_wait_read_1();
+                    __syncwarp();
+                    __half* ot = sm.otile[warp - W_OUT][nbox & 1] + (lane >> 3) * (2 * TB) + b;
 #pragma unroll
                     for (int kk = 0; kk < 16; kk++) {
                         const int k2 = 16 * g + kk;
                         const float2 y = cmul(make_float2(__uint_as_float(v[2 * kk]), __uint_as_float(v[2 * kk + 1])),
                                               fst[k2][b]);
                         const __half2 hv = __floats2half2_rn(y.x, y.y);
-                        ot[kk * (16 * 2 * TB)] = __low2half(hv);
-                        ot[kk * (16 * 2 * TB) + TB] = __high2half(hv);
+                        ot[kk * (4 * 2 * TB)] = __low2half(hv);
+                        ot[kk * (4 * 2 * TB) + TB] = __high2half(hv);
                         if constexpr (AMAX) {
                             // max(|Re|, |Im|) of the stored values over the item's 8 FFTs: the 8 lanes
                             // b = 0..7 of a channel are consecutive (lane = 8 (kl % 4) + b)
@@ -421,11 +422,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a, const __grid_con
                         }
                     }
                     fence_async_smem();   // these writes, visible to the tensor store
-                    if (issuer) bulk_wait_read_all();   // the group's previous store has read the other buffer
-                    named_bar(3 + g, 128);
-                    if (issuer) {
-                        // box origin: FFT tb0, row 2 ant, k1 = 16 j, k2 = 16 g of subband sb
-                        tma_store_4d(&omap, sm.otile[g][nbox & 1], it.tb0, 2 * it.ant, 16 * j, K2H * it.sb + 16 * g);
+                    __syncwarp();
+                    if (lane == 0) {
+                        // box origin: FFT tb0, row 2 ant, k1 = 16 j + 4 q, k2 = 16 g of subband sb
+                        tma_store_4d(&omap, sm.otile[warp - W_OUT][nbox & 1], it.tb0, 2 * it.ant, 16 * j + 4 * q,
+                                     K2H * it.sb + 16 * g);
                         bulk_commit();
                     }
                     nbox++;
@@ -443,7 +444,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a, const __grid_con
             mbar_arrive(&sm.fs_empty[i & 1]);   // done with the item's fstep table
         }
         if constexpr (OUT16) {
-            if (issuer) bulk_wait_all();   // the stores are complete before the CTA exits
+            if (lane == 0) bulk_wait_all();   // the stores are complete before the CTA exits
         }
         if (!ok) {
             if (!*abort_flag) atomicCAS(a.err, 0, ERR_WAIT);
@@ -643,7 +644,7 @@ cudaError_t launch_ftc32(int mode, const FArgs& a, cudaStream_t st)
     std::memset(&omap, 0, sizeof(omap));
     if (mode == kSpecF16) {
         // FP16 K-major spectra [sb][k2][k1][row][T] (channel k1 + 32 k2) as a 4-D tensor
-        // (T, row, k1, 32 sb + k2); boxes of 8 FFTs x 2 rows x 16 k1 x 16 k2.  T % 8 == 0 keeps
+        // (T, row, k1, 32 sb + k2); boxes of 8 FFTs x 2 rows x 4 k1 x 16 k2 (one output warp's).  T % 8 == 0 keeps
         // every stride a multiple of 16 bytes, and box origins at FFT tb0 (a multiple of 8) keep
         // the innermost coordinate 16-byte aligned.
         auto enc = tc::tensor_map_encoder();
@@ -651,7 +652,7 @@ cudaError_t launch_ftc32(int mode, const FArgs& a, cudaStream_t st)
         const cuuint64_t row_b = (cuuint64_t)a.T * 2;
         const cuuint64_t dims[4] = {(cuuint64_t)a.T, (cuuint64_t)a.rows, (cuuint64_t)F1, (cuuint64_t)K2H * a.nsb};
         const cuuint64_t strides[3] = {row_b, row_b * a.rows, row_b * a.rows * F1};
-        const cuuint32_t box[4] = {(cuuint32_t)TB, 2, 16, 16};
+        const cuuint32_t box[4] = {(cuuint32_t)TB, 2, 4, 16};
         const cuuint32_t estr[4] = {1, 1, 1, 1};
         if (enc(&omap, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 4, a.spec, dims, strides, box, estr,
                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
