@@ -31,16 +31,30 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // FFT 0 of the tile's first row / column signal in the stage; signals are SK elements apart, FFTs
 // TKS.  The operands of FFT tk + 1 are loaded while FFT tk's 256 FMAs run, so the shared-memory
 // latency hides behind independent arithmetic at two warps per scheduler.
+//
+// Each complex multiply-accumulate is two packed FP32 FMAs (fma.rn.f32x2 on the (re, im) pair):
+//   acc += (a.y, a.x) * (b.y, -b.y), then acc += (a.x, a.y) * (b.x, b.x)
+// i.e. re += a.y b.y then a.x b.x, im += -a.x b.y then a.y b.x: the operations and their order
+// of the scalar form fma(a.x, b.x, fma(a.y, b.y, re)), fma(a.y, b.x, fma(-a.x, b.y, im)), so
+// the sums are bit-identical to it, at half the FMA instructions.
+__device__ __forceinline__ void cmac2(float2& acc, float2 a, float2 asw, float2 bxx, float2 byn)
+{
+    acc = __ffma2_rn(asw, byn, acc);
+    acc = __ffma2_rn(a, bxx, acc);
+}
+
 template <int TK, int SK, int TKS>
 __device__ __forceinline__ void tile_fma(float2 (&acc)[8][8], const float2 (&a)[8], const float2 (&b)[8])
 {
+    float2 asw[8];
 #pragma unroll
-    for (int jj = 0; jj < 8; jj++)
+    for (int ii = 0; ii < 8; ii++) asw[ii] = make_float2(a[ii].y, a[ii].x);
 #pragma unroll
-        for (int ii = 0; ii < 8; ii++) {
-            acc[ii][jj].x = fmaf(a[ii].x, b[jj].x, fmaf(a[ii].y, b[jj].y, acc[ii][jj].x));
-            acc[ii][jj].y = fmaf(a[ii].y, b[jj].x, fmaf(-a[ii].x, b[jj].y, acc[ii][jj].y));
-        }
+    for (int jj = 0; jj < 8; jj++) {
+        const float2 bxx = make_float2(b[jj].x, b[jj].x), byn = make_float2(b[jj].y, -b[jj].y);
+#pragma unroll
+        for (int ii = 0; ii < 8; ii++) cmac2(acc[ii][jj], a[ii], asw[ii], bxx, byn);
+    }
 }
 
 template <int SK>
@@ -78,17 +92,22 @@ __device__ __forceinline__ void tile_stage(float2 (&acc)[8][8], const float2* pi
 // pa and B at pb: 72 pairs, the work of one tile, with the same alternating operand sets.
 __device__ __forceinline__ void diag_fma(float2 (&acc)[2][36], const float2 (&a)[8], const float2 (&b)[8])
 {
+    float2 asw[8], bsw[8];
 #pragma unroll
-    for (int jj = 0; jj < 8; jj++)
+    for (int ii = 0; ii < 8; ii++) {
+        asw[ii] = make_float2(a[ii].y, a[ii].x);
+        bsw[ii] = make_float2(b[ii].y, b[ii].x);
+    }
+#pragma unroll
+    for (int jj = 0; jj < 8; jj++) {
+        const float2 axx = make_float2(a[jj].x, a[jj].x), ayn = make_float2(a[jj].y, -a[jj].y);
+        const float2 bxx = make_float2(b[jj].x, b[jj].x), byn = make_float2(b[jj].y, -b[jj].y);
 #pragma unroll
         for (int ii = 0; ii <= jj; ii++) {
-            float2& u = acc[0][jj * (jj + 1) / 2 + ii];
-            float2& v = acc[1][jj * (jj + 1) / 2 + ii];
-            u.x = fmaf(a[ii].x, a[jj].x, fmaf(a[ii].y, a[jj].y, u.x));
-            u.y = fmaf(a[ii].y, a[jj].x, fmaf(-a[ii].x, a[jj].y, u.y));
-            v.x = fmaf(b[ii].x, b[jj].x, fmaf(b[ii].y, b[jj].y, v.x));
-            v.y = fmaf(b[ii].y, b[jj].x, fmaf(-b[ii].x, b[jj].y, v.y));
+            cmac2(acc[0][jj * (jj + 1) / 2 + ii], a[ii], asw[ii], axx, ayn);
+            cmac2(acc[1][jj * (jj + 1) / 2 + ii], b[ii], bsw[ii], bxx, byn);
         }
+    }
 }
 
 template <int TK, int SK, int TKS>
