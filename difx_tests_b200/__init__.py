@@ -81,6 +81,7 @@ SIGNATURES = {
     "fxc_device_input": (_I, [_P, C.POINTER(_P), C.POINTER(C.c_size_t)]),
     "fxc_get_visibilities": (_I, [_P, _FP, _IP, _I]),
     "fxc_get_visibilities_device": (_I, [_P, _P, _I]),
+    "fxc_get_amp_phase": (_I, [_P, _FP, _I]),
     "fxc_set_stream": (_I, [_P, _P]),
     "fxc_synchronize": (_I, [_P]),
     "fxc_host_alloc": (_I, [C.POINTER(_P), C.c_size_t]),
@@ -262,6 +263,16 @@ class Correlator:
                                            1 if normalize else 0), "fxc_get_visibilities")
         vis = out.view(np.complex64).reshape(self.nsb, self.nbl + self.nant, self.npol ** 2, self.nchan)
         return vis, counts
+
+    def amp_phase(self, normalize=False):
+        """-> (amplitude, phase) float32 [nsb][nbl + nant][npol^2][nchan] each, computed on the
+        device from the visibilities (the columns the reference's vis.out prints beside re, im)."""
+        n = self.nsb * (self.nbl + self.nant) * self.npol ** 2 * self.nchan
+        out = np.empty(2 * n, dtype=np.float32)
+        _check(_lib().fxc_get_amp_phase(self._ctx, out.ctypes.data_as(_FP), 1 if normalize else 0),
+               "fxc_get_amp_phase")
+        ap = out.reshape(self.nsb, self.nbl + self.nant, self.npol ** 2, self.nchan, 2)
+        return ap[..., 0], ap[..., 1]
 
     def visibilities_device(self, d_ptr, normalize=False):
         """Visibilities into device memory at d_ptr (vis_count complex64 values, the layout of

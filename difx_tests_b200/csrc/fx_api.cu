@@ -840,6 +840,22 @@ int fxc_get_visibilities(fxc_ctx* x, float* vis, int* counts, int normalize)
     return device_status(x);
 }
 
+int fxc_get_amp_phase(fxc_ctx* x, float* ampphase, int normalize)
+{
+    if (!x || !ampphase) return FXC_ERR_INVALID;
+    FXC_CK(cudaSetDevice(x->device));
+    for (int sb = 0; sb < x->cfg.nsubband; sb++) {
+        const int st = finalize_subbands(x, sb, 1, reinterpret_cast<float*>(x->d_vis), normalize);
+        if (st != FXC_OK) return st;
+        FXC_CK(launch_amp_phase(reinterpret_cast<float2*>(x->d_vis), (long long)(x->vis_bytes / sizeof(float2)),
+                                x->stream));
+        FXC_CK(cudaMemcpyAsync(reinterpret_cast<char*>(ampphase) + (size_t)sb * x->vis_bytes, x->d_vis, x->vis_bytes,
+                               cudaMemcpyDeviceToHost, x->stream));
+    }
+    FXC_CK(cudaStreamSynchronize(x->stream));
+    return device_status(x);
+}
+
 int fxc_set_plan(fxc_ctx* x, int fft_block, int x_variant)
 {
     if (!x || (fft_block != 8 && fft_block != 16 && fft_block != 32) || (x_variant != 0 && x_variant != 1))

@@ -189,4 +189,23 @@ cudaError_t launch_finalize(const float2* acc, int acc_layout, int nsig, int npo
     return cudaGetLastError();
 }
 
+// Amplitude and phase of each visibility in place, as saveVisibilities prints them (kernel.c:594-596,
+// vectorMagnitude / vectorPhase): |v| = sqrt(re^2 + im^2) with the two squares and their sum
+// rounded separately (no fused multiply-add), phase = atan2(im, re) in radians.
+__global__ void k_amp_phase(float2* __restrict__ v, long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float2 z = v[i];
+        v[i] = make_float2(sqrtf(__fadd_rn(__fmul_rn(z.x, z.x), __fmul_rn(z.y, z.y))), atan2f(z.y, z.x));
+    }
+}
+
+cudaError_t launch_amp_phase(float2* vis, long long n, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    const long long blocks = (n + 255) / 256;
+    k_amp_phase<<<(int)(blocks < 1184 ? blocks : 1184), 256, 0, st>>>(vis, n);
+    return cudaGetLastError();
+}
+
 }  // namespace fx

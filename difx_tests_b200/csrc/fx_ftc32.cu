@@ -371,7 +371,6 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc32(FArgs a, const __grid_con
         const int r = 32 * q + lane;                // D2 row: k1 % 16 = r / 8, b = r % 8
         const int kl = r >> 3, b = r & 7;
         const uint32_t lane_off = (uint32_t)(32 * q) << 16;
-        const int to = threadIdx.x - 32 * W_OUT;
         const int nsig = a.nant;
         bool ok = true;
         int nbox = 0;   // tensor stores of this warp (FP16 output): buffer nbox & 1 is the next to fill

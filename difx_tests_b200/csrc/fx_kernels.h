@@ -20,6 +20,7 @@ cudaError_t launch_delay_table_window(const double* delays, const double* fileof
 cudaError_t launch_counts(const uint32_t* vbits, int nant, int nwords, int* counts, cudaStream_t st);
 cudaError_t launch_finalize(const float2* acc, int acc_layout, int nsig, int npol, int nant, int nchan, int nsb,
                             const int* counts, int normalize, float2* vis, cudaStream_t st);
+cudaError_t launch_amp_phase(float2* vis, long long n, cudaStream_t st);
 cudaError_t launch_fstage(int nchan, int mode, const FArgs& a, cudaStream_t st);
 // tensor-core F stage (F16 layout, 2048-point FFTs of one polarisation of 2-bit real input)
 bool ftc_supported(int nchan, int mode, const FArgs& a);

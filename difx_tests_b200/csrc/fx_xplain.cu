@@ -51,9 +51,13 @@ __device__ __forceinline__ void tile_fma(float2 (&acc)[8][8], const float2 (&a)[
     for (int ii = 0; ii < 8; ii++) asw[ii] = make_float2(a[ii].y, a[ii].x);
 #pragma unroll
     for (int jj = 0; jj < 8; jj++) {
+        // the two FMAs of one accumulator eight instructions apart (the FMA latency hides behind
+        // the other accumulators of the column)
         const float2 bxx = make_float2(b[jj].x, b[jj].x), byn = make_float2(b[jj].y, -b[jj].y);
 #pragma unroll
-        for (int ii = 0; ii < 8; ii++) cmac2(acc[ii][jj], a[ii], asw[ii], bxx, byn);
+        for (int ii = 0; ii < 8; ii++) acc[ii][jj] = __ffma2_rn(asw[ii], byn, acc[ii][jj]);
+#pragma unroll
+        for (int ii = 0; ii < 8; ii++) acc[ii][jj] = __ffma2_rn(a[ii], bxx, acc[ii][jj]);
     }
 }
 

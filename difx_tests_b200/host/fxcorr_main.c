@@ -223,7 +223,8 @@ static void* read_subint(void* arg)
     return NULL;
 }
 
-static void write_visout(const char* path, const float* vis, int nbl, int np2, int nchan, double bw)
+/* vis: (re, im) pairs, ap: (amplitude, phase) pairs of the same visibilities (fxc_get_amp_phase) */
+static void write_visout(const char* path, const float* vis, const float* ap, int nbl, int np2, int nchan, double bw)
 {
     FILE* f = fopen(path, "w");
     if (!f) {
@@ -234,10 +235,9 @@ static void write_visout(const char* path, const float* vis, int nbl, int np2, i
         fprintf(f, "%5d %11.6f", c, (c + 0.5) / nchan * bw / 1e6);
         for (int b = 0; b < nbl; b++)
             for (int p = 0; p < np2; p++) {
-                const float re = vis[2 * (((size_t)b * np2 + p) * nchan + c)];
-                const float im = vis[2 * (((size_t)b * np2 + p) * nchan + c) + 1];
-                fprintf(f, " %11.6f %11.6f", re, im);
-                fprintf(f, " %11.6f %10.6f", sqrtf(re * re + im * im), atan2f(im, re));
+                const size_t e = 2 * (((size_t)b * np2 + p) * nchan + c);
+                fprintf(f, " %11.6f %11.6f", vis[e], vis[e + 1]);
+                fprintf(f, " %11.6f %10.6f", ap[e], ap[e + 1]);
             }
         fprintf(f, "\n");
     }
@@ -318,6 +318,7 @@ int main(int argc, char** argv)
     const size_t nvis = fxc_vis_count(&cfg);
     float* vis = NULL;
     if (fxc_host_alloc((void**)&vis, 2 * sizeof(float) * nvis) != FXC_OK) vis = malloc(2 * sizeof(float) * nvis);
+    float* ap = malloc(2 * sizeof(float) * nvis);
     int* counts = malloc(sizeof(int) * (nbl + c.nant));
     double* d = malloc(3 * sizeof(double) * c.nant);
     FILE* fbin = bin_path ? fopen(bin_path, "wb") : NULL;
@@ -345,6 +346,7 @@ int main(int argc, char** argv)
         st = fxc_reset(ctx);
         if (st == FXC_OK) st = fxc_process_host(ctx, (const uint8_t* const*)cur, d, c.offsets, 0, c.numffts);
         if (st == FXC_OK) st = fxc_get_visibilities(ctx, vis, counts, normalize);
+        if (st == FXC_OK) st = fxc_get_amp_phase(ctx, ap, normalize);
         if (threaded) pthread_join(reader, NULL);
         else if (s + 1 < nsubint) read_subint(&next);
         if (st != FXC_OK) {
@@ -359,7 +361,8 @@ int main(int argc, char** argv)
             /* one text file per subband: <out>[.<subint>][.sb<subband>] */
             if (c.nsubband > 1) snprintf(name, sizeof name, "%s.sb%d", base, sb);
             else snprintf(name, sizeof name, "%s", base);
-            write_visout(name, vis + 2 * (size_t)sb * (nbl + c.nant) * np2 * c.nchan, nbl, np2, c.nchan, c.bw);
+            const size_t o = 2 * (size_t)sb * (nbl + c.nant) * np2 * c.nchan;
+            write_visout(name, vis + o, ap + o, nbl, np2, c.nchan, c.bw);
         }
         if (fbin) {
             const int32_t hdr[4] = {c.nsubband, nbl + c.nant, c.npol * c.npol, c.nchan};

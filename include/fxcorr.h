@@ -175,6 +175,12 @@ int fxc_get_visibilities(fxc_ctx* ctx, float* vis, int* counts, int normalize);
 /* Same into device memory (d_vis: fxc_vis_count complex values). */
 int fxc_get_visibilities_device(fxc_ctx* ctx, float* d_vis, int normalize);
 
+/* Amplitude and phase (radians) of every visibility, computed on the device: the
+ * layout of fxc_get_visibilities with each (re, im) pair replaced by (|v|,
+ * atan2(im, re)), the two columns saveVisibilities prints beside re and im
+ * (kernel.c:594-596, vectorMagnitude / vectorPhase). */
+int fxc_get_amp_phase(fxc_ctx* ctx, float* ampphase, int normalize);
+
 /* Stream used by the context (a cudaStream_t); NULL restores the context's own. */
 int fxc_set_stream(fxc_ctx* ctx, void* stream);
 int fxc_synchronize(fxc_ctx* ctx);

@@ -96,6 +96,7 @@ def test_null_arguments_rejected():
     assert L.fxc_reset(None) == fx.FXC_ERR_INVALID
     assert L.fxc_process_host(None, None, None, None, 0, 1) == fx.FXC_ERR_INVALID
     assert L.fxc_get_visibilities(None, None, None, 0) == fx.FXC_ERR_INVALID
+    assert L.fxc_get_amp_phase(None, None, 0) == fx.FXC_ERR_INVALID
     assert L.fxc_strerror(fx.FXC_ERR_NOMEM).decode().startswith("out of")
 
 
