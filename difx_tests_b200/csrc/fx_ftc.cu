@@ -431,52 +431,76 @@ __global__ void __launch_bounds__(NTHREADS, 1) k_ftc(FArgs a)
                     atomicCAS(a.err, 0, ERR_WAIT);
                     sm.drain_fail = 1;
                 }
-    } else if (lane == 0) {
+    } else if (warp == 12) {
         // ================================================================ MMA issuer
+        // The whole warp runs the issue loop (warp-uniform descriptors) and one elected lane issues
+        // each group of MMAs and its commits; a single lane running the loop in a divergent branch
+        // spends far longer per MMA (measured on the FP32-grade F stage, fx_ftc32.cu).
+        const uint32_t dsm = (uint32_t)umma_desc(smem_u32(&sm));
+        auto dlo = [&](const void* p) -> uint32_t {
+            return dsm + (uint32_t)(((const char*)p - (const char*)&sm) >> 4);
+        };
+        constexpr uint32_t AH = sizeof(sm.a2[0][0]) >> 4, BH = sizeof(sm.b2[0]) >> 4;   // K halves
         bool ok = true;
         for (int i = 0; i < nitem && ok; i++) {
             for (int p = 0; p < NPAIR; p++) {
                 const int g = i * NPAIR + p;
                 const int s = g % NA1, dslot = g % ND1;
-                if (!mbar_wait(&sm.a1_full[s], (g / NA1) & 1, abort_flag) ||
-                    !mbar_wait(&sm.d1_empty[dslot], ((g / ND1) & 1) ^ 1, abort_flag)) {
+                if (!mbar_wait_warp(&sm.a1_full[s], (g / NA1) & 1, abort_flag) ||
+                    !mbar_wait_warp(&sm.d1_empty[dslot], ((g / ND1) & 1) ^ 1, abort_flag)) {
                     ok = false;
                     break;
                 }
                 tc_fence_after();
-                const uint32_t sa = smem_u32(sm.a1[s]), sb = smem_u32(sm.b1);
+                const uint32_t da = dlo(sm.a1[s]), db = dlo(sm.b1);
+                if (elect_one()) {
+                    umma_ss_acc<false>(tmem + dslot * 64, udesc(da), udesc(db), kIdesc);
 #pragma unroll
-                for (int kk = 0; kk < 4; kk++)
-                    umma<false>(tmem + dslot * 64, umma_desc(sa + kk * 32), umma_desc(sb + kk * 32), kIdesc,
-                                kk > 0 ? 1u : 0u);
-                umma_commit(&sm.a1_empty[s]);
-                umma_commit(&sm.d1_full[dslot]);
+                    for (int kk = 1; kk < 4; kk++)
+                        umma_ss_acc<true>(tmem + dslot * 64, udesc(da + 2 * kk), udesc(db + 2 * kk), kIdesc);
+                    umma_commit(&sm.a1_empty[s]);
+                    umma_commit(&sm.d1_full[dslot]);
+                }
+                __syncwarp();
             }
             if (!ok) break;
-            if (!mbar_wait(&sm.a2_full, i & 1, abort_flag) || !mbar_wait(&sm.d2_empty, (i & 1) ^ 1, abort_flag)) {
+            if (!mbar_wait_warp(&sm.a2_full, i & 1, abort_flag) || !mbar_wait_warp(&sm.d2_empty, (i & 1) ^ 1, abort_flag)) {
                 ok = false;
                 break;
             }
             tc_fence_after();
+            const uint32_t db = dlo(sm.b2[0]);
 #pragma unroll 1
-            for (int j = 0; j < 4; j++)
+            for (int j = 0; j < 4; j++) {
+                const uint32_t da = dlo(sm.a2[j][0]);
+                if (elect_one()) {
+                    umma_ss_acc<false>(tmem + D2_COL + 64 * j, udesc(da), udesc(db), kIdesc);
 #pragma unroll
-                for (int kk = 0; kk < 8; kk++)
-                    umma<false>(tmem + D2_COL + 64 * j, umma_desc(smem_u32(sm.a2[j][kk >> 2]) + (kk & 3) * 32),
-                                umma_desc(smem_u32(sm.b2[kk >> 2]) + (kk & 3) * 32), kIdesc, kk > 0 ? 1u : 0u);
-            umma_commit(&sm.a2_empty);
-            umma_commit(&sm.d2_full);
+                    for (int kk = 1; kk < 8; kk++)
+                        umma_ss_acc<true>(tmem + D2_COL + 64 * j, udesc(da + (kk >> 2) * AH + 2 * (kk & 3)),
+                                          udesc(db + (kk >> 2) * BH + 2 * (kk & 3)), kIdesc);
+                    if (j == 3) {
+                        umma_commit(&sm.a2_empty);
+                        umma_commit(&sm.d2_full);
+                    }
+                }
+                __syncwarp();
+            }
         }
-        if (!ok) {
+        if (!ok && lane == 0) {
             if (!*abort_flag) atomicCAS(a.err, 0, ERR_WAIT);
             *abort_flag = 1;
         }
-        // every MMA issued must have retired before TMEM is freed
-        umma_commit(&sm.drain);
-        if (!mbar_drain(&sm.drain, 0)) {
-            atomicCAS(a.err, 0, ERR_WAIT);
-            sm.drain_fail = 1;
+        // every MMA issued must have retired before TMEM is freed (the commit comes from the lane
+        // that issued them: elect.sync elects the same lowest active lane every time)
+        if (elect_one()) {
+            umma_commit(&sm.drain);
+            if (!mbar_drain(&sm.drain, 0)) {
+                atomicCAS(a.err, 0, ERR_WAIT);
+                sm.drain_fail = 1;
+            }
         }
+        __syncwarp();
     }
 
     __syncthreads();
