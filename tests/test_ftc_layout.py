@@ -175,3 +175,39 @@ def test_tc32_output_indices_cover_the_item_once():
         assert len(got) == 16 * 32 * TB32
     allk = {(16 * j + (r >> 3) + 32 * k2) for j in range(2) for r in range(128) for k2 in range(32)}
     assert allk == set(range(1024))
+
+
+def test_tc32_output_boxes_cover_the_item_once_and_store_conflict_free():
+    # FP16 output: output warp w = 4 g + q (group g, TMEM lane quarter q) takes D2 columns 32 g ..
+    # 32 g + 31 (k2 = 16 g + kk) of its 32 rows (kl = 4 q + lane // 8, b = lane % 8) of tile j; it
+    # writes half (kk, kl % 4, c, b) at kk * 64 + (lane // 8) * 16 + c * 8 + b of a 1024-half box
+    # [k2 % 16][k1 % 4][re|im][b], stored by one tensor store at (T = tb0, row 2 ant, k1 = 16 j + 4 q,
+    # 32 sb + 16 g) with box extents (8, 2, 4, 16).
+    covered = set()
+    for j in range(2):
+        for g in range(2):
+            for q in range(4):
+                box = {}
+                for lane in range(32):
+                    kl, b = 4 * q + lane // 8, lane % 8
+                    for kk in range(16):
+                        for c in range(2):
+                            idx = kk * 64 + (lane // 8) * 16 + c * 8 + b
+                            assert 0 <= idx < 16 * 4 * 2 * TB32
+                            # the tensor store's box order (T innermost, then row, k1, k2)
+                            t_, r_, z_, w_ = idx % 8, (idx // 8) % 2, (idx // 16) % 4, idx // 64
+                            assert (t_, r_, z_, w_) == (b, c, kl % 4, kk)
+                            k1 = 16 * j + 4 * q + z_
+                            k2 = 16 * g + w_
+                            box[idx] = (k1 + 32 * k2, c, b)
+                assert len(box) == 1024 and len(set(box.values())) == 1024
+                covered |= set(box.values())
+                # one store instruction (fixed kk, c): 32 lanes, four 16-byte runs 32 bytes apart,
+                # so each 4-byte bank word is shared by one lane pair only and 16 distinct banks
+                for kk in range(16):
+                    for c in range(2):
+                        words = [(kk * 64 + (lane // 8) * 16 + c * 8 + lane % 8) // 2 for lane in range(32)]
+                        assert len(set(words)) == 16 and len({w % 32 for w in words}) == 16
+    assert covered == {(k, c, b) for k in range(1024) for c in range(2) for b in range(TB32)}
+    # box origins: k1 = 16 j + 4 q in [0, 28], k2 = 16 g in {0, 16}: boxes stay inside the 32 x 32 channel grid
+    assert max(16 * j + 4 * q + 4 for j in range(2) for q in range(4)) <= 32
