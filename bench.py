@@ -353,8 +353,9 @@ def run_reference_arm(args):
 # DRAM bytes per input sample of the F-stage kernels (2048-point FFTs), dram__bytes_read.sum +
 # dram__bytes_write.sum from one ncu capture each on the 64-antenna x 1024-channel profiling case,
 # divided by the samples of that launch: key (fstage, F16 output)
-# (profiles/kernels_cfg2s_ncu_full.txt for k_fstage, profiles/k_ftc_cfg2s_ncu.txt for k_ftc).
-FSTAGE_DRAM_BYTES_PER_SAMPLE = {(1, True): 2.17, (1, False): 4.16, (2, True): 2.17}
+# (profiles/kernels_cfg2s_ncu_full.txt for k_fstage, profiles/k_ftc_cfg2s_ncu.txt for k_ftc,
+# profiles/k_ftc32_cfg2s_ncu.txt for k_ftc32).
+FSTAGE_DRAM_BYTES_PER_SAMPLE = {(1, True): 2.17, (1, False): 4.16, (2, True): 2.17, (3, True): 2.18}
 
 
 # form -> (fxc_config.xmode, fxc_config.fstage)
@@ -525,10 +526,11 @@ def run_gpu_arm(args):
         line["tc_vs_plain"] = {"gsamps": head["value"] / p["value"],
                                "x_stage_only": (p["stage_ms"][2] / max(1e-9, sm[2])),
                                "form": forms[0]}
-        for f in ("tc", "tc32f", "tc16f", "fp8"):
-            if f in res and f != forms[0]:
-                line[f + "_vs_plain"] = {"gsamps": res[f]["value"] / p["value"],
-                                         "x_stage_only": p["stage_ms"][2] / max(1e-9, res[f]["stage_ms"][2])}
+        # the other forms' ratios, by form name (the headline's is tc_vs_plain above)
+        line["forms_vs_plain"] = {
+            f: {"gsamps": res[f]["value"] / p["value"],
+                "x_stage_only": p["stage_ms"][2] / max(1e-9, res[f]["stage_ms"][2])}
+            for f in ("tc32f", "tc", "tc16f", "fp8") if f in res and f != forms[0]}
 
     corr = head["corr"]
     # ---- end to end through the C ABI with pinned host buffers (rank-local)

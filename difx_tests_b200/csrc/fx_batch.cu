@@ -1,5 +1,5 @@
-// fx_batch.cu -- many independent correlation jobs in grouped persistent
-// launches, replayed as one CUDA graph, with an autotuner for the F-stage FFT
+// fx_batch.cu -- many independent correlation jobs in grouped launches,
+// replayed as one CUDA graph, with an autotuner for the F-stage FFT
 // block size and the plain X-stage tile variant (include/fxcorr.h, fxc_batch_*).
 //
 // Each job owns an ordinary context (device input, delay table, spectra chunk,
@@ -8,7 +8,8 @@
 //   one k_xplain_batch launch per X group  {8-signal blocks, tile variant} (plain form, <= 64 signals)
 //   one X launch per remaining job: the FP16 tensor-core X stage, or the plain X stage of
 //   more than 64 signals
-// CTAs of a grouped launch stride over a task table, so small and large jobs share the
+// A grouped launch works through a task table (F: persistent CTAs striding over it; plain X:
+// one CTA per task), so small and large jobs share the
 // machine inside one launch.  The delay tables and baseline counts run first.
 #include <algorithm>
 #include <cmath>

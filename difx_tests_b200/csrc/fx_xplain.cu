@@ -313,18 +313,18 @@ k_xplain(XArgs a)
     xplain_block<NB, CG, TK>(a, blockIdx.y, blockIdx.x * CG, smem);
 }
 
-// Many jobs with the same tile plan in one persistent launch: CTAs stride over
-// a task table {job, subband, first channel}.
+// Many jobs with the same tile plan in one launch: CTA i takes task i {job, subband, first
+// channel} of the table, and the hardware's block scheduler balances the uneven jobs over the
+// SMs (a persistent grid striding over the table measured 13 % slower on the 12-job batch).
 template <int NB, int CG, int TK>
 __global__ void __launch_bounds__(XPlan<NB, CG, TK>::NTHREADS, 1)
 k_xplain_batch(const XArgs* __restrict__ jobs, const int4* __restrict__ tasks, int ntask)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    for (int i = blockIdx.x; i < ntask; i += gridDim.x) {
-        const int4 tk = tasks[i];
-        const XArgs a = jobs[tk.x];
+    if (blockIdx.x < ntask) {
+        const int4 tk = tasks[blockIdx.x];
+        const XArgs& a = jobs[tk.x];   // read where used (global, cached)
         xplain_block<NB, CG, TK>(a, tk.y, tk.z, smem);
-        __syncthreads();   // the next task refills the staging buffers
     }
 }
 
@@ -352,13 +352,8 @@ static cudaError_t launch_xb(const XArgs* d_jobs, const int4* d_tasks, int ntask
     static unsigned configured = 0;
     cudaError_t e = set_smem_once(kern, sm, &configured);
     if (e != cudaSuccess) return e;
-    int dev = 0, nsm = 0, per_sm = 0;
-    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
-    if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, P::NTHREADS, sm)) != cudaSuccess) return e;
-    int grid = nsm * (per_sm > 0 ? per_sm : 1);
-    if (grid > ntask) grid = ntask;
-    kern<<<grid, P::NTHREADS, sm, st>>>(d_jobs, d_tasks, ntask);
+    if (ntask <= 0) return cudaSuccess;
+    kern<<<ntask, P::NTHREADS, sm, st>>>(d_jobs, d_tasks, ntask);
     return cudaGetLastError();
 }
 

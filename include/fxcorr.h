@@ -212,14 +212,15 @@ int fxc_correlate_noalloc(const fxc_config* cfg, const uint8_t* d_data, size_t p
                           const double* fileoffsets, int first_fft, int nfft, float* d_vis, int* d_counts,
                           int normalize, void* stream);
 
-/* ---- many independent jobs in grouped persistent launches -------------------
+/* ---- many independent jobs in grouped launches ------------------------------
  * A batch holds jobs of uneven geometry (antennas, polarisations, channels,
  * subbands, subintegration length) and X form (plain FP32 or FP16 tensor cores).
  * fxc_batch_process runs every job's whole subintegration: one persistent
  * F-stage launch per group of jobs sharing FFT length, polarisation count and
- * spectra precision, one persistent plain X-stage launch per group of jobs of at
- * most 64 signals sharing an X tile plan (CTAs stride over a task table of {job,
- * subband, antenna or channel block}), and one X launch per other job (FP16
+ * spectra precision (CTAs stride over a task table of {job, subband, antenna
+ * block}), one plain X-stage launch per group of jobs of at most 64 signals
+ * sharing an X tile plan (one CTA per {job, subband, channel block} task), and
+ * one X launch per other job (FP16
  * tensor-core jobs, plain jobs of more than 64 signals), in rounds when a job
  * needs several spectra chunks.  The first call runs eagerly; later calls replay
  * one CUDA graph of the whole sequence.  FXC_ERR_UNSUPPORTED for the FP8 form,
