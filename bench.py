@@ -463,7 +463,7 @@ def run_gpu_arm(args):
 
     forms = {"all": ["tc32f", "tc", "tc16f", "fp8", "plain"], "both": ["tc32f", "plain"]}.get(args.xmode, [args.xmode])
     if w["nchan"] != 1024 or w["npol"] != 1:   # the tensor-core F stages cover 1024 ch x 1 pol only
-        forms = [f for f in forms if f not in ("tc16f", "tc32f")]
+        forms = list(dict.fromkeys("tc" if f in ("tc16f", "tc32f") else f for f in forms))
     res, failed = {}, {}
     for form in forms:
         try:
@@ -586,12 +586,29 @@ def run_gpu_arm(args):
         torch.cuda.empty_cache()
         sub.steps, sub.warmup = 2, 1
         line["cfg4"] = run_large_arm(sub, emit=False, max_windows=2)
+        # configs 1 and 0 (their own processes: fresh device memory, their own clocks)
+        line["cfg1"] = sub_bench(["--workload", "cfg1", "--xmode", "both", "--steps", "3", "--warmup", "3"])
+        line["cfg0"] = sub_bench(["--workload", "cfg0", "--xmode", "plain", "--steps", "10", "--warmup", "3"])
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def sub_bench(argv):
+    """One bounded bench.py run of another workload in a child process -> its JSON line (or the
+    error), recorded beside the headline."""
+    cmd = [sys.executable, os.path.abspath(__file__), *argv, "--no-extra", "--no-cpu"]
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+        lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+        if r.returncode == 0 and lines:
+            return json.loads(lines[-1])
+        return {"error": f"exit {r.returncode}: {r.stderr.strip()[-300:]}"}
+    except (subprocess.TimeoutExpired, ValueError) as e:
+        return {"error": str(e)[:300]}
 
 
 def run_shard_arm(args):
