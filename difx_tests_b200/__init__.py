@@ -250,7 +250,7 @@ class Correlator:
 
         out: optional caller-owned buffer of the same number of complex64 values (any
         shape); pinned memory (fxc_host_alloc, torch pin_memory) reads back at full
-        bandwidth, a fresh pageable array goes through the driver's staging copies."""
+        bandwidth, a fresh pageable array goes through CUDA's staging copies."""
         n = self.nsb * (self.nbl + self.nant) * self.npol ** 2 * self.nchan
         if out is None:
             out = np.empty(2 * n, dtype=np.float32)

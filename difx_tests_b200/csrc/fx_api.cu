@@ -106,7 +106,7 @@ const char* fxc_strerror(int s)
     case FXC_ERR_INVALID: return "invalid configuration or argument";
     case FXC_ERR_CUDA: return "CUDA runtime error";
     case FXC_ERR_NOMEM: return "out of device or pinned host memory";
-    case FXC_ERR_UNSUPPORTED: return "not supported by this build";
+    case FXC_ERR_UNSUPPORTED: return "not supported by this library";
     case FXC_ERR_NODEVICE: return "no sm_100 CUDA device";
     case FXC_ERR_TIMEOUT: return "device-side wait expired (result invalid)";
     default: return "unknown status";

@@ -38,7 +38,7 @@ extern "C" {
 #define FXC_ERR_INVALID      -1   /* bad configuration or argument */
 #define FXC_ERR_CUDA         -2   /* CUDA runtime error (see fxc_last_cuda_error) */
 #define FXC_ERR_NOMEM        -3   /* device or pinned-host allocation failed */
-#define FXC_ERR_UNSUPPORTED  -4   /* valid request this build does not implement */
+#define FXC_ERR_UNSUPPORTED  -4   /* valid request this library does not implement */
 #define FXC_ERR_NODEVICE     -5   /* no sm_100 CUDA device */
 #define FXC_ERR_TIMEOUT      -6   /* a bounded device-side wait expired; that call's result is invalid */
 

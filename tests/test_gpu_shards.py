@@ -4,7 +4,7 @@ processes, merged over torch.distributed, against one process correlating it who
 The reference splits a subintegration's FFTs into `split` partial accumulations and sums them
 (main.c:398-433, kernel.c:856-878); sharding.correlate_shard does that across ranks (time
 shards: one all-reduce of visibilities and counts) or hands each rank whole subbands (one
-all-gather).  This pool gives one GPU per call, so both ranks share it: their kernels are
+all-gather).  The test runs on one GPU, so both ranks share it: their kernels are
 independent (nothing on the device waits on the other rank) and the collectives run on the
 host through gloo; under NCCL the same code keeps the buffers on the device."""
 import multiprocessing as mp
