@@ -48,6 +48,9 @@ WORKLOADS = {
     # profiling case: cfg2 geometry, 1 subband, 4096 FFTs (134 MB input > L2, ~1.2 GB on the device)
     "cfg2s": dict(nant=64, npol=1, nchan=1024, nsb=1, numffts=4096, bw=64e6, lo=1.4e9, rho=0.1,
                   desc="64 ant x 1 pol x 1 subband x 1024 ch, 4096 FFTs (profiling size)"),
+    # profiling case: cfg1 geometry (4096-point FFTs, dual polarisation), 1 subband, 4096 FFTs
+    "cfg1s": dict(nant=16, npol=2, nchan=2048, nsb=1, numffts=4096, bw=64e6, lo=1.4e9, rho=0.05,
+                  desc="16 ant x 2 pol x 1 subband x 2048 ch, 4096 FFTs (profiling size)"),
 }
 
 # Batched uneven workload: 12 independent jobs, antenna counts fixed, FFT length, subband count and
