@@ -49,6 +49,10 @@ struct FPlan {
     static constexpr int BUF = F + F / 16;                    // padded exchange buffer (float2)
     static constexpr bool TWREG = (F <= 2048);                // twiddles cached in registers
     static constexpr int TWQ = F / 4;                         // quarter-wave twiddle table
+    // pass twiddle tables beside it (F > 2048): W256^(r j) [r][j] for pass 1, and W4096^(r l) [r][l],
+    // W4096^(16 r h) [r][h] for pass 2 (j = 16 h + l), so a warp's twiddle loads are consecutive or
+    // broadcast words instead of the strided quarter-wave reads (r j stride) that conflict
+    static constexpr int TWP = 3 * 256;
     static constexpr int MINB = (NTHREADS <= 256) ? 2 : 1;    // CTAs per SM the registers must allow
 };
 
@@ -213,6 +217,7 @@ template <int F, int PASS>
 __device__ __forceinline__ void pass_load(const float2* buf, const float2* tq, const PassTw<F, PASS>* tw,
                                           float2* v, int t)
 {
+    const float2* tp = tq + FPlan<F>::TWQ;   // pass tables (F > 2048)
     using PI = PassInfo<F, PASS>;
     constexpr int NT = FPlan<F>::NT;
     constexpr int STEP = F / PI::R;
@@ -228,6 +233,9 @@ __device__ __forceinline__ void pass_load(const float2* buf, const float2* tq, c
             if (r > 0) {
                 float2 w;
                 if constexpr (FPlan<F>::TWREG) w = tw->w[b * PI::R + r];
+                else if constexpr (PI::NS == 16 && PI::R == 16) w = tp[16 * r + jm];
+                else if constexpr (PI::NS == 256 && PI::R == 16)
+                    w = cmul(tp[512 + 16 * r + (jm >> 4)], tp[256 + 16 * r + (jm & 15)]);
                 else w = twiddle_q<F>(tq, r * jm * (F / (PI::NS * PI::R)));
                 x = cmul(x, w);
             }
@@ -356,7 +364,7 @@ template <int F, bool CPX>
 __device__ __forceinline__ uint64_t* fstage_bars(unsigned char* smem)
 {
     using P = FPlan<F, CPX>;
-    float2* rtabs = reinterpret_cast<float2*>(smem) + P::NSLOT * P::BUF + (P::TWREG ? 0 : P::TWQ);
+    float2* rtabs = reinterpret_cast<float2*>(smem) + P::NSLOT * P::BUF + (P::TWREG ? 0 : P::TWQ + P::TWP);
     return reinterpret_cast<uint64_t*>(reinterpret_cast<float*>(rtabs + 2 * P::NSLOT * P::NROT) + P::FS + P::FST);
 }
 
@@ -370,7 +378,7 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
     constexpr int INB = fstage_inb<F, NPOL, CPX>();                    // staged bytes per slot
     float2* bufs = reinterpret_cast<float2*>(smem);                   // [NSLOT][BUF]
     float2* tq = bufs + P::NSLOT * P::BUF;                              // [TWQ]
-    float2* rtabs = tq + (P::TWREG ? 0 : P::TWQ);                      // [NSLOT][2][NROT]
+    float2* rtabs = tq + (P::TWREG ? 0 : P::TWQ + P::TWP);             // [NSLOT][2][NROT]
     float* ctab = reinterpret_cast<float*>(rtabs + 2 * P::NSLOT * P::NROT);   // [FS + FST] channel freqs
     uint64_t* bars = reinterpret_cast<uint64_t*>(ctab + P::FS + P::FST);    // [NSLOT] (16 B each)
     uint8_t* inbs = reinterpret_cast<uint8_t*>(bars + 2 * P::NSLOT);        // [NSLOT][INB]
@@ -660,6 +668,14 @@ __device__ __forceinline__ void fstage_prologue(unsigned char* smem, PassTw<F, 1
     if constexpr (!P::TWREG) {
         float2* tq = reinterpret_cast<float2*>(smem) + P::NSLOT * P::BUF;
         for (int m = tid; m < P::TWQ; m += P::NTHREADS) tq[m] = twiddle_exact(m, F);
+        __syncthreads();
+        // pass tables from the quarter-wave table (pass 1 entries are exactly what twiddle_q returns)
+        float2* tp = tq + P::TWQ;
+        for (int e = tid; e < P::TWP; e += P::NTHREADS) {
+            const int k = e >> 8, r = (e >> 4) & 15, j = e & 15;
+            const int m = k == 0 ? r * j * (F / 256) : (k == 1 ? r * j : 16 * r * j) * (F / 4096);
+            tp[e] = twiddle_q<F>(tq, m);
+        }
     } else {
         init_pass_tw<F, 1>(tw1, t);
         if constexpr (P::NPASS > 2) init_pass_tw<F, 2>(tw2, t);
@@ -718,7 +734,7 @@ size_t fstage_smem(int mode, int tb, int npol)
 {
     using P = FPlan<F, CPX>;
     size_t s = (size_t)P::NSLOT * P::BUF * sizeof(float2);
-    if (!P::TWREG) s += (size_t)P::TWQ * sizeof(float2);
+    if (!P::TWREG) s += (size_t)(P::TWQ + P::TWP) * sizeof(float2);
     s += (size_t)2 * P::NSLOT * P::NROT * sizeof(float2);
     s += (size_t)(P::FS + P::FST) * sizeof(float);
     s += (size_t)P::NSLOT * 16;   // staging mbarriers
