@@ -48,11 +48,12 @@ struct FPlan {
     static constexpr int NTHREADS = NT * NSLOT;
     static constexpr int BUF = F + F / 16;                    // padded exchange buffer (float2)
     static constexpr bool TWREG = (F <= 2048);                // twiddles cached in registers
-    static constexpr int TWQ = F / 4;                         // quarter-wave twiddle table
-    // pass twiddle tables beside it (F > 2048): W256^(r j) [r][j] for pass 1, and W4096^(r l) [r][l],
-    // W4096^(16 r h) [r][h] for pass 2 (j = 16 h + l), so a warp's twiddle loads are consecutive or
-    // broadcast words instead of the strided quarter-wave reads (r j stride) that conflict
-    static constexpr int TWP = 3 * 256;
+    // pass twiddle tables in shared memory (F > 2048): W256^(r j) [r][j] for pass 1, W4096^(r l) [r][l]
+    // and W4096^(16 r h) [r][h] for pass 2 (j = 16 h + l), and for 8192 points W8192^(64 h) [h], W8192^l
+    // [l] for pass 3 (j = 64 h + l): a warp's twiddle loads are consecutive or broadcast words (reads of
+    // one quarter-wave table at the stride r j conflicted 16 ways), and the tables take 6-7 KB instead
+    // of the quarter wave's F / 4 entries, which leaves room for the F16 stage
+    static constexpr int TWP = 3 * 256 + (F == 8192 ? 128 : 0);
     static constexpr int MINB = (NTHREADS <= 256) ? 2 : 1;    // CTAs per SM the registers must allow
 };
 
@@ -74,12 +75,15 @@ struct PassInfo {
 
 __device__ __forceinline__ int padi(int i) { return i + (i >> 4); }
 
-// e^{-2 pi i m / F} from a quarter-wave table tq[m'] = e^{-2 pi i m'/F}, m' < F/4
+__device__ __forceinline__ float2 twiddle_exact(int m, int n);
+
+// e^{-2 pi i m / F} for 0 <= m < F: the first-quadrant value e^{-2 pi i m'/F} (m' = m mod F/4)
+// turned by the quadrant (exact: swaps and negations)
 template <int F>
-__device__ __forceinline__ float2 twiddle_q(const float2* tq, int m)
+__device__ __forceinline__ float2 twiddle_q(int m)
 {
     const int q = m / (F / 4);
-    const float2 b = tq[m & (F / 4 - 1)];
+    const float2 b = twiddle_exact(m & (F / 4 - 1), F);
     switch (q & 3) {
     case 0: return b;
     case 1: return make_float2(b.y, -b.x);
@@ -214,10 +218,9 @@ __device__ __forceinline__ void init_pass_tw(PassTw<F, PASS>& tw, int t)
 // offsets are multiples of 16 elements, so padi(t + c) = padi(t) + c + c/16 and
 // every shared-memory access is one base register plus an immediate.
 template <int F, int PASS>
-__device__ __forceinline__ void pass_load(const float2* buf, const float2* tq, const PassTw<F, PASS>* tw,
+__device__ __forceinline__ void pass_load(const float2* buf, const float2* tp, const PassTw<F, PASS>* tw,
                                           float2* v, int t)
 {
-    const float2* tp = tq + FPlan<F>::TWQ;   // pass tables (F > 2048)
     using PI = PassInfo<F, PASS>;
     constexpr int NT = FPlan<F>::NT;
     constexpr int STEP = F / PI::R;
@@ -236,7 +239,10 @@ __device__ __forceinline__ void pass_load(const float2* buf, const float2* tq, c
                 else if constexpr (PI::NS == 16 && PI::R == 16) w = tp[16 * r + jm];
                 else if constexpr (PI::NS == 256 && PI::R == 16)
                     w = cmul(tp[512 + 16 * r + (jm >> 4)], tp[256 + 16 * r + (jm & 15)]);
-                else w = twiddle_q<F>(tq, r * jm * (F / (PI::NS * PI::R)));
+                else {
+                    static_assert(PI::NS == 4096 && PI::R == 2, "every pass of F > 2048 has its table");
+                    w = cmul(tp[768 + (jm >> 6)], tp[832 + (jm & 63)]);
+                }
                 x = cmul(x, w);
             }
             v[b * PI::R + r] = x;
@@ -364,7 +370,7 @@ template <int F, bool CPX>
 __device__ __forceinline__ uint64_t* fstage_bars(unsigned char* smem)
 {
     using P = FPlan<F, CPX>;
-    float2* rtabs = reinterpret_cast<float2*>(smem) + P::NSLOT * P::BUF + (P::TWREG ? 0 : P::TWQ + P::TWP);
+    float2* rtabs = reinterpret_cast<float2*>(smem) + P::NSLOT * P::BUF + (P::TWREG ? 0 : P::TWP);
     return reinterpret_cast<uint64_t*>(reinterpret_cast<float*>(rtabs + 2 * P::NSLOT * P::NROT) + P::FS + P::FST);
 }
 
@@ -377,8 +383,8 @@ __device__ __forceinline__ void fstage_block(const FArgs& args, int sb, int ant,
     constexpr int C = P::C;
     constexpr int INB = fstage_inb<F, NPOL, CPX>();                    // staged bytes per slot
     float2* bufs = reinterpret_cast<float2*>(smem);                   // [NSLOT][BUF]
-    float2* tq = bufs + P::NSLOT * P::BUF;                              // [TWQ]
-    float2* rtabs = tq + (P::TWREG ? 0 : P::TWQ + P::TWP);             // [NSLOT][2][NROT]
+    float2* tq = bufs + P::NSLOT * P::BUF;                              // [TWP] pass twiddle tables
+    float2* rtabs = tq + (P::TWREG ? 0 : P::TWP);                      // [NSLOT][2][NROT]
     float* ctab = reinterpret_cast<float*>(rtabs + 2 * P::NSLOT * P::NROT);   // [FS + FST] channel freqs
     uint64_t* bars = reinterpret_cast<uint64_t*>(ctab + P::FS + P::FST);    // [NSLOT] (16 B each)
     uint8_t* inbs = reinterpret_cast<uint8_t*>(bars + 2 * P::NSLOT);        // [NSLOT][INB]
@@ -666,15 +672,16 @@ __device__ __forceinline__ void fstage_prologue(unsigned char* smem, PassTw<F, 1
     const int tid = threadIdx.x;
     const int t = tid % P::NT;
     if constexpr (!P::TWREG) {
-        float2* tq = reinterpret_cast<float2*>(smem) + P::NSLOT * P::BUF;
-        for (int m = tid; m < P::TWQ; m += P::NTHREADS) tq[m] = twiddle_exact(m, F);
-        __syncthreads();
-        // pass tables from the quarter-wave table (pass 1 entries are exactly what twiddle_q returns)
-        float2* tp = tq + P::TWQ;
+        float2* tp = reinterpret_cast<float2*>(smem) + P::NSLOT * P::BUF;
         for (int e = tid; e < P::TWP; e += P::NTHREADS) {
-            const int k = e >> 8, r = (e >> 4) & 15, j = e & 15;
-            const int m = k == 0 ? r * j * (F / 256) : (k == 1 ? r * j : 16 * r * j) * (F / 4096);
-            tp[e] = twiddle_q<F>(tq, m);
+            int m;
+            if (e < 768) {
+                const int k = e >> 8, r = (e >> 4) & 15, j = e & 15;
+                m = k == 0 ? r * j * (F / 256) : (k == 1 ? r * j : 16 * r * j) * (F / 4096);
+            } else {
+                m = e < 832 ? 64 * (e - 768) : e - 832;   // 8192 points, pass 3
+            }
+            tp[e] = twiddle_q<F>(m);
         }
     } else {
         init_pass_tw<F, 1>(tw1, t);
@@ -734,7 +741,7 @@ size_t fstage_smem(int mode, int tb, int npol)
 {
     using P = FPlan<F, CPX>;
     size_t s = (size_t)P::NSLOT * P::BUF * sizeof(float2);
-    if (!P::TWREG) s += (size_t)(P::TWQ + P::TWP) * sizeof(float2);
+    if (!P::TWREG) s += (size_t)P::TWP * sizeof(float2);
     s += (size_t)2 * P::NSLOT * P::NROT * sizeof(float2);
     s += (size_t)(P::FS + P::FST) * sizeof(float);
     s += (size_t)P::NSLOT * 16;   // staging mbarriers
