@@ -51,6 +51,9 @@ WORKLOADS = {
     # profiling case: cfg1 geometry (4096-point FFTs, dual polarisation), 1 subband, 4096 FFTs
     "cfg1s": dict(nant=16, npol=2, nchan=2048, nsb=1, numffts=4096, bw=64e6, lo=1.4e9, rho=0.05,
                   desc="16 ant x 2 pol x 1 subband x 2048 ch, 4096 FFTs (profiling size)"),
+    # profiling case: the cfg4 FFT (8192 points, dual polarisation) on 16 antennas, 1 subband, 2048 FFTs
+    "cfg4s": dict(nant=16, npol=2, nchan=4096, nsb=1, numffts=2048, bw=64e6, lo=1.4e9, rho=0.05,
+                  desc="16 ant x 2 pol x 1 subband x 4096 ch, 2048 FFTs (profiling size)"),
 }
 
 # Batched uneven workload: 12 independent jobs, antenna counts fixed, FFT length, subband count and
