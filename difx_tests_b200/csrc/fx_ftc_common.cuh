@@ -17,9 +17,6 @@ static_assert(fstage_inb<2048, 1, false>() + 16 <= INB, "staging buffer holds th
 // 16-byte chunk c of row r of a K-major SWIZZLE_128B tile
 __device__ __forceinline__ uint32_t sw128(int r, int c) { return (uint32_t)(r * 128 + ((c ^ (r & 7)) << 4)); }
 
-// bar.sync over `n` threads on named barrier `id`
-__device__ __forceinline__ void named_bar(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
-
 // bar.red.or over `n` threads on named barrier `id`: true if any thread passed p
 __device__ __forceinline__ bool bar_or(int id, int n, bool p)
 {
