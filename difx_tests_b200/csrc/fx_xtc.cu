@@ -173,51 +173,67 @@ k_xtc(const __grid_constant__ CUtensorMap tmap, XArgs a, int* err)
         }
     } else if (warp == 1) {
         // ------------------------------------------------------------ MMA issuer
-        if (lane == 0) {
-            int stage = 0;
-            uint32_t phase = 0;
-            int buf = 0;
-            uint32_t acc_phase = 0;
-            for (int item = blockIdx.x; item < nitems && !*abort_flag; item += gridDim.x) {
-                int I = 0, J = 0;
-                if (MB) block_pair(item % nbp, nb, I, J);
-                if (!mbar_wait(&sm.acc_empty[buf], acc_phase ^ 1, abort_flag)) {
+        // The whole warp runs the issue loop (warp-uniform waits and descriptors) and one elected
+        // lane issues each stage's MMAs and commits: one lane running the loop in a divergent
+        // branch spent ~130 cycles per MMA in the tensor-core F stage (fx_ftc32.cu).
+        const uint32_t dsm = (uint32_t)umma_desc(smem_u32(&sm));
+        auto dlo = [&](const void* p) -> uint32_t {
+            return dsm + (uint32_t)(((const char*)p - (const char*)&sm) >> 4);
+        };
+        int stage = 0;
+        uint32_t phase = 0;
+        int buf = 0;
+        uint32_t acc_phase = 0;
+        for (int item = blockIdx.x; item < nitems && !__any_sync(0xffffffffu, *abort_flag); item += gridDim.x) {
+            int I = 0, J = 0;
+            if (MB) block_pair(item % nbp, nb, I, J);
+            if (!mbar_wait_warp(&sm.acc_empty[buf], acc_phase ^ 1, abort_flag)) {
+                if (lane == 0) {
                     if (!*abort_flag) atomicCAS(err, 0, 3);
                     *abort_flag = 1;
+                }
+                break;
+            }
+            tc_fence_after();
+            const uint32_t d = tmem + buf * 128;
+            bool ok = true;
+            for (int kb = 0; kb < nk; kb++) {
+                if (!mbar_wait_warp(&sm.full[stage], phase, abort_flag)) {
+                    if (lane == 0) {
+                        if (!*abort_flag) atomicCAS(err, 0, 1);
+                        *abort_flag = 1;
+                    }
+                    ok = false;
                     break;
                 }
                 tc_fence_after();
-                const uint32_t d = tmem + buf * 128;
-                bool ok = true;
-                for (int kb = 0; kb < nk; kb++) {
-                    if (!mbar_wait(&sm.full[stage], phase, abort_flag)) {
-                        if (!*abort_flag) atomicCAS(err, 0, 1);
-                        *abort_flag = 1;
-                        ok = false;
-                        break;
-                    }
-                    tc_fence_after();
-                    const uint32_t sa = smem_u32(sm.stage[stage][0]);
-                    const uint32_t sb = (MB && I != J) ? smem_u32(sm.stage[stage][MB ? 1 : 0]) : sa;
+                const uint32_t da = dlo(sm.stage[stage][0]);
+                const uint32_t db = (MB && I != J) ? dlo(sm.stage[stage][MB ? 1 : 0]) : da;
+                if (elect_one()) {
+                    // 32 bytes of K per MMA (+2 in the descriptors' start field): K16 for f16, K32 for e4m3
+                    umma<F8>(d, udesc(da), udesc(db), kIdesc, kb > 0 ? 1u : 0u);
 #pragma unroll
-                    for (int k = 0; k < 4; k++) {   // 32 bytes of K per MMA: K16 for f16, K32 for e4m3
-                        umma<F8>(d, umma_desc(sa + k * 32), umma_desc(sb + k * 32), kIdesc, (kb > 0 || k > 0) ? 1u : 0u);
-                    }
+                    for (int k = 1; k < 4; k++) umma<F8>(d, udesc(da + 2 * k), udesc(db + 2 * k), kIdesc, 1u);
                     umma_commit(&sm.empty[stage]);
-                    if (++stage == NST) {
-                        stage = 0;
-                        phase ^= 1;
-                    }
                 }
-                if (!ok) break;
-                umma_commit(&sm.acc_full[buf]);
-                if (++buf == 2) {
-                    buf = 0;
-                    acc_phase ^= 1;
+                __syncwarp();
+                if (++stage == NST) {
+                    stage = 0;
+                    phase ^= 1;
                 }
             }
-            // drain: wait for every issued MMA before TMEM is freed
-            // (a dedicated barrier: committing to acc_full would advance it past a lagging epilogue)
+            if (!ok) break;
+            if (elect_one()) umma_commit(&sm.acc_full[buf]);
+            __syncwarp();
+            if (++buf == 2) {
+                buf = 0;
+                acc_phase ^= 1;
+            }
+        }
+        // drain: wait for every issued MMA before TMEM is freed, committed by the lane that issued
+        // them (elect.sync elects the same lowest active lane every time); a dedicated barrier:
+        // committing to acc_full would advance it past a lagging epilogue
+        if (elect_one()) {
             uint64_t* fin = &sm.drain;
             umma_commit(fin);
             const unsigned long long t0 = globaltimer();
@@ -229,6 +245,7 @@ k_xtc(const __grid_constant__ CUtensorMap tmap, XArgs a, int* err)
                 }
             }
         }
+        __syncwarp();
     } else {
         // ------------------------------------------------------------ epilogue
         const int q = warp & 3;                  // TMEM lane quadrant of this warp
