@@ -386,6 +386,16 @@ F_KERNELS = {1: "k_fstage (fused unpack/shift/fringe/FFT/frac-delay, FP32 radix-
                 "three products each, twiddles, frac-delay)"}
 
 
+def select_forms(xmode, w):
+    """Forms to time, the headline first: all -> tc32f, tc, tc16f, fp8, plain; both -> tc32f, plain;
+    a form name -> that form.  Geometries the tensor-core F stages do not cover (other than
+    1024 channels x 1 polarisation) take the tc form in their place."""
+    forms = {"all": ["tc32f", "tc", "tc16f", "fp8", "plain"], "both": ["tc32f", "plain"]}.get(xmode, [xmode])
+    if w["nchan"] != 1024 or w["npol"] != 1:
+        forms = list(dict.fromkeys("tc" if f in ("tc16f", "tc32f") else f for f in forms))
+    return forms
+
+
 def time_form(torch, dist, fx, w, form, data, pitch, delays, offs, steps, warmup, world, dev, stream):
     """Warm up, then time `steps` subintegrations of one form; returns a result dict."""
     F = 2 * w["nchan"]
@@ -467,9 +477,7 @@ def run_gpu_arm(args):
                            device=dev)
     torch.cuda.synchronize()
 
-    forms = {"all": ["tc32f", "tc", "tc16f", "fp8", "plain"], "both": ["tc32f", "plain"]}.get(args.xmode, [args.xmode])
-    if w["nchan"] != 1024 or w["npol"] != 1:   # the tensor-core F stages cover 1024 ch x 1 pol only
-        forms = list(dict.fromkeys("tc" if f in ("tc16f", "tc32f") else f for f in forms))
+    forms = select_forms(args.xmode, w)
     res, failed = {}, {}
     for form in forms:
         try:

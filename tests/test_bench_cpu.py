@@ -22,3 +22,16 @@ def test_reference_geometry_per_workload():
     for g in bench.REF_GEOMS.values():
         assert math.isqrt(g["nchan"]) ** 2 == g["nchan"]  # kernel.c:31-35 needs a square channel count
     bench.ref_geom_for("cfg2")
+
+
+def test_forms_headline_first_and_geometry_fallback():
+    w2 = bench.WORKLOADS["cfg2"]
+    assert bench.select_forms("all", w2) == ["tc32f", "tc", "tc16f", "fp8", "plain"]
+    assert bench.select_forms("both", w2) == ["tc32f", "plain"]
+    # 2048 channels x 2 pol: no tensor-core F stage, the FP32 FFT form leads
+    w1 = bench.WORKLOADS["cfg1"]
+    assert bench.select_forms("all", w1) == ["tc", "fp8", "plain"]
+    assert bench.select_forms("both", w1) == ["tc", "plain"]
+    assert bench.select_forms("plain", w1) == ["plain"]
+    for f, (xmode, fstage) in bench.FORMS.items():
+        assert f in bench.DTYPES and fstage in bench.F_KERNELS
