@@ -211,20 +211,12 @@ __device__ __forceinline__ void xplain_stages(const XArgs& a, int sb, int c0, fl
         } else if constexpr (P::PIPE) {
             tile_stage<TK, TK * CG, CG>(acc, pi, pj);
         } else {
+            // one operand set at a time (no prefetch: more than 256 threads leave no registers for
+            // a second set), the same packed FMAs
             for (int tk = 0; tk < TK; tk++) {
-                float2 xi[8];
-#pragma unroll
-                for (int ii = 0; ii < 8; ii++) xi[ii] = pi[ii * TK * CG + tk * CG];
-#pragma unroll
-                for (int jj = 0; jj < 8; jj++) {
-                    const float2 xj = pj[jj * TK * CG + tk * CG];
-#pragma unroll
-                    for (int ii = 0; ii < 8; ii++) {
-                        // acc += xi * conj(xj)
-                        acc[ii][jj].x = fmaf(xi[ii].x, xj.x, fmaf(xi[ii].y, xj.y, acc[ii][jj].x));
-                        acc[ii][jj].y = fmaf(xi[ii].y, xj.x, fmaf(-xi[ii].x, xj.y, acc[ii][jj].y));
-                    }
-                }
+                float2 xi[8], xj[8];
+                load8<TK * CG>(xi, xj, pi, pj, tk * CG);
+                tile_fma<TK, TK * CG, CG>(acc, xi, xj);
             }
         }
         __syncthreads();   // buffer (blk & 1) is refilled by the next issue
