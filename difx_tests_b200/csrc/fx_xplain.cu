@@ -132,10 +132,12 @@ __device__ __forceinline__ void diag_pair_stage(float2 (&acc)[2][36], const floa
 // re-cut as 28 off-diagonal tiles plus 4 threads that each take the upper triangles of two
 // diagonal blocks (b, 7 - b): 32 equal threads per channel, so 8 channels fill 8 warps and each
 // thread keeps the registers for the prefetched operands (a scheduler's register file is shared
-// by its warps; 9 warps would leave 168 per thread).
+// by its warps; 9 warps would leave 168 per thread).  With NB = 4 the same cut gives 6 + 2 = 8
+// equal threads per channel instead of 10 (4 of them half idle on diagonal tiles): 32 channels
+// fill 8 warps, again with the prefetch.
 template <int NB, int CG, int TK>
 struct XPlan {
-    static constexpr bool PAIRED = NB == 8;
+    static constexpr bool PAIRED = NB == 8 || NB == 4;
     static constexpr int NOFF = NB * (NB - 1) / 2;
     static constexpr int NTILE = PAIRED ? NOFF + NB / 2 : NB * (NB + 1) / 2;
     static constexpr int NTHREADS = CG * NTILE;

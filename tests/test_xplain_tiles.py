@@ -1,13 +1,13 @@
 """CPU check of the plain X stage's tile plan (difx_tests_b200/csrc/fx_xplain.cu), restated from
 the kernel's decode: every signal pair i <= j of a channel is accumulated by exactly one thread,
-and with 8 blocks of 8 signals the diagonal-pair threads fill whole warps (their branch is
-warp-uniform) and the CTA is 8 warps."""
+and with 8 (or 4) blocks of 8 signals the diagonal-pair threads fill whole warps (their branch
+is warp-uniform) and the CTA is 8 warps."""
 
 
 def decode(tile, nb):
     """(kind, I, J) of a thread's tile: 'tile' = the I x J block pair, 'pair' = the upper triangles of
     diagonal blocks I and J."""
-    paired = nb == 8
+    paired = nb in (4, 8)
     noff = nb * (nb - 1) // 2
     if paired and tile >= noff:
         i = tile - noff
@@ -21,7 +21,7 @@ def decode(tile, nb):
 
 
 def ntile(nb):
-    return nb * (nb - 1) // 2 + nb // 2 if nb == 8 else nb * (nb + 1) // 2
+    return nb * (nb - 1) // 2 + nb // 2 if nb in (4, 8) else nb * (nb + 1) // 2
 
 
 def test_every_pair_once():
@@ -47,3 +47,11 @@ def test_paired_plan_is_eight_whole_warps():
     assert len(kinds) == 256
     for w in range(8):
         assert len(set(kinds[32 * w: 32 * w + 32])) == 1
+
+
+def test_paired_plan_of_four_blocks_is_whole_warps():
+    for cg, nthreads in ((32, 256), (16, 128)):       # the two 32-signal plans
+        kinds = [decode(tid // cg, 4)[0] for tid in range(ntile(4) * cg)]
+        assert len(kinds) == nthreads
+        for w in range(nthreads // 32):
+            assert len(set(kinds[32 * w: 32 * w + 32])) == 1
