@@ -369,7 +369,7 @@ FORMS = {"plain": (0, 1),     # FXC_X_PLAIN_FP32, FXC_F_FFT32
          "tc": (1, 1),        # FXC_X_TC_FP16 on the FP32 FFT F stage
          "tc16f": (1, 2),     # FXC_X_TC_FP16 on the FP16 tensor-core F stage (FXC_F_TC16)
          "tc32f": (1, 3),     # FXC_X_TC_FP16 on the FP32-grade tensor-core F stage (FXC_F_TC32), the headline
-         "fp8": (2, 1)}       # FXC_X_TC_FP8 on the FP32 FFT F stage
+         "fp8": (2, 3)}       # FXC_X_TC_FP8 on the FP32-grade tensor-core F stage (FP32 FFT where not covered)
 XMODES = {k: v[0] for k, v in FORMS.items()}
 DTYPES = {"plain": "f32 (FFT F stage and X stage on the CUDA cores)",
           "tc": "f32 FFT F stage (CUDA cores), spectra cast to f16 for the tensor-core X stage, f32 accumulate",
@@ -377,8 +377,11 @@ DTYPES = {"plain": "f32 (FFT F stage and X stage on the CUDA cores)",
                    "f32 accumulate",
           "tc32f": "f32-grade tensor-core F stage (k_ftc32: f16 hi+lo operand pairs, three products per GEMM, "
                    "f32 accumulate), spectra cast to f16 for the tensor-core X stage, f32 accumulate",
-          "fp8": "f32 FFT F stage (CUDA cores), spectra cast to e4m3 scaled per signal and channel for the "
-                 "tensor-core X stage, f32 accumulate"}
+          "fp8": "f32-grade tensor-core F stage (k_ftc32), spectra cast to e4m3 scaled per signal and channel "
+                 "for the tensor-core X stage, f32 accumulate"}
+# the FP8 form where the tensor-core F stages do not apply
+DTYPE_FP8_FFT = ("f32 FFT F stage (CUDA cores), spectra cast to e4m3 scaled per signal and channel for the "
+                 "tensor-core X stage, f32 accumulate")
 F_KERNELS = {1: "k_fstage (fused unpack/shift/fringe/FFT/frac-delay, FP32 radix-16 FFT on the CUDA cores)",
              2: "k_ftc (tcgen05 F stage: unpack/fringe, 32x64 DFT as two FP16 tensor-core GEMMs, twiddles, "
                 "frac-delay, F16 store)",
@@ -386,12 +389,30 @@ F_KERNELS = {1: "k_fstage (fused unpack/shift/fringe/FFT/frac-delay, FP32 radix-
                 "three products each, twiddles, frac-delay)"}
 
 
+def tcf_geometry(w):
+    """The tensor-core F stages cover 1024 channels x 1 polarisation (2048-point real FFTs)."""
+    return w["nchan"] == 1024 and w["npol"] == 1
+
+
+def form_params(form, w):
+    """(xmode, fstage) of a form on workload w: a tensor-core F stage falls back to the FP32 FFT where
+    the geometry is not covered."""
+    xmode, fstage = FORMS[form]
+    if fstage in (2, 3) and not tcf_geometry(w):
+        fstage = 1
+    return xmode, fstage
+
+
+def form_dtype(form, w):
+    return DTYPE_FP8_FFT if form == "fp8" and not tcf_geometry(w) else DTYPES[form]
+
+
 def select_forms(xmode, w):
     """Forms to time, the headline first: all -> tc32f, tc, tc16f, fp8, plain; both -> tc32f, plain;
     a form name -> that form.  Geometries the tensor-core F stages do not cover (other than
     1024 channels x 1 polarisation) take the tc form in their place."""
     forms = {"all": ["tc32f", "tc", "tc16f", "fp8", "plain"], "both": ["tc32f", "plain"]}.get(xmode, [xmode])
-    if w["nchan"] != 1024 or w["npol"] != 1:
+    if not tcf_geometry(w):
         forms = list(dict.fromkeys("tc" if f in ("tc16f", "tc32f") else f for f in forms))
     return forms
 
@@ -400,7 +421,7 @@ def time_form(torch, dist, fx, w, form, data, pitch, delays, offs, steps, warmup
     """Warm up, then time `steps` subintegrations of one form; returns a result dict."""
     F = 2 * w["nchan"]
     nsig = w["nant"] * w["npol"]
-    xmode, fstage = FORMS[form]
+    xmode, fstage = form_params(form, w)
     cfg = fx.make_config(w["nant"], w["nchan"], w["numffts"], w["bw"], w["lo"], npol=w["npol"], nsubband=w["nsb"],
                          xmode=xmode, fstage=fstage)
     corr = fx.Correlator(cfg)
@@ -492,7 +513,7 @@ def run_gpu_arm(args):
             res[form]["corr"].close()
     forms = [f for f in forms if f in res]
     head = res[forms[0]]
-    xmode, fstage = FORMS[forms[0]]
+    xmode, fstage = form_params(forms[0], w)
 
     # ---- roofline of the dominant kernel of the headline form (the F stage)
     hbm, tc_peak, peak_kind = peaks()
@@ -517,7 +538,7 @@ def run_gpu_arm(args):
         "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": head["ms_max"] / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
-        "dtype": DTYPES[forms[0]],
+        "dtype": form_dtype(forms[0], w),
         "data": "synthetic (seeded, generated on device)",
         "config": {"workload": w["desc"], "form": forms[0], "parallelism": f"replicas x{world}",
                    "l2": "inputs (8.2 GB packed per step at cfg2) exceed L2; no flush",
@@ -532,7 +553,7 @@ def run_gpu_arm(args):
     }
     for form in forms[1:]:
         p = res[form]
-        line[form] = {"value": p["value"], "unit": UNIT, "ms_per_step": p["ms_max"] / args.steps, "dtype": DTYPES[form],
+        line[form] = {"value": p["value"], "unit": UNIT, "ms_per_step": p["ms_max"] / args.steps, "dtype": form_dtype(form, w),
                       "stages_ms_per_step": {"F": p["stage_ms"][1] / args.steps, "X": p["stage_ms"][2] / args.steps},
                       "x_tflops": p["x_tflops"], "clocks": p["clocks"], "gpu_launches": int(p["launches"].sum())}
     if "plain" in res and forms[0] != "plain":
@@ -581,7 +602,7 @@ def run_gpu_arm(args):
     for f, msg in failed.items():
         line[f] = {"error": msg}
     if rank == 0 and not args.no_accuracy:
-        line["accuracy"] = {f: accuracy_sample(w, *FORMS[f]) for f in forms}
+        line["accuracy"] = {f: accuracy_sample(w, *form_params(f, w)) for f in forms}
     if rank == 0 and world == 1 and not args.no_cpu:
         ref_geom_for(args.workload)
         cb = cpu_baseline_one_core()
@@ -647,7 +668,7 @@ def run_shard_arm(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
     w = WORKLOADS[args.workload]
     sform = args.xmode if args.xmode in FORMS else ("tc32f" if w["nchan"] == 1024 and w["npol"] == 1 else "tc")
-    xmode, fstage = FORMS[sform]
+    xmode, fstage = form_params(sform, w)
     cfg = fx.make_config(w["nant"], w["nchan"], w["numffts"], w["bw"], w["lo"], npol=w["npol"], nsubband=w["nsb"],
                          xmode=xmode, fstage=fstage)
     subint = fx.lib().fxc_subint_bytes(cfg)
@@ -687,7 +708,7 @@ def run_shard_arm(args):
         print(json.dumps({
             "metric": METRIC, "value": samples / (ms / 1e3) / 1e9, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-            "scaling": "strong", "vs_baseline": None, "dtype": DTYPES[sform],
+            "scaling": "strong", "vs_baseline": None, "dtype": form_dtype(sform, w),
             "data": "synthetic (seeded, generated on device)",
             "config": {"workload": w["desc"], "parallelism": f"{args.shard} shards x{world}",
                        "merge": "all-reduce of visibilities and counts" if args.shard == "time" else "all-gather",

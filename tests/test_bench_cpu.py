@@ -35,3 +35,10 @@ def test_forms_headline_first_and_geometry_fallback():
     assert bench.select_forms("plain", w1) == ["plain"]
     for f, (xmode, fstage) in bench.FORMS.items():
         assert f in bench.DTYPES and fstage in bench.F_KERNELS
+
+
+def test_form_parameters_fall_back_where_the_tensor_core_f_stages_do_not_apply():
+    w2, w1 = bench.WORKLOADS["cfg2"], bench.WORKLOADS["cfg1"]
+    assert bench.form_params("tc32f", w2) == (1, 3) and bench.form_params("fp8", w2) == (2, 3)
+    assert bench.form_params("fp8", w1) == (2, 1) and bench.form_params("tc", w1) == (1, 1)
+    assert "k_ftc32" in bench.form_dtype("fp8", w2) and "FFT" in bench.form_dtype("fp8", w1)
