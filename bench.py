@@ -369,7 +369,7 @@ FORMS = {"plain": (0, 1),     # FXC_X_PLAIN_FP32, FXC_F_FFT32
          "tc": (1, 1),        # FXC_X_TC_FP16 on the FP32 FFT F stage
          "tc16f": (1, 2),     # FXC_X_TC_FP16 on the FP16 tensor-core F stage (FXC_F_TC16)
          "tc32f": (1, 3),     # FXC_X_TC_FP16 on the FP32-grade tensor-core F stage (FXC_F_TC32), the headline
-         "fp8": (2, 3)}       # FXC_X_TC_FP8 on the FP32-grade tensor-core F stage (FP32 FFT where not covered)
+         "fp8": (2, 1)}       # FXC_X_TC_FP8 on the FP32 FFT F stage
 XMODES = {k: v[0] for k, v in FORMS.items()}
 DTYPES = {"plain": "f32 (FFT F stage and X stage on the CUDA cores)",
           "tc": "f32 FFT F stage (CUDA cores), spectra cast to f16 for the tensor-core X stage, f32 accumulate",
@@ -377,11 +377,8 @@ DTYPES = {"plain": "f32 (FFT F stage and X stage on the CUDA cores)",
                    "f32 accumulate",
           "tc32f": "f32-grade tensor-core F stage (k_ftc32: f16 hi+lo operand pairs, three products per GEMM, "
                    "f32 accumulate), spectra cast to f16 for the tensor-core X stage, f32 accumulate",
-          "fp8": "f32-grade tensor-core F stage (k_ftc32), spectra cast to e4m3 scaled per signal and channel "
-                 "for the tensor-core X stage, f32 accumulate"}
-# the FP8 form where the tensor-core F stages do not apply
-DTYPE_FP8_FFT = ("f32 FFT F stage (CUDA cores), spectra cast to e4m3 scaled per signal and channel for the "
-                 "tensor-core X stage, f32 accumulate")
+          "fp8": "f32 FFT F stage (CUDA cores), spectra cast to e4m3 scaled per signal and channel for the "
+                 "tensor-core X stage, f32 accumulate"}
 F_KERNELS = {1: "k_fstage (fused unpack/shift/fringe/FFT/frac-delay, FP32 radix-16 FFT on the CUDA cores)",
              2: "k_ftc (tcgen05 F stage: unpack/fringe, 32x64 DFT as two FP16 tensor-core GEMMs, twiddles, "
                 "frac-delay, F16 store)",
@@ -404,7 +401,8 @@ def form_params(form, w):
 
 
 def form_dtype(form, w):
-    return DTYPE_FP8_FFT if form == "fp8" and not tcf_geometry(w) else DTYPES[form]
+    return DTYPES[form if form_params(form, w)[1] == FORMS[form][1] else "tc"] if form in ("tc16f", "tc32f") \
+        else DTYPES[form]
 
 
 def select_forms(xmode, w):

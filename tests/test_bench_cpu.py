@@ -39,6 +39,6 @@ def test_forms_headline_first_and_geometry_fallback():
 
 def test_form_parameters_fall_back_where_the_tensor_core_f_stages_do_not_apply():
     w2, w1 = bench.WORKLOADS["cfg2"], bench.WORKLOADS["cfg1"]
-    assert bench.form_params("tc32f", w2) == (1, 3) and bench.form_params("fp8", w2) == (2, 3)
-    assert bench.form_params("fp8", w1) == (2, 1) and bench.form_params("tc", w1) == (1, 1)
-    assert "k_ftc32" in bench.form_dtype("fp8", w2) and "FFT" in bench.form_dtype("fp8", w1)
+    assert bench.form_params("tc32f", w2) == (1, 3) and bench.form_params("tc16f", w2) == (1, 2)
+    assert bench.form_params("tc32f", w1) == (1, 1) and bench.form_params("fp8", w1) == (2, 1)
+    assert "k_ftc32" in bench.form_dtype("tc32f", w2) and "FFT" in bench.form_dtype("tc32f", w1)
