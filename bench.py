@@ -401,8 +401,8 @@ def form_params(form, w):
 
 
 def form_dtype(form, w):
-    return DTYPES[form if form_params(form, w)[1] == FORMS[form][1] else "tc"] if form in ("tc16f", "tc32f") \
-        else DTYPES[form]
+    """dtype label of the form as it runs on w (a tensor-core F form that fell back reads as tc)."""
+    return DTYPES[form] if form_params(form, w) == FORMS[form] else DTYPES["tc"]
 
 
 def select_forms(xmode, w):
