@@ -218,6 +218,7 @@ static void free_ctx(fxc_ctx* x)
     cudaFree(x->d_amax);
     cudaFree(x->d_inv);
     cudaFree(x->d_acc);
+    cudaFree(x->d_xpart);
     cudaFree(x->d_counts);
     cudaFree(x->d_err);
     cudaFree(x->d_vis);
@@ -343,6 +344,15 @@ int ctx_create(const fxc_config* cfg, fxc_ctx** out, bool group_subbands)
         if ((e = cudaMalloc(&x->d_inv, nsc * sizeof(float))) != cudaSuccess) return fail(e);
     }
     if ((e = cudaMalloc(&x->d_acc, x->acc_bytes)) != cudaSuccess) return fail(e);
+    if (c.xmode == FXC_X_PLAIN_FP32) {
+        // segment partials of the plain X stage when its channel groups underfill the SMs
+        int tl = 0;
+        xplain_segments(x->nsig, c.nchan, c.nsubband, x->T, x->nsm, &x->xseg_max, &tl);
+        if (x->xseg_max > 1 &&
+            (e = cudaMalloc(&x->d_xpart, (size_t)x->xseg_max * x->nsb_g * x->npair * c.nchan * sizeof(float2))) !=
+                cudaSuccess)
+            return fail(e);
+    }
     if ((e = cudaMalloc(&x->d_counts, sizeof(int) * x->npair_ant)) != cudaSuccess) return fail(e);
     // d_err[0]: tensor-core X wait-expiry code; d_err[1]: input-window misses
     if ((e = cudaMalloc(&x->d_err, 2 * sizeof(int))) != cudaSuccess) return fail(e);
@@ -537,6 +547,17 @@ extern "C" {
 
 }  // extern "C"
 
+// The plain X stage's time segments of this context and tile variant (fx_xplain.cu)
+void ctx_xsegments(const fxc_ctx* x, XArgs& xa)
+{
+    xa.tseg = 1;
+    xa.tlen = x->T;
+    xa.part = nullptr;
+    if (!x->d_xpart || xa.nsig > 64) return;
+    xplain_segments(xa.nsig, x->cfg.nchan, x->cfg.nsubband, x->T, x->nsm, &xa.tseg, &xa.tlen);
+    xa.part = xa.tseg > 1 ? x->d_xpart : nullptr;
+}
+
 // One call's correlation of device rows: whole subintegrations (win_base null) or windows.
 static int ctx_correlate(fxc_ctx* x, const uint8_t* d_data, size_t pitch, const double* d_meta,
                          const double* delays, const double* offs, int first, int nfft)
@@ -561,6 +582,7 @@ static int ctx_correlate(fxc_ctx* x, const uint8_t* d_data, size_t pitch, const 
     xa.nsb = x->cfg.nsubband;
     xa.rows = x->rows;
     xa.alt = x->plan_alt;
+    ctx_xsegments(x, xa);
     const int nsb = x->cfg.nsubband, G = x->nsb_g;
     const FArgs fall = fa;
     const XArgs xall = xa;
@@ -930,6 +952,7 @@ int fxc_autotune(fxc_ctx* x, int reps)
         best = 1e30f;
         for (int alt : {0, 1}) {
             xa.alt = alt;
+            ctx_xsegments(x, xa);
             float ms = 0.f;
             err = timeit([&] { return launch_xplain(xa, x->stream); }, &ms);
             if (err != cudaSuccess) break;

@@ -5,7 +5,8 @@
 // Each job owns an ordinary context (device input, delay table, spectra chunk,
 // accumulators).  Per round r (spectra chunk r of every job that has one):
 //   one k_fstage_batch launch per F group  {FFT length, npol, spectra precision, FFTs per CTA}
-//   one k_xplain_batch launch per X group  {8-signal blocks, tile variant} (plain form, <= 64 signals)
+//   one k_xplain_batch launch per X group  {8-signal blocks, tile variant} (plain form, <= 64 signals),
+//   then one k_xplain_reduce per job of the group cut into time segments (as its single-job path cuts it)
 //   one X launch per remaining job: the FP16 tensor-core X stage, or the plain X stage of
 //   more than 64 signals
 // A grouped launch works through a task table (F: persistent CTAs striding over it; plain X:
@@ -37,7 +38,7 @@ struct XGroup {
     int nsig8, alt;   // signal blocks of 8 (jobs with the same count share tile plans)
     std::vector<int> jobs;
 };
-enum LaunchKind { kFGroup = 0, kXGroup = 1, kXJob = 2 };
+enum LaunchKind { kFGroup = 0, kXGroup = 1, kXJob = 2, kXReduce = 3 };
 struct Launch {       // one launch of the recorded sequence
     int kind;         // LaunchKind
     int group;        // F / X group, or the job of a kXJob launch
@@ -125,6 +126,7 @@ static int build_tables(fxc_batch* b)
         x.nsb = c->cfg.nsubband;
         x.rows = c->rows;
         x.alt = b->job_xg[j] >= 0 ? b->xg[b->job_xg[j]].alt : c->plan_alt;
+        if (c->cfg.xmode == FXC_X_PLAIN_FP32) ctx_xsegments(c, x);   // the single-job path's cut
         xa[j] = x;
     }
     b->xa_host = xa;
@@ -146,13 +148,18 @@ static int build_tables(fxc_batch* b)
         for (int g = 0; g < (int)b->xg.size(); g++) {
             const size_t off = tasks.size();
             const int cg = xplain_channel_group(b->xg[g].nsig8 * 8, b->xg[g].alt);
+            std::vector<int> segd;   // jobs of the group cut into time segments: a reduce each after it
             for (int j : b->xg[g].jobs) {
                 const fxc_ctx* c = b->ctx[j];
                 if (r >= nchunks(c)) continue;
+                const int nseg = xa[j].tseg > 1 ? xa[j].tseg : 1;
                 for (int sb = 0; sb < c->cfg.nsubband; sb++)
-                    for (int c0 = 0; c0 < c->cfg.nchan; c0 += cg) tasks.push_back(make_int4(j, sb, c0, 0));
+                    for (int c0 = 0; c0 < c->cfg.nchan; c0 += cg)
+                        for (int s = 0; s < nseg; s++) tasks.push_back(make_int4(j, sb, c0, s));
+                if (nseg > 1) segd.push_back(j);
             }
             if (tasks.size() > off) b->launches.push_back({kXGroup, g, off, (int)(tasks.size() - off)});
+            for (int j : segd) b->launches.push_back({kXReduce, j, 0, 0});
         }
         for (int j = 0; j < J; j++)
             if (b->job_xg[j] < 0 && r < nchunks(b->ctx[j])) b->launches.push_back({kXJob, j, 0, 0});
@@ -186,6 +193,8 @@ static int enqueue_launch(fxc_batch* b, const Launch& l)
     } else if (l.kind == kXGroup) {
         const XGroup& g = b->xg[l.group];
         FB_CK(launch_xplain_batch(g.nsig8 * 8, g.alt, b->d_xargs, b->d_tasks + l.task_off, l.ntask, b->stream));
+    } else if (l.kind == kXReduce) {
+        FB_CK(launch_xplain_reduce(b->xa_host[l.group], b->stream));
     } else {
         fxc_ctx* c = b->ctx[l.group];
         const XArgs& x = b->xa_host[l.group];

@@ -38,6 +38,8 @@ struct fxc_ctx {
     float* d_inv = nullptr;       // FP8 form: [nsb*nchan][nsig] inverse scales
     float2* d_acc = nullptr;
     size_t acc_bytes = 0;
+    void* d_xpart = nullptr;      // plain form with few channel groups: X-stage segment partial sums
+    int xseg_max = 1;             // segments it holds
     int* d_counts = nullptr;
     int* d_err = nullptr;   // device-side wait expiry code of the tensor-core X stage
     int nsm = 148;
@@ -95,3 +97,5 @@ int ctx_run_delay_table(fxc_ctx* x, const double* delays, const double* offs, in
                         const double* d_meta = nullptr);
 // F-stage arguments of this context for device input rows d_data of `pitch` bytes
 fx::FArgs ctx_fargs(fxc_ctx* x, const uint8_t* d_data, size_t pitch, int ld);
+// the plain X stage's time segments for xa (its nsig and alt set): tseg, tlen, part
+void ctx_xsegments(const fxc_ctx* x, fx::XArgs& xa);

@@ -75,6 +75,11 @@ struct XArgs {
     int alt;     // plain-form tile variant: 0 = default, 1 = alternative (chosen by the plan / autotuner)
     const float* inv_scale;   // FP8 form: [nsb*nchan][nsig] factors applied to each Gram product
     int ntk;                  // slots [0, ntk) of each spectra row consumed (0 = T; multiple of 64 / 128 for FP8)
+    // plain form with few channel groups: the slots are cut into tseg segments of tlen FFTs (a
+    // multiple of 16), each CTA sums one segment into part [tseg][nsb][pair][chan], and a reduce
+    // adds the segments to acc in order (tseg <= 1: no segments, CTAs add to acc directly)
+    int tseg, tlen;
+    void* part;
 };
 
 }  // namespace fx

@@ -12,6 +12,11 @@
 // read from HBM/L2 once.  Time blocks of TK samples are double-buffered in
 // shared memory with cp.async; lanes of a warp are (CG channels) x (32/CG
 // tiles), so the operand loads are broadcasts or conflict-free.
+//
+// Small jobs (few channels, few signals) give fewer CTAs than SMs; there the
+// time axis is cut too: CTA (c, sb, seg) sums FFT slots of segment seg into
+// its own partials, and k_xplain_reduce adds the segments to acc in segment
+// order, so the result does not depend on which CTA ran first.
 #include "fx_common.cuh"
 #include "fx_kernels.h"
 
@@ -156,7 +161,7 @@ __device__ __forceinline__ int xoff(int s, int tk, int cl)
 // Stages of one X-stage block for one thread: tiles (DP false) or diagonal pairs (DP true).
 template <int NB, int CG, int TK, bool DP>
 __device__ __forceinline__ void xplain_stages(const XArgs& a, int sb, int c0, float2* xs, int tid, int cl, int I,
-                                              int J)
+                                              int J, int seg)
 {
     using P = XPlan<NB, CG, TK>;
     const int nsig = a.nsig;
@@ -194,11 +199,16 @@ __device__ __forceinline__ void xplain_stages(const XArgs& a, int sb, int c0, fl
 #pragma unroll
         for (int i = 0; i < 36; i++) dacc[h][i] = make_float2(0.f, 0.f);
 
-    const int nblk = (a.ntk ? a.ntk : a.T) / TK;
-    issue(0, 0);
+    // FFT slots [t_lo, t_hi): all of them, or segment seg of tlen slots (an empty segment adds zeros)
+    const int nslot = a.ntk ? a.ntk : a.T;
+    const bool segd = a.tseg > 1;
+    const int t_lo = segd ? min(seg * a.tlen, nslot) : 0;
+    const int t_hi = segd ? min(t_lo + a.tlen, nslot) : nslot;
+    const int nblk = (t_hi - t_lo) / TK;
+    if (nblk > 0) issue(0, t_lo);
     for (int blk = 0; blk < nblk; blk++) {
         if (blk + 1 < nblk) {
-            issue((blk + 1) & 1, (blk + 1) * TK);
+            issue((blk + 1) & 1, t_lo + (blk + 1) * TK);
             cp_async_wait<1>();
         } else {
             cp_async_wait<0>();
@@ -226,6 +236,8 @@ __device__ __forceinline__ void xplain_stages(const XArgs& a, int sb, int c0, fl
 
     float2* out = reinterpret_cast<float2*>(a.acc);
     const int npair = nsig * (nsig + 1) / 2;
+    // this segment's partial sums: [seg][sb][pair][chan], the layout of acc per segment
+    float2* part = segd ? reinterpret_cast<float2*>(a.part) + (size_t)seg * a.nsb * npair * C : nullptr;
     if constexpr (DP) {
 #pragma unroll
         for (int h = 0; h < 2; h++) {
@@ -237,11 +249,16 @@ __device__ __forceinline__ void xplain_stages(const XArgs& a, int sb, int c0, fl
                     const int i = B * 8 + ii, j = B * 8 + jj;
                     if (j < nsig) {
                         const int p = i * nsig - (i * (i - 1)) / 2 + (j - i);
-                        float2* o = out + ((size_t)sb * npair + p) * C + c0 + cl;
-                        float2 cur = *o;
-                        cur.x += dacc[h][jj * (jj + 1) / 2 + ii].x;
-                        cur.y += dacc[h][jj * (jj + 1) / 2 + ii].y;
-                        *o = cur;
+                        const size_t e = ((size_t)sb * npair + p) * C + c0 + cl;
+                        const float2 v = dacc[h][jj * (jj + 1) / 2 + ii];
+                        if (segd) {
+                            part[e] = v;
+                        } else {
+                            float2 cur = out[e];
+                            cur.x += v.x;
+                            cur.y += v.y;
+                            out[e] = cur;
+                        }
                     }
                 }
         }
@@ -254,11 +271,15 @@ __device__ __forceinline__ void xplain_stages(const XArgs& a, int sb, int c0, fl
                 const int j = J * 8 + jj;
                 if (i <= j && j < nsig) {
                     const int p = i * nsig - (i * (i - 1)) / 2 + (j - i);
-                    float2* o = out + ((size_t)sb * npair + p) * C + c0 + cl;
-                    float2 cur = *o;
-                    cur.x += acc[ii][jj].x;
-                    cur.y += acc[ii][jj].y;
-                    *o = cur;
+                    const size_t e = ((size_t)sb * npair + p) * C + c0 + cl;
+                    if (segd) {
+                        part[e] = acc[ii][jj];
+                    } else {
+                        float2 cur = out[e];
+                        cur.x += acc[ii][jj].x;
+                        cur.y += acc[ii][jj].y;
+                        out[e] = cur;
+                    }
                 }
             }
         }
@@ -267,7 +288,7 @@ __device__ __forceinline__ void xplain_stages(const XArgs& a, int sb, int c0, fl
 
 // One X-stage block: channels [c0, c0 + CG) of subband sb over all T FFT slots.
 template <int NB, int CG, int TK>
-__device__ __forceinline__ void xplain_block(const XArgs& a, int sb, int c0, unsigned char* smem)
+__device__ __forceinline__ void xplain_block(const XArgs& a, int sb, int c0, int seg, unsigned char* smem)
 {
     using P = XPlan<NB, CG, TK>;
     float2* xs = reinterpret_cast<float2*>(smem);   // [2][STAGE]
@@ -294,9 +315,9 @@ __device__ __forceinline__ void xplain_block(const XArgs& a, int sb, int c0, uns
 
     // the two thread kinds in separate instantiations, so each keeps only its own accumulators
     if (dpair)
-        xplain_stages<NB, CG, TK, true>(a, sb, c0, xs, tid, cl, I, J);
+        xplain_stages<NB, CG, TK, true>(a, sb, c0, xs, tid, cl, I, J, seg);
     else
-        xplain_stages<NB, CG, TK, false>(a, sb, c0, xs, tid, cl, I, J);
+        xplain_stages<NB, CG, TK, false>(a, sb, c0, xs, tid, cl, I, J, seg);
 }
 
 template <int NB, int CG, int TK>
@@ -304,7 +325,7 @@ __global__ void __launch_bounds__(XPlan<NB, CG, TK>::NTHREADS, 1)
 k_xplain(XArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    xplain_block<NB, CG, TK>(a, blockIdx.y, blockIdx.x * CG, smem);
+    xplain_block<NB, CG, TK>(a, blockIdx.y, blockIdx.x * CG, blockIdx.z, smem);
 }
 
 // Many jobs with the same tile plan in one launch: CTA i takes task i {job, subband, first
@@ -318,7 +339,7 @@ k_xplain_batch(const XArgs* __restrict__ jobs, const int4* __restrict__ tasks, i
     if (blockIdx.x < ntask) {
         const int4 tk = tasks[blockIdx.x];
         const XArgs& a = jobs[tk.x];   // read where used (global, cached)
-        xplain_block<NB, CG, TK>(a, tk.y, tk.z, smem);
+        xplain_block<NB, CG, TK>(a, tk.y, tk.z, tk.w, smem);
     }
 }
 
@@ -332,9 +353,12 @@ static cudaError_t launch_x(const XArgs& a, cudaStream_t st)
     static unsigned configured = 0;  // per instantiation and device
     cudaError_t e = set_smem_once(kern, sm, &configured);
     if (e != cudaSuccess) return e;
-    dim3 grid(a.nchan / CG, a.nsb);
+    const int tseg = a.tseg > 1 ? a.tseg : 1;
+    if (tseg > 1 && !a.part) return cudaErrorInvalidValue;
+    dim3 grid(a.nchan / CG, a.nsb, tseg);
     kern<<<grid, P::NTHREADS, sm, st>>>(a);
-    return cudaGetLastError();
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    return tseg > 1 ? launch_xplain_reduce(a, st) : cudaSuccess;
 }
 
 template <int NB, int CG, int TK>
@@ -490,6 +514,53 @@ static cudaError_t launch_xbig(const XArgs& a, cudaStream_t st)
     case 16: OP(8, 8, 16); case 17: OP(8, 8, 8);                                \
     default: return cudaErrorNotSupported;                                      \
     }
+
+// acc[e] += (part[0][e] + part[1][e] + ... + part[tseg - 1][e]), summed in segment order
+__global__ void k_xplain_reduce(float2* __restrict__ acc, const float2* __restrict__ part, int tseg, long long n)
+{
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        float2 s = part[e];
+        for (int t = 1; t < tseg; t++) {
+            const float2 v = part[t * n + e];
+            s.x += v.x;
+            s.y += v.y;
+        }
+        float2 cur = acc[e];
+        cur.x += s.x;
+        cur.y += s.y;
+        acc[e] = cur;
+    }
+}
+
+cudaError_t launch_xplain_reduce(const XArgs& a, cudaStream_t st)
+{
+    if (a.tseg <= 1) return cudaSuccess;
+    const long long n = (long long)a.nsb * (a.nsig * (a.nsig + 1) / 2) * a.nchan;
+    const long long blocks = (n + 255) / 256;
+    k_xplain_reduce<<<(int)(blocks < 1184 ? blocks : 1184), 256, 0, st>>>(
+        reinterpret_cast<float2*>(a.acc), reinterpret_cast<const float2*>(a.part), a.tseg, n);
+    return cudaGetLastError();
+}
+
+// Time segments of the plain X stage (up to 64 signals): while the channel groups alone (of the
+// default tile variant) give fewer CTAs than SMs, the T FFT slots are cut into up to 32 segments
+// of at least 64 FFTs (tlen a multiple of 16), at most two CTAs per SM in all.  A function of the
+// job's geometry only (not of the tile variant), so a batch and the single-job path cut a job the
+// same way and sum it in the same order, tuned or not.
+void xplain_segments(int nsig, int nchan, int nsb, int T, int nsm, int* tseg, int* tlen)
+{
+    *tseg = 1;
+    *tlen = T;
+    if (nsig > 64 || nsig < 1) return;
+    const int ctas = nchan / xplain_channel_group(nsig, 0) * nsb;
+    if (ctas >= nsm) return;
+    int s = 1;
+    while (s < 32 && ctas * 2 * s <= 2 * nsm && T / (2 * s) >= 64) s *= 2;
+    if (s == 1) return;
+    const int len = ((T + s - 1) / s + 15) / 16 * 16;
+    *tlen = len;
+    *tseg = (T + len - 1) / len;
+}
 
 int xplain_channel_group(int nsig, int alt)
 {

@@ -371,6 +371,26 @@ def test_plain_multiblock_vs_fp64_oracle(nant, npol, nchan, numffts, nsb):
         assert_vis_close(vis[sb], ref)
 
 
+@pytest.mark.parametrize("nant,npol,nchan,numffts,nsb,chunk,calls",
+                         [(4, 1, 256, 1000, 1, 0, [(0, 1000)]),
+                          (6, 2, 128, 700, 2, 512, [(0, 300), (300, 400)]),
+                          (8, 1, 512, 640, 1, 256, [(0, 129), (129, 511)])])
+def test_plain_time_segments_vs_fp64_oracle(nant, npol, nchan, numffts, nsb, chunk, calls):
+    """Few channel groups: the plain X stage cuts the FFT slots into time segments, sums each
+    segment into its own partials and reduces them into the accumulator (chunks that fill only
+    some segments, calls that split a chunk)."""
+    job = synth.make_job(nant=nant, npol=npol, nchan=nchan, numffts=numffts, bw=64e6, lo=1.4e9, rho=0.1,
+                         seed=nant + nchan + numffts, nsubband=nsb)
+    with corr_for(job, chunk_ffts=chunk) as c:
+        for first, n in calls:
+            c.process(job.data, job.delays, job.fileoffsets, first, n)
+        vis, counts = c.visibilities()
+    for sb in range(nsb):
+        ref, rc = oracle_vis(job, sb)
+        np.testing.assert_array_equal(counts, rc)
+        assert_vis_close(vis[sb], ref)
+
+
 def test_tc_matches_plain_multiblock():
     job = synth.make_job(nant=70, npol=2, nchan=256, numffts=256, bw=64e6, lo=1.4e9, rho=0.1, seed=71)
     out = {}
