@@ -41,9 +41,10 @@ struct XGroup {
 enum LaunchKind { kFGroup = 0, kXGroup = 1, kXJob = 2, kXReduce = 3 };
 struct Launch {       // one launch of the recorded sequence
     int kind;         // LaunchKind
-    int group;        // F / X group, or the job of a kXJob launch
+    int group;        // F / X group, or the job of a kXJob / kXReduce launch
     size_t task_off;  // into d_tasks (int4)
     int ntask;
+    int round;        // kXJob / kXReduce: the round (spectra chunk) whose X arguments it takes
 };
 
 thread_local int g_batch_cuda = 0;
@@ -73,9 +74,9 @@ struct fxc_batch {
     std::vector<FGroup> fg;
     std::vector<XGroup> xg;
     std::vector<int> job_fg, job_xg;   // job_xg -1: the job's X stage is its own launch
-    std::vector<XArgs> xa_host;        // per job, for its own X launch
+    std::vector<XArgs> xa_host;        // [nrounds][J], for the launches of one job
     int nrounds = 0;
-    // device tables: FArgs [nrounds][J], XArgs [J], tasks (int4) for every recorded launch
+    // device tables: FArgs [nrounds][J], XArgs [nrounds][J], tasks (int4) for every recorded launch
     FArgs* d_fargs = nullptr;
     XArgs* d_xargs = nullptr;
     int4* d_tasks = nullptr;
@@ -99,6 +100,14 @@ static void drop_graph(fxc_batch* b)
 
 static int nchunks(const fxc_ctx* c) { return (c->cfg.numffts + c->T - 1) / c->T; }
 
+// Slots chunk r of a job uses: its FFTs rounded up to the X stage's depth, as the single-job path
+// rounds them (the F stage writes zeros after the last FFT, the X stage reads no further)
+static int chunk_span(const fxc_ctx* c, int r)
+{
+    const int nfft = std::min(c->T, c->cfg.numffts - r * c->T);
+    return std::min(c->T, (nfft + 63) / 64 * 64);
+}
+
 // Builds the F/X argument tables and the task list of every launch.
 static int build_tables(fxc_batch* b)
 {
@@ -107,13 +116,14 @@ static int build_tables(fxc_batch* b)
     b->nrounds = 0;
     for (auto* c : b->ctx) b->nrounds = std::max(b->nrounds, nchunks(c));
     std::vector<FArgs> fa((size_t)b->nrounds * J);
-    std::vector<XArgs> xa(J);
+    std::vector<XArgs> xa((size_t)b->nrounds * J);
     for (int j = 0; j < J; j++) {
         fxc_ctx* c = b->ctx[j];
         for (int r = 0; r < nchunks(c); r++) {
             FArgs a = ctx_fargs(c, c->d_in, c->pitch, c->ld);
             a.t_base = r * c->T;
             a.nfft = std::min(c->T, c->cfg.numffts - r * c->T);
+            a.tspan = chunk_span(c, r);
             a.tb = b->fg[b->job_fg[j]].tb;
             fa[(size_t)r * J + j] = a;
         }
@@ -127,7 +137,10 @@ static int build_tables(fxc_batch* b)
         x.rows = c->rows;
         x.alt = b->job_xg[j] >= 0 ? b->xg[b->job_xg[j]].alt : c->plan_alt;
         if (c->cfg.xmode == FXC_X_PLAIN_FP32) ctx_xsegments(c, x);   // the single-job path's cut
-        xa[j] = x;
+        for (int r = 0; r < nchunks(c); r++) {
+            xa[(size_t)r * J + j] = x;
+            xa[(size_t)r * J + j].ntk = chunk_span(c, r);
+        }
     }
     b->xa_host = xa;
     std::vector<int4> tasks;
@@ -141,9 +154,10 @@ static int build_tables(fxc_batch* b)
                 if (r >= nchunks(c)) continue;
                 for (int sb = 0; sb < c->cfg.nsubband; sb++)
                     for (int ant = 0; ant < c->cfg.nant; ant++)
-                        for (int t0 = 0; t0 < c->T; t0 += tb) tasks.push_back(make_int4(r * J + j, sb, ant, t0));
+                        for (int t0 = 0; t0 < chunk_span(c, r); t0 += tb)
+                            tasks.push_back(make_int4(r * J + j, sb, ant, t0));
             }
-            if (tasks.size() > off) b->launches.push_back({kFGroup, g, off, (int)(tasks.size() - off)});
+            if (tasks.size() > off) b->launches.push_back({kFGroup, g, off, (int)(tasks.size() - off), r});
         }
         for (int g = 0; g < (int)b->xg.size(); g++) {
             const size_t off = tasks.size();
@@ -152,17 +166,18 @@ static int build_tables(fxc_batch* b)
             for (int j : b->xg[g].jobs) {
                 const fxc_ctx* c = b->ctx[j];
                 if (r >= nchunks(c)) continue;
-                const int nseg = xa[j].tseg > 1 ? xa[j].tseg : 1;
+                const XArgs& xj = xa[(size_t)r * J + j];
+                const int nseg = xplain_segments_used(xj);
                 for (int sb = 0; sb < c->cfg.nsubband; sb++)
                     for (int c0 = 0; c0 < c->cfg.nchan; c0 += cg)
-                        for (int s = 0; s < nseg; s++) tasks.push_back(make_int4(j, sb, c0, s));
+                        for (int s = 0; s < nseg; s++) tasks.push_back(make_int4(r * J + j, sb, c0, s));
                 if (nseg > 1) segd.push_back(j);
             }
-            if (tasks.size() > off) b->launches.push_back({kXGroup, g, off, (int)(tasks.size() - off)});
-            for (int j : segd) b->launches.push_back({kXReduce, j, 0, 0});
+            if (tasks.size() > off) b->launches.push_back({kXGroup, g, off, (int)(tasks.size() - off), r});
+            for (int j : segd) b->launches.push_back({kXReduce, j, 0, 0, r});
         }
         for (int j = 0; j < J; j++)
-            if (b->job_xg[j] < 0 && r < nchunks(b->ctx[j])) b->launches.push_back({kXJob, j, 0, 0});
+            if (b->job_xg[j] < 0 && r < nchunks(b->ctx[j])) b->launches.push_back({kXJob, j, 0, 0, r});
     }
     FB_CK(cudaSetDevice(b->device));
     cudaFree(b->d_fargs);
@@ -194,10 +209,10 @@ static int enqueue_launch(fxc_batch* b, const Launch& l)
         const XGroup& g = b->xg[l.group];
         FB_CK(launch_xplain_batch(g.nsig8 * 8, g.alt, b->d_xargs, b->d_tasks + l.task_off, l.ntask, b->stream));
     } else if (l.kind == kXReduce) {
-        FB_CK(launch_xplain_reduce(b->xa_host[l.group], b->stream));
+        FB_CK(launch_xplain_reduce(b->xa_host[(size_t)l.round * b->ctx.size() + l.group], b->stream));
     } else {
         fxc_ctx* c = b->ctx[l.group];
-        const XArgs& x = b->xa_host[l.group];
+        const XArgs& x = b->xa_host[(size_t)l.round * b->ctx.size() + l.group];
         FB_CK(c->cfg.xmode == FXC_X_TC_FP16 ? launch_xtc(x, c->d_err, c->nsm, b->stream) : launch_xplain(x, b->stream));
     }
     return FXC_OK;

@@ -353,12 +353,12 @@ static cudaError_t launch_x(const XArgs& a, cudaStream_t st)
     static unsigned configured = 0;  // per instantiation and device
     cudaError_t e = set_smem_once(kern, sm, &configured);
     if (e != cudaSuccess) return e;
-    const int tseg = a.tseg > 1 ? a.tseg : 1;
-    if (tseg > 1 && !a.part) return cudaErrorInvalidValue;
+    const int tseg = xplain_segments_used(a);
+    if (a.tseg > 1 && !a.part) return cudaErrorInvalidValue;
     dim3 grid(a.nchan / CG, a.nsb, tseg);
     kern<<<grid, P::NTHREADS, sm, st>>>(a);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    return tseg > 1 ? launch_xplain_reduce(a, st) : cudaSuccess;
+    return a.tseg > 1 ? launch_xplain_reduce(a, st) : cudaSuccess;
 }
 
 template <int NB, int CG, int TK>
@@ -532,13 +532,21 @@ __global__ void k_xplain_reduce(float2* __restrict__ acc, const float2* __restri
     }
 }
 
+// Segments a launch computes: those holding slots below ntk (later ones would only add zeros)
+int xplain_segments_used(const XArgs& a)
+{
+    if (a.tseg <= 1) return 1;
+    const int nslot = a.ntk ? a.ntk : a.T;
+    return std::max(1, std::min(a.tseg, (nslot + a.tlen - 1) / a.tlen));
+}
+
 cudaError_t launch_xplain_reduce(const XArgs& a, cudaStream_t st)
 {
     if (a.tseg <= 1) return cudaSuccess;
     const long long n = (long long)a.nsb * (a.nsig * (a.nsig + 1) / 2) * a.nchan;
     const long long blocks = (n + 255) / 256;
     k_xplain_reduce<<<(int)(blocks < 1184 ? blocks : 1184), 256, 0, st>>>(
-        reinterpret_cast<float2*>(a.acc), reinterpret_cast<const float2*>(a.part), a.tseg, n);
+        reinterpret_cast<float2*>(a.acc), reinterpret_cast<const float2*>(a.part), xplain_segments_used(a), n);
     return cudaGetLastError();
 }
 
