@@ -550,24 +550,64 @@ cudaError_t launch_xplain_reduce(const XArgs& a, cudaStream_t st)
     return cudaGetLastError();
 }
 
-// Time segments of the plain X stage (up to 64 signals): while the channel groups alone (of the
-// default tile variant) give fewer CTAs than SMs, the T FFT slots are cut into up to 32 segments
-// of at least 64 FFTs (tlen a multiple of 16), at most two CTAs per SM in all.  A function of the
-// job's geometry only (not of the tile variant), so a batch and the single-job path cut a job the
-// same way and sum it in the same order, tuned or not.
+// CTAs of the plain X kernel of nsig signals and tile variant alt resident on one SM
+template <int NB, int CG, int TK>
+static cudaError_t occ_x(int* per_sm)
+{
+    using P = XPlan<NB, CG, TK>;
+    const size_t sm = 2 * (size_t)P::STAGE * sizeof(float2);
+    auto kern = k_xplain<NB, CG, TK>;
+    static unsigned configured = 0;
+    cudaError_t e = set_smem_once(kern, sm, &configured);
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, kern, P::NTHREADS, sm);
+}
+
+static cudaError_t xplain_occupancy(int nsig, int alt, int* per_sm)
+{
+    const int nb = (nsig + 7) / 8;
+#define FX_OP(NB_, CG_, TK_) return occ_x<NB_, CG_, TK_>(per_sm)
+    FX_XPLANS(FX_OP)
+#undef FX_OP
+}
+
+// Time segments of the plain X stage (up to 64 signals).  With C CTAs of channel groups (default
+// tile variant) and R = SMs x resident CTAs of its kernel, cutting the T FFT slots into s segments
+// of L = ceil(T / s) slots (a multiple of 16, at least 64) takes about ceil(C s / R) waves of L + 32
+// slots each (32: a CTA's fixed cost, its first stage load and its partial sums); the s of the
+// least time is taken, up to 32 (s = 1: no segments, the CTAs add to the accumulators).  A
+// function of the job's geometry and the device only (not of the tile variant), so a batch and the
+// single-job path cut a job the same way and sum it in the same order, tuned or not.
 void xplain_segments(int nsig, int nchan, int nsb, int T, int nsm, int* tseg, int* tlen)
 {
     *tseg = 1;
     *tlen = T;
-    if (nsig > 64 || nsig < 1) return;
-    const int ctas = nchan / xplain_channel_group(nsig, 0) * nsb;
-    if (ctas >= nsm) return;
-    int s = 1;
-    while (s < 32 && ctas * 2 * s <= 2 * nsm && T / (2 * s) >= 64) s *= 2;
-    if (s == 1) return;
-    const int len = ((T + s - 1) / s + 15) / 16 * 16;
-    *tlen = len;
-    *tseg = (T + len - 1) / len;
+    if (nsig > 64 || nsig < 1 || T < 128) return;
+    const long long ctas = (long long)(nchan / xplain_channel_group(nsig, 0)) * nsb;
+    int occ = 0;
+    if (xplain_occupancy(nsig, 0, &occ) != cudaSuccess || occ < 1) {
+        (void)cudaGetLastError();
+        occ = 1;
+    }
+    const long long slots = (long long)nsm * occ;
+    auto cost = [&](int len) {
+        const long long nseg = (T + len - 1) / len;
+        return ((ctas * nseg + slots - 1) / slots) * (long long)(len + 32);
+    };
+    int best_len = T;
+    long long best = cost(T);
+    for (int sg = 2; sg <= 32; sg++) {
+        const int len = ((T + sg - 1) / sg + 15) / 16 * 16;
+        if (len < 64) break;
+        const long long c = cost(len);
+        if (c < best) {
+            best = c;
+            best_len = len;
+        }
+    }
+    if (best_len >= T) return;
+    *tlen = best_len;
+    *tseg = (T + best_len - 1) / best_len;
 }
 
 int xplain_channel_group(int nsig, int alt)
