@@ -261,18 +261,19 @@ int ctx_create(const fxc_config* cfg, fxc_ctx** out, bool group_subbands)
     x->pitch = round_up(x->subint + 16, 256);
     x->rows = (int)round_up((size_t)2 * x->nsig, 128);
 
-    // Spectra chunk: T FFT slots of nsb_g subbands within a budget of 2 GiB (plain) / 16 GiB
-    // (tensor cores), or FXC_SPECTRA_BUDGET_MB.  Every subband goes into one chunk while that leaves >= 512 slots (or the
-    // whole call); larger problems take the subbands in groups so the chunk stays long: the
-    // tensor-core X stage adds each chunk's Gram to the accumulators once, so short chunks
-    // would make it bound by those additions.
+    // Spectra chunk: T FFT slots of nsb_g subbands within a budget of 16 GiB, or
+    // FXC_SPECTRA_BUDGET_MB.  Every subband goes into one chunk while that leaves >= 512 slots (or the
+    // whole call); larger problems take the subbands in groups so the chunk stays long: both X
+    // stages add each chunk's sums to the accumulators once per CTA, so short chunks make them
+    // bound by those additions and by each CTA's pipeline fill (the plain X stage at 64 signals
+    // x 1024 channels x 8 subbands: 40.9 TFLOP/s at 2 GiB = 504 slots, 48.4 at 16 GiB).
     // Bytes per FFT slot and subband: plain f32x2 [sb][sig][T][chan]; TC f16 [sb][chan][rows][T]
     // (the FP8 form adds an e4m3 copy of half that size; its chunk is a multiple of 128 FFTs).
     const bool tc = c.xmode != FXC_X_PLAIN_FP32;
     const bool fp8 = c.xmode == FXC_X_TC_FP8;
     const size_t tq = fp8 ? 128 : 64;
     const size_t per_sb = tc ? (size_t)c.nchan * x->rows * sizeof(uint16_t) : (size_t)x->nsig * c.nchan * sizeof(float2);
-    size_t budget = (size_t)(tc ? 16 : 2) << 30;
+    size_t budget = (size_t)16 << 30;
     if (const char* mb = std::getenv("FXC_SPECTRA_BUDGET_MB")) {   // operator override of the budget
         const long long v = std::atoll(mb);
         if (v > 0) budget = (size_t)v << 20;
