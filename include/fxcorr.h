@@ -61,7 +61,7 @@ typedef struct fxc_config {
     double bw;         /* bandwidth per subband, Hz; sampling interval 1/(2 bw) (kernel.c:14) */
     double sb_spacing; /* LO step between consecutive subbands, Hz */
     int chunk_ffts;    /* FFTs per F->X chunk (multiple of 64), 0 = chosen by the library: the
-                          spectra of a chunk stay within 2 GiB (plain) / 16 GiB (tensor cores), or
+                          spectra of a chunk stay within 16 GiB, or
                           the environment variable FXC_SPECTRA_BUDGET_MB; problems too large for
                           long chunks of every subband are chunked over groups of subbands */
     int window_ffts;   /* FFTs per streamed input window (fxc_process_host*); 0 = the chunk length,
