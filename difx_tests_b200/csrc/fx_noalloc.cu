@@ -18,8 +18,7 @@
 //
 // In host code the array's name is only a host-side stand-in; its device
 // address is obtained once per device with cudaGetSymbolAddress (with that
-// device current) and cached.  The first call on a device performs that
-// lookup, so make the first call before any stream capture begins.
+// device current) and cached by the first call on that device.
 //
 // A bounded device wait of the F stage that runs out (its input copy never
 // completed) is reported in the outputs, since the call returns before the GPU

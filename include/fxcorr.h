@@ -203,9 +203,7 @@ int fxc_host_free(void* p);
  * (FXC_ERR_UNSUPPORTED otherwise).  Work is queued on `stream` (a cudaStream_t,
  * NULL = legacy default stream); the call returns before it completes, so a
  * device wait that runs out is reported in the outputs instead: every
- * visibility NaN and every count -6.  The first call on a device looks up the
- * array's device address, so make it before any stream capture starts.  All
- * calls share the array: calls that overlap on the GPU race, so order them (one
+ * visibility NaN and every count -6.  All calls share the array: calls that overlap on the GPU race, so order them (one
  * stream, or events). */
 #define FXC_NOALLOC_SCRATCH_BYTES (64u << 20)
 int fxc_correlate_noalloc(const fxc_config* cfg, const uint8_t* d_data, size_t pitch, const double* delays,
