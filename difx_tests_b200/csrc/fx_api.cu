@@ -267,12 +267,25 @@ int ctx_create(const fxc_config* cfg, fxc_ctx** out, bool group_subbands)
     // stages add each chunk's sums to the accumulators once per CTA, so short chunks make them
     // bound by those additions and by each CTA's pipeline fill (the plain X stage at 64 signals
     // x 1024 channels x 8 subbands: 40.9 TFLOP/s at 2 GiB = 504 slots, 48.4 at 16 GiB).
-    // Bytes per FFT slot and subband: plain f32x2 [sb][sig][T][chan]; TC f16 [sb][chan][rows][T]
-    // (the FP8 form adds an e4m3 copy of half that size; its chunk is a multiple of 128 FFTs).
+    // Bytes per FFT slot and subband: f32x2 [sb][sig][T][chan] (plain, and the FP16 tensor-core
+    // form of up to 64 signals on the FFT F stage: its X stage casts while loading); otherwise
+    // f16 [sb][chan][rows][T] (the FP8 form adds an e4m3 copy of half that size; its chunk is a
+    // multiple of 128 FFTs).  The F stage's FP32 stores are channel-contiguous, its FP16 K-major
+    // stores a corner turn through shared memory per block of FFTs (2048 points, 1 pol: 107 against
+    // 90 ms per cfg2 step; 4096 points, 2 pol: 61 against 47 ms per cfg1 step).
+    // FXC_TC_SPECTRA=f16 keeps the FP16 layout for every tensor-core form (comparisons).
     const bool tc = c.xmode != FXC_X_PLAIN_FP32;
     const bool fp8 = c.xmode == FXC_X_TC_FP8;
+    {
+        const char* ts = std::getenv("FXC_TC_SPECTRA");
+        const bool force16 = ts && std::strcmp(ts, "f16") == 0;
+        x->xf32 = c.xmode == FXC_X_TC_FP16 && (c.fstage == FXC_F_AUTO || c.fstage == FXC_F_FFT32) && x->nsig <= 64 &&
+                  c.nchan % 4 == 0 && !force16;
+        x->spec_mode = (tc && !x->xf32) ? kSpecF16 : kSpecF32;
+    }
     const size_t tq = fp8 ? 128 : 64;
-    const size_t per_sb = tc ? (size_t)c.nchan * x->rows * sizeof(uint16_t) : (size_t)x->nsig * c.nchan * sizeof(float2);
+    const size_t per_sb = x->spec_mode == kSpecF16 ? (size_t)c.nchan * x->rows * sizeof(uint16_t)
+                                                   : (size_t)x->nsig * c.nchan * sizeof(float2);
     size_t budget = (size_t)16 << 30;
     if (const char* mb = std::getenv("FXC_SPECTRA_BUDGET_MB")) {   // operator override of the budget
         const long long v = std::atoll(mb);
@@ -606,7 +619,7 @@ static int ctx_correlate(fxc_ctx* x, const uint8_t* d_data, size_t pitch, const 
         {
             StageScope sc(x, 1, 1);
             if (fp8) FXC_CK(cudaMemsetAsync(x->d_amax, 0, sizeof(unsigned) * xa.nsb * xa.nchan * xa.nsig, x->stream));
-            FXC_CK(launch_fstage(x->cfg.nchan, tc ? kSpecF16 : kSpecF32, fa, x->stream));
+            FXC_CK(launch_fstage(x->cfg.nchan, x->spec_mode, fa, x->stream));
         }
         {
             StageScope sc(x, 2, fp8 ? 2 : 1);
@@ -619,7 +632,9 @@ static int ctx_correlate(fxc_ctx* x, const uint8_t* d_data, size_t pitch, const 
                 x8.inv_scale = x->d_inv;
                 FXC_CK(launch_xtc8(x8, x->d_err, x->nsm, x->stream));
             } else {
-                FXC_CK(tc ? launch_xtc(xa, x->d_err, x->nsm, x->stream) : launch_xplain(xa, x->stream));
+                FXC_CK(!tc ? launch_xplain(xa, x->stream)
+                           : x->xf32 ? launch_xtc32(xa, x->d_err, x->nsm, x->stream)
+                                     : launch_xtc(xa, x->d_err, x->nsm, x->stream));
             }
         }
     }
@@ -933,7 +948,7 @@ int fxc_autotune(fxc_ctx* x, int reps)
     for (int tb : {8, 16, 32}) {
         fa.tb = tb;
         float ms = 0.f;
-        err = timeit([&] { return launch_fstage(c.nchan, tc ? kSpecF16 : kSpecF32, fa, x->stream); }, &ms);
+        err = timeit([&] { return launch_fstage(c.nchan, x->spec_mode, fa, x->stream); }, &ms);
         if (err != cudaSuccess) break;
         if (ms < best) {
             best = ms;

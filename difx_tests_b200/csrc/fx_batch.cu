@@ -31,7 +31,7 @@ using namespace fx;
 namespace {
 
 struct FGroup {
-    int nchan, npol, mode, tb;   // mode: kSpecF32 (plain X) or kSpecF16 (tensor-core X)
+    int nchan, npol, mode, tb;   // mode: the jobs' spectra layout (fxc_ctx::spec_mode)
     std::vector<int> jobs;
 };
 struct XGroup {
@@ -213,7 +213,9 @@ static int enqueue_launch(fxc_batch* b, const Launch& l)
     } else {
         fxc_ctx* c = b->ctx[l.group];
         const XArgs& x = b->xa_host[(size_t)l.round * b->ctx.size() + l.group];
-        FB_CK(c->cfg.xmode == FXC_X_TC_FP16 ? launch_xtc(x, c->d_err, c->nsm, b->stream) : launch_xplain(x, b->stream));
+        FB_CK(c->cfg.xmode != FXC_X_TC_FP16 ? launch_xplain(x, b->stream)
+              : c->xf32                     ? launch_xtc32(x, c->d_err, c->nsm, b->stream)
+                                            : launch_xtc(x, c->d_err, c->nsm, b->stream));
     }
     return FXC_OK;
 }
@@ -273,7 +275,7 @@ int fxc_batch_create(const fxc_config* cfgs, int njobs, fxc_batch** out)
     const auto plans = plan_cache_load();
     for (int j = 0; j < njobs; j++) {
         const fxc_ctx* c = b->ctx[j];
-        const int mode = c->cfg.xmode == FXC_X_PLAIN_FP32 ? kSpecF32 : kSpecF16;
+        const int mode = c->spec_mode;   // the layout the job's X stage reads
         int g = -1;
         for (int k = 0; k < (int)b->fg.size(); k++)
             if (b->fg[k].nchan == c->cfg.nchan && b->fg[k].npol == c->cfg.npol && b->fg[k].mode == mode) g = k;

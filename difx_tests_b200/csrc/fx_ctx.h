@@ -33,6 +33,11 @@ struct fxc_ctx {
     uint32_t* d_vbits = nullptr;
     void* d_spec = nullptr;
     size_t spec_bytes = 0;
+    // F-stage output layout: kSpecF32 [sb][sig][T][chan] (the plain form, and the FP16 tensor-core
+    // form of up to 64 signals on the FFT F stage, whose X stage casts to FP16 on the way into the
+    // MMA operand: xf32) or kSpecF16 K-major [sb][chan][rows][T] (the other tensor-core forms)
+    int spec_mode = 0;
+    bool xf32 = false;
     uint8_t* d_spec8 = nullptr;   // FP8 form: e4m3 spectra [nsb][nchan][rows][T]
     unsigned* d_amax = nullptr;   // FP8 form: [nsb*nchan][nsig] absmax bits of the chunk
     float* d_inv = nullptr;       // FP8 form: [nsb*nchan][nsig] inverse scales

@@ -39,6 +39,8 @@ cudaError_t launch_xplain_batch(int nsig, int alt, const XArgs* d_jobs, const in
                                 cudaStream_t st);
 int xplain_channel_group(int nsig, int alt);
 cudaError_t launch_xtc(const XArgs& a, int* d_err, int nsm, cudaStream_t st);
+// the same Gram on the plain form's FP32 spectra, cast to FP16 in shared memory (up to 64 signals)
+cudaError_t launch_xtc32(const XArgs& a, int* d_err, int nsm, cudaStream_t st);
 // FP8 form: e4m3 copy of the F16 spectra scaled by 448/absmax per (item = sb*nchan + chan, signal),
 // then the e4m3 Gram with the inverse scales applied per product
 cudaError_t launch_cast_fp8(const void* spec16, const unsigned* amax, int rows, int nsig, int T, int ts, int nitems,

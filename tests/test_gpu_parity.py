@@ -218,6 +218,35 @@ def test_tc_vis_vs_fp64_oracle(nant, npol, nchan, nsb, numffts):
         assert mx.max() < TC_MAX_TOL, f"max {mx.max():.3e}"
 
 
+@pytest.mark.parametrize("nant,npol,nchan,nsb,numffts,chunk,calls",
+                         [(8, 2, 256, 2, 300, 128, [(0, 150), (150, 150)]),
+                          (64, 1, 1024, 1, 256, 0, [(0, 256)]),
+                          (5, 2, 4096, 1, 100, 0, [(0, 100)]),
+                          (3, 1, 128, 3, 200, 64, [(0, 77), (77, 123)]),
+                          (33, 1, 512, 1, 130, 0, [(0, 130)])])
+def test_tc_fp32_spectra_path_bit_identical(nant, npol, nchan, nsb, numffts, chunk, calls, monkeypatch):
+    """The FP16 tensor-core form of up to 64 signals reads the FFT F stage's FP32 spectra and casts
+    to FP16 in the X stage; with FXC_TC_SPECTRA=f16 the F stage writes the FP16 K-major layout
+    instead.  Same FP16 values, same MMAs in the same order: the same visibilities, bit for bit."""
+    job = synth.make_job(nant=nant, npol=npol, nchan=nchan, numffts=numffts, bw=64e6, lo=1.4e9, rho=0.1,
+                         seed=nant * 11 + nchan, nsubband=nsb)
+    out = {}
+    for layout in ("f32", "f16"):
+        if layout == "f16":
+            monkeypatch.setenv("FXC_TC_SPECTRA", "f16")
+        else:
+            monkeypatch.delenv("FXC_TC_SPECTRA", raising=False)
+        with corr_for(job, xmode=fx.FXC_X_TC_FP16, chunk_ffts=chunk) as c:
+            for first, n in calls:
+                c.process(job.data, job.delays, job.fileoffsets, first, n)
+            out[layout] = c.visibilities()
+    np.testing.assert_array_equal(out["f32"][1], out["f16"][1])
+    np.testing.assert_array_equal(out["f32"][0], out["f16"][0])
+    ref, _ = oracle_vis(job, 0)
+    mx, rms = fo.vis_error(out["f32"][0][0], ref)
+    assert rms.max() < TC_RMS_TOL and mx.max() < TC_MAX_TOL
+
+
 def test_tc_matches_plain_and_accumulates_over_chunks():
     job = synth.make_job(nant=24, npol=1, nchan=1024, numffts=300, bw=64e6, lo=1.4e9, rho=0.1, seed=31)
     out = {}
