@@ -400,6 +400,17 @@ def form_params(form, w):
     return xmode, fstage
 
 
+def spectra_f16(xmode, fstage, w):
+    """Whether the F stage writes the FP16 K-major spectra layout: the tensor-core forms, except the
+    FP16 form on the FFT F stage at up to 64 signals and a multiple of 4 channels, whose X stage
+    reads FP32 spectra and casts them itself (the library's rule, fx_api.cu ctx_create)."""
+    import difx_tests_b200 as fx
+    if xmode == fx.FXC_X_PLAIN_FP32:
+        return False
+    return not (xmode == fx.FXC_X_TC_FP16 and fstage in (0, 1) and w["nant"] * w["npol"] <= 64
+                and w["nchan"] % 4 == 0 and os.environ.get("FXC_TC_SPECTRA") != "f16")
+
+
 def form_dtype(form, w):
     """dtype label of the form as it runs on w (a tensor-core F form that fell back reads as tc)."""
     return DTYPES[form] if form_params(form, w) == FORMS[form] else DTYPES["tc"]
@@ -515,7 +526,7 @@ def run_gpu_arm(args):
 
     # ---- roofline of the dominant kernel of the headline form (the F stage)
     hbm, tc_peak, peak_kind = peaks()
-    f16 = xmode != fx.FXC_X_PLAIN_FP32
+    f16 = spectra_f16(xmode, fstage, w)
     spec_bpc = 4 if f16 else 8       # bytes per complex spectrum value written
     f_bytes = head["samples_per_launch"] * (0.25 + 0.5 * spec_bpc)
     f_gbs = f_bytes / (head["f_ms_launch"] / 1e3) / 1e9

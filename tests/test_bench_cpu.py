@@ -42,3 +42,18 @@ def test_form_parameters_fall_back_where_the_tensor_core_f_stages_do_not_apply()
     assert bench.form_params("tc32f", w2) == (1, 3) and bench.form_params("tc16f", w2) == (1, 2)
     assert bench.form_params("tc32f", w1) == (1, 1) and bench.form_params("fp8", w1) == (2, 1)
     assert "k_ftc32" in bench.form_dtype("tc32f", w2) and "FFT" in bench.form_dtype("tc32f", w1)
+
+
+def test_spectra_layout_follows_the_library_rule(monkeypatch):
+    """The F stage writes FP32 spectra for the FP16 tensor-core form on the FFT at up to 64 signals
+    (its X stage casts them), FP16 K-major for the other tensor-core forms and geometries."""
+    monkeypatch.delenv("FXC_TC_SPECTRA", raising=False)
+    w1, w2 = bench.WORKLOADS["cfg1"], bench.WORKLOADS["cfg2"]
+    w4 = dict(w1, nant=256)                                 # the large array: 512 signals
+    assert not bench.spectra_f16(0, 1, w2)                 # plain
+    assert not bench.spectra_f16(1, 1, w1) and not bench.spectra_f16(1, 1, w2)   # tc on the FFT
+    assert bench.spectra_f16(1, 3, w2) and bench.spectra_f16(1, 2, w2)          # tensor-core F stages
+    assert bench.spectra_f16(2, 1, w2)                      # FP8
+    assert bench.spectra_f16(1, 1, w4)                      # 512 signals
+    monkeypatch.setenv("FXC_TC_SPECTRA", "f16")
+    assert bench.spectra_f16(1, 1, w1)
