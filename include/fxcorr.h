@@ -44,7 +44,10 @@ extern "C" {
 
 /* X-stage arithmetic */
 #define FXC_X_PLAIN_FP32 0        /* FP32 CUDA-core cross-multiply-accumulate */
-#define FXC_X_TC_FP16    1        /* tcgen05 tensor cores, FP16 inputs, FP32 accumulation */
+#define FXC_X_TC_FP16    1        /* tcgen05 tensor cores, FP16 inputs, FP32 accumulation (on the FFT F
+                                     stage with <= 64 signals the F stage writes FP32 spectra and the X
+                                     stage rounds them to FP16 itself; FXC_TC_SPECTRA=f16 in the
+                                     environment at context creation keeps the F stage's FP16 layout) */
 #define FXC_X_TC_FP8     2        /* tcgen05 tensor cores, FP8-E4M3 inputs scaled per antenna, polarisation and
                                      channel by 448/absmax over each spectra chunk, FP32 accumulation */
 
