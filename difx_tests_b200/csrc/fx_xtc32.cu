@@ -15,7 +15,7 @@
 // of each spectrum row, so every DRAM sector fetched is used once):
 //   warp 0     TMA producer: box {4 channels, 32 FFTs, nsig signals} of the FP32 spectra
 //              (unswizzled: {Re, Im} of the 4 channels of FFT t of signal s at 1024 s + 32 t)
-//              into a ring of FP32 stages
+//              into a ring of FP32 stages (as many as 128 KB holds: 2 at 64 signals, 4 at 32)
 //   warp 1     MMA issuer: per stage and channel 2 x tcgen05.mma.kind::f16 M128 N128 K16 on the
 //              channel's FP16 tile (A and B descriptors the same tile)
 //   warps 2-9  cast: FP32 stage j -> K half j % 2 (FFTs 32 (j % 2) .. + 31) of the four channels'
@@ -42,8 +42,8 @@ namespace tcx32 {
 constexpr int BT = 32;                       // FFTs per FP32 stage (a K half of the FP16 tiles)
 constexpr int CB = 4;                        // channels per work item
 constexpr int MAXSIG = 64;
-constexpr int NS32 = 2;                      // FP32 stages
-constexpr int F32_BYTES = MAXSIG * BT * CB * 8;   // 64 KB: [sig][t][ch] float2
+constexpr int RING_BYTES = 2 * MAXSIG * BT * CB * 8;   // 128 KB of FP32 stages ([sig][t][ch] float2):
+constexpr int MAXS32 = 8;                    // 2 at 64 signals, 4 at 32, up to 8
 constexpr int TILE_BYTES = 128 * 128;        // 128 rows x 64 FP16
 constexpr int NCW = 8;                       // cast warps
 constexpr int NTHREADS = 32 * (2 + NCW + 4);   // producer, MMA, cast, 4 epilogue warps
@@ -51,10 +51,10 @@ constexpr int TMEM_COLS = 512;               // 4 channels x 128 FP32 columns
 constexpr uint32_t kIdesc = tc::idesc_f16(128, 128);
 
 struct Smem {
-    alignas(1024) uint8_t f32[NS32][F32_BYTES];
+    alignas(1024) uint8_t f32[RING_BYTES];
     alignas(1024) uint8_t f16[CB][TILE_BYTES];
-    alignas(8) uint64_t full32[NS32];
-    uint64_t empty32[NS32];
+    alignas(8) uint64_t full32[MAXS32];
+    uint64_t empty32[MAXS32];
     uint64_t full16[2];                      // per K half
     uint64_t empty16[2];
     uint64_t acc_full;
@@ -102,9 +102,10 @@ k_xtc32(const __grid_constant__ CUtensorMap tmap, XArgs a, int* err)
     const int nitems = a.nsb * ncq;
     const int nk = (a.ntk ? a.ntk : a.T) / BT;    // FP32 stages per item (even)
     const uint32_t stage_bytes = (uint32_t)nsig * BT * CB * 8;
+    const int ns32 = min(MAXS32, (int)(RING_BYTES / stage_bytes));   // FP32 stages in flight
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < NS32; s++) {
+        for (int s = 0; s < ns32; s++) {
             mbar_init(&sm.full32[s], 1);
             mbar_init(&sm.empty32[s], NCW);   // one arrival per cast warp
         }
@@ -152,20 +153,20 @@ k_xtc32(const __grid_constant__ CUtensorMap tmap, XArgs a, int* err)
                         break;
                     }
                     mbar_expect_tx(&sm.full32[stage], stage_bytes);
-                    tma_load_4d(&tmap, &sm.full32[stage], sm.f32[stage], c0, kb * BT, 0, sb);
+                    tma_load_4d(&tmap, &sm.full32[stage], sm.f32 + (size_t)stage * stage_bytes, c0, kb * BT, 0, sb);
                     issued++;
-                    if (++stage == NS32) {
+                    if (++stage == ns32) {
                         stage = 0;
                         phase ^= 1;
                     }
                 }
             }
-            // drain: the last NS32 fills are the only ones that may still be in flight
-            for (int s = 0; s < NS32 && issued > 0; s++) {
+            // drain: the last ns32 fills are the only ones that may still be in flight
+            for (int s = 0; s < ns32 && issued > 0; s++) {
                 const long long idx = issued - 1 - s;
                 if (idx < 0) break;
-                const int st = (int)(idx % NS32);
-                const uint32_t ph = (uint32_t)((idx / NS32) & 1);
+                const int st = (int)(idx % ns32);
+                const uint32_t ph = (uint32_t)((idx / ns32) & 1);
                 const unsigned long long t0 = globaltimer();
                 while (!mbar_try(&sm.full32[st], ph)) {
                     if (globaltimer() - t0 > WAIT_NS) {
@@ -274,7 +275,7 @@ k_xtc32(const __grid_constant__ CUtensorMap tmap, XArgs a, int* err)
                     stop = true;
                     break;
                 }
-                const uint8_t* src = sm.f32[s32];
+                const uint8_t* src = sm.f32 + (size_t)s32 * stage_bytes;
                 const int k = 4 * h + kq;                      // chunk of the 128-byte tile row
                 // four signals per pass, their reads issued together (the chain read -> shuffles ->
                 // stores of one signal is latency-bound)
@@ -309,7 +310,7 @@ k_xtc32(const __grid_constant__ CUtensorMap tmap, XArgs a, int* err)
                     mbar_arrive(&sm.empty32[s32]);
                     mbar_arrive(&sm.full16[h]);
                 }
-                if (++s32 == NS32) {
+                if (++s32 == ns32) {
                     s32 = 0;
                     ph32 ^= 1;
                 }
