@@ -22,8 +22,9 @@
 //              FP16 tiles, 128 rows x 64 FFTs, K-major SWIZZLE_128B, rows >= 2 nsig zero; the two
 //              halves of a tile are disjoint, so the cast fills one while the MMAs read the other
 //   warps 10-13 epilogue: tcgen05.ld of the four channels' accumulators (512 TMEM columns), Re/Im
-//              combination, FP32 accumulate into acc[sb][c][pair(i,j)], i <= j; an item is 2 T / 64
-//              stages long, so its epilogue is a small part of it.
+//              combination, FP32 accumulate into acc[sb][c][pair(i,j)], i <= j; an item is T / 32
+//              stages long, so its epilogue (one accumulator set, not double-buffered) is a small
+//              part of it.
 // Every wait is bounded by time; on expiry the CTA records an error code, drains what it
 // issued (again bounded), frees TMEM and returns.
 #include <cuda.h>
