@@ -246,7 +246,8 @@ k_xtc32(const __grid_constant__ CUtensorMap tmap, XArgs a, int* err)
         // of {Re, Im} of the four channels per (s, t).  The 8 lanes of FFTs 8q .. 8q+7 then
         // transpose through shuffles: lane L writes word L % 4 (FFTs 2w, 2w+1) of the Re (L % 8 < 4)
         // or Im row of signal s, chunk 4h + q, in each channel's tile (the Re and Im rows' chunks
-        // differ after the swizzle, so the stores do not conflict).
+        // differ after the swizzle, so the 8 lanes of a group hit 8 banks; groups q and q ^ 1 meet,
+        // so a store takes at most two bank passes).
         const int t = lane;
         const int kq = t >> 3;
         const int w = lane & 3;
