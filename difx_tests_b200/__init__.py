@@ -114,6 +114,7 @@ SIGNATURES = {
     "fxc_debug_spectra": (_I, [_P, _DP, _DP, _I, _I, _FP]),
     "fxc_debug_expire_wait": (_I, [_P]),
     "fxc_debug_expire_wait_tc": (_I, [_P]),
+    "fxc_debug_xplain_segments": (_I, [C.c_longlong, C.c_longlong, _I, _IP, _IP]),
 }
 
 

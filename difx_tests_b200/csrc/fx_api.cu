@@ -561,6 +561,13 @@ extern "C" {
 
 }  // extern "C"
 
+extern "C" int fxc_debug_xplain_segments(long long ctas, long long slots, int T, int* tseg, int* tlen)
+{
+    if (!tseg || !tlen || T < 0) return FXC_ERR_INVALID;
+    xplain_segment_model(ctas, slots, T, tseg, tlen);
+    return FXC_OK;
+}
+
 // The plain X stage's time segments of this context and tile variant (fx_xplain.cu)
 void ctx_xsegments(const fxc_ctx* x, XArgs& xa)
 {

@@ -33,6 +33,7 @@ cudaError_t launch_fstage_batch(int nchan, int npol, int mode, int tb, const FAr
                                 int ntask, cudaStream_t st);
 cudaError_t launch_xplain_reduce(const XArgs& a, cudaStream_t st);
 void xplain_segments(int nsig, int nchan, int nsb, int T, int nsm, int* tseg, int* tlen);
+void xplain_segment_model(long long ctas, long long slots, int T, int* tseg, int* tlen);
 int xplain_segments_used(const XArgs& a);
 cudaError_t launch_xplain(const XArgs& a, cudaStream_t st);
 cudaError_t launch_xplain_batch(int nsig, int alt, const XArgs* d_jobs, const int4* d_tasks, int ntask,

@@ -578,18 +578,11 @@ static cudaError_t xplain_occupancy(int nsig, int alt, int* per_sm)
 // least time is taken, up to 32 (s = 1: no segments, the CTAs add to the accumulators).  A
 // function of the job's geometry and the device only (not of the tile variant), so a batch and the
 // single-job path cut a job the same way and sum it in the same order, tuned or not.
-void xplain_segments(int nsig, int nchan, int nsb, int T, int nsm, int* tseg, int* tlen)
+void xplain_segment_model(long long ctas, long long slots, int T, int* tseg, int* tlen)
 {
     *tseg = 1;
     *tlen = T;
-    if (nsig > 64 || nsig < 1 || T < 128) return;
-    const long long ctas = (long long)(nchan / xplain_channel_group(nsig, 0)) * nsb;
-    int occ = 0;
-    if (xplain_occupancy(nsig, 0, &occ) != cudaSuccess || occ < 1) {
-        (void)cudaGetLastError();
-        occ = 1;
-    }
-    const long long slots = (long long)nsm * occ;
+    if (ctas < 1 || slots < 1 || T < 128) return;
     auto cost = [&](int len) {
         const long long nseg = (T + len - 1) / len;
         return ((ctas * nseg + slots - 1) / slots) * (long long)(len + 32);
@@ -608,6 +601,20 @@ void xplain_segments(int nsig, int nchan, int nsb, int T, int nsm, int* tseg, in
     if (best_len >= T) return;
     *tlen = best_len;
     *tseg = (T + best_len - 1) / best_len;
+}
+
+void xplain_segments(int nsig, int nchan, int nsb, int T, int nsm, int* tseg, int* tlen)
+{
+    *tseg = 1;
+    *tlen = T;
+    if (nsig > 64 || nsig < 1 || T < 128) return;
+    const long long ctas = (long long)(nchan / xplain_channel_group(nsig, 0)) * nsb;
+    int occ = 0;
+    if (xplain_occupancy(nsig, 0, &occ) != cudaSuccess || occ < 1) {
+        (void)cudaGetLastError();
+        occ = 1;
+    }
+    xplain_segment_model(ctas, (long long)nsm * occ, T, tseg, tlen);
 }
 
 int xplain_channel_group(int nsig, int alt)

@@ -315,6 +315,12 @@ int fxc_debug_expire_wait(fxc_ctx* ctx);
  * the next synchronising call returns FXC_ERR_TIMEOUT and fxc_last_device_error() gives 7. */
 int fxc_debug_expire_wait_tc(fxc_ctx* ctx);
 
+/* The plain X stage's time-segment cut (up to 64 signals) for `ctas` CTAs of channel groups,
+ * `slots` resident CTA slots (SMs x CTAs of the kernel per SM) and T FFT slots per chunk:
+ * *tseg segments of *tlen slots (1 and T: no cut).  Host arithmetic only; the library takes
+ * the occupancy of its default tile variant on the context's GPU for `slots`. */
+int fxc_debug_xplain_segments(long long ctas, long long slots, int T, int* tseg, int* tlen);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif
